@@ -1,0 +1,115 @@
+/*
+ * svp3d.h -- C ABI of libsvp3d, the B200 (sm_100a) implementation of the certified-registration hot path of
+ * seq_vp_3d (Python package jd_curl): the whole-cell Jacobian-determinant certificate, the cubic B-spline image
+ * sampler, the per-cell Q1 energy/gradient/GGN kernels and the DST-I Poisson preconditioner.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer unless its comment says "host".
+ *  - Node fields are C-order (nz, ny, nx, 3) float64 with components x, y, z (x fastest in memory); cell c has
+ *    coordinates x0 = c % cx, y0 = (c / cx) % cy, z0 = c / (cx cy) with (cx, cy, cz) = (nx-1, ny-1, nz-1) and vertex
+ *    a = x + 2y + 4z.  Free-node vectors ("theta") are component-major (3, nz-2, ny-2, nx-2).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are stream-ordered; a call that returns host
+ *    results (marked "synchronizes") waits for its stream.
+ *  - Every function returns SVP_OK (0) or an error code; svp_last_error() gives the calling thread's message.
+ *    No function frees memory it did not allocate.  Handles are not shared between threads without external
+ *    locking; separate handles may be used concurrently on separate streams.
+ */
+#ifndef SVP3D_H
+#define SVP3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SVP_OK 0
+#define SVP_EINVAL 1   /* invalid argument (shape, size, pointer, configuration) */
+#define SVP_ECUDA 2    /* CUDA runtime error (launch, copy, device) */
+#define SVP_ENOMEM 3   /* device allocation failed */
+#define SVP_ENUMERIC 4 /* a numerical precondition failed (non-finite value, non-positive scale) */
+
+/* Rectangular node grid: nx, ny, nz nodes (each >= 2), spacing and origin per axis (x, y, z).
+ * Replaces jd_curl/three_d/grid.py:11 Grid3D / :49 make_grid_3d (the node axes are origin + h * arange(n)). */
+typedef struct svp_grid {
+    int64_t nx, ny, nz;
+    double hx, hy, hz;
+    double x0, y0, z0;
+} svp_grid;
+
+/* Copies the calling thread's last error message into buf (always NUL-terminated); returns its full length. */
+int svp_last_error(char *buf, size_t len);
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int svp_version(void);
+
+/* ============================================================================================ certificate
+ * Status codes: 0 certified_feasible, 1 infeasible, 2 uncertain.  Reason codes (index into this list):
+ *  0 positive_enclosure_cover  1 positive_bernstein_cover  2 JACOBIAN_VIOLATION  3 arithmetic_uncertain
+ *  4 subdivision_budget  5 NONFINITE_STATE  6 NONZERO_BOUNDARY  7 INVALID_DOMAIN  8 unsupported_arithmetic
+ *  9 sample_witness  10 subdivision_witness  11 box_budget  12 depth_budget
+ * Arithmetic: binary64 round-to-nearest with one outward ulp step (bit steps) after every interval operation, no
+ * FMA contraction, IEEE division -- the reference's exact operation sequence, so margins, verdicts and records are
+ * bit-identical to jd_curl's CPU certifier. */
+typedef struct svp_cert_config {
+    double delta;       /* J > delta is proven; 0 <= delta < 1 */
+    int64_t max_depth;  /* subdivision depth budget (reference default 48) */
+    int64_t max_boxes;  /* boxes per cell budget (reference default 255) */
+    int64_t tile_size;  /* cells per tile of the edge-hull flag rule (reference default 65536) */
+    int32_t prescreen;  /* 1: float Bernstein prescreen between hull and interval fallback (PrescreenCertificateConfig) */
+    int32_t reserved;
+} svp_cert_config;
+
+/* Mirrors feasibility.py:148-179 FeasibilityResult / PrescreenFeasibilityResult (state_hash and ids excluded). */
+typedef struct svp_cert_result {
+    int32_t status, reason;
+    int64_t n_cells_checked, n_uncertain, n_infeasible, n_boxes, max_depth, witness_cell; /* witness_cell -1: none */
+    int64_t n_fast_cells, n_fallback_cells, n_prescreen_cells;
+    int32_t has_min_jd, has_sampled_min;
+    double min_jd_lower_bound, min_margin_lower_bound, sampled_min_jd; /* NaN when absent */
+    double witness_point[3];                                           /* reference coordinates in [0,1]^3 or NaN */
+} svp_cert_result;
+
+/* One cell's subdivision verdict, mirrors feasibility.py:136 CellCertificate (status, reason, boxes, depth,
+ * min_margin_lower_bound, witness_reference_point). */
+typedef struct svp_cell_verdict {
+    int32_t status, reason, has_margin, has_witness;
+    int64_t boxes, depth;
+    double margin, witness[3];
+} svp_cell_verdict;
+
+/* Per-cell lo(J - delta) of the edge-hull enclosure and an invalid-step flag (1 = some operation non-finite or
+ * inverted).  Replaces compiled_enclosure.py:303 parallel_margins and backends/edge_hull_gpu.py:317
+ * GpuEdgeHull.margins.  margin: (ncell,) float64, flag: (ncell,) uint8. */
+int svp_edge_hull_margins(const svp_grid *g, const double *u, double delta, double *margin, uint8_t *flag,
+                          void *stream);
+
+/* Rigorous float Bernstein lower bounds of J over the listed cells (NaN where not finite).
+ * Replaces certificate_prescreen.py:125 prescreen_lower_bounds.  cells: (n,) int64 cell ids; out: (n,) float64. */
+int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, const int64_t *cells, int64_t n, double *out,
+                               void *stream);
+
+/* Interval J - delta at the closed27 points, its interval Bernstein coefficients and float64 samples of standalone
+ * cells.  Replaces compiled_fallback.py:330 fallback_arrays (per cell: ok[i] = 0 where the reference returns None).
+ * vertices: (n, 8, 3) displacements; spacing3: host (3,) hx, hy, hz; the five outputs are (n, 27) float64 in
+ * storage order 9 iz + 3 iy + ix; ok: (n,) uint8. */
+int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta, double *p_lo,
+                        double *p_hi, double *c_lo, double *c_hi, double *samples, uint8_t *ok, void *stream);
+
+/* Lowest-bound-first Bernstein subdivision of n cells (one warp per cell, heap in a stream-ordered scratch
+ * allocation).  Replaces feasibility.py:295 _classify.  Inputs (n, 27) from svp_fallback_arrays; out: (n,). */
+int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi, int64_t n,
+                       double delta, int64_t max_depth, int64_t max_boxes, svp_cell_verdict *out, void *stream);
+
+/* Whole-map certificate with owned workspace.  svp_certify_map replaces feasibility.py:393 certify_map and :558
+ * certify_map_owned (PrescreenCertificateConfig execution) and synchronizes; out is a host struct. */
+typedef struct svp_certifier svp_certifier;
+int svp_certifier_create(const svp_grid *g, const svp_cert_config *cfg, svp_certifier **out);
+int svp_certifier_destroy(svp_certifier *c);
+int svp_certify_map(svp_certifier *c, const double *u, svp_cert_result *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVP3D_H */

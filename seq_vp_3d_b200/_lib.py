@@ -1,0 +1,91 @@
+"""ctypes binding of libsvp3d.so (the sm_100a CUDA library built from seq_vp_3d_b200/csrc).
+
+There is no CPU fallback: if the library is missing or CUDA is unavailable, every entry point raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsvp3d.so")
+
+P, I64, D, I32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int32
+
+SVP_OK, SVP_EINVAL, SVP_ECUDA, SVP_ENOMEM, SVP_ENUMERIC = 0, 1, 2, 3, 4
+
+
+class SvpError(RuntimeError):
+    """A libsvp3d call returned a non-zero status."""
+
+    def __init__(self, code, message):
+        super().__init__(f"libsvp3d error {code}: {message}")
+        self.code = code
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", I64), ("ny", I64), ("nz", I64), ("hx", D), ("hy", D), ("hz", D),
+                ("x0", D), ("y0", D), ("z0", D)]
+
+
+class CertConfig(ctypes.Structure):
+    _fields_ = [("delta", D), ("max_depth", I64), ("max_boxes", I64), ("tile_size", I64),
+                ("prescreen", I32), ("reserved", I32)]
+
+
+class CertResult(ctypes.Structure):
+    _fields_ = [("status", I32), ("reason", I32), ("n_cells_checked", I64), ("n_uncertain", I64),
+                ("n_infeasible", I64), ("n_boxes", I64), ("max_depth", I64), ("witness_cell", I64),
+                ("n_fast_cells", I64), ("n_fallback_cells", I64), ("n_prescreen_cells", I64),
+                ("has_min_jd", I32), ("has_sampled_min", I32), ("min_jd_lower_bound", D),
+                ("min_margin_lower_bound", D), ("sampled_min_jd", D), ("witness_point", D * 3)]
+
+
+class CellVerdict(ctypes.Structure):
+    _fields_ = [("status", I32), ("reason", I32), ("has_margin", I32), ("has_witness", I32),
+                ("boxes", I64), ("depth", I64), ("margin", D), ("witness", D * 3)]
+
+
+# name -> argtypes (restype int)
+SIGNATURES = {
+    "svp_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+    "svp_version": [],
+    "svp_edge_hull_margins": [P, P, D, P, P, P],
+    "svp_prescreen_lower_bounds": [P, P, P, I64, P, P],
+    "svp_fallback_arrays": [P, I64, P, D, P, P, P, P, P, P, P],
+    "svp_classify_cells": [P, P, P, P, I64, D, I64, I64, P, P],
+    "svp_certifier_create": [P, P, P],
+    "svp_certifier_destroy": [P],
+    "svp_certify_map": [P, P, P, P],
+}
+
+_lib = None
+
+
+def load():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m seq_vp_3d_b200.build` (no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(4096)
+    load().svp_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(code):
+    if code != SVP_OK:
+        raise SvpError(code, last_error())
+    return code
+
+
+def call(name, *args):
+    return check(getattr(load(), name)(*args))

@@ -1,0 +1,1075 @@
+// Whole-cell Jacobian-determinant certificate on the GPU, bit-identical to the reference CPU certifier.
+//
+// Stages (jd_curl/three_d/feasibility.py:623 _certify_map_parallel):
+//   1. edge-hull interval enclosure of every cell (compiled_enclosure.py:210 _chunk_hoisted_margins),
+//      with the per-tile flag rule (feasibility.py:650);
+//   2. float Bernstein prescreen with an a-priori rounding bound (certificate_prescreen.py:66) of the unproven cells;
+//   3. interval Bernstein fallback arrays (compiled_fallback.py:63) and lowest-bound-first subdivision
+//      (feasibility.py:295 _classify), one warp per cell with the box heap in scratch memory;
+//   4. the record: status, reason, counts, bounds and the first witness (feasibility.py:755-771).
+// This file is compiled with -fmad=false and uses explicit round-to-nearest intrinsics for every certificate
+// operation, so no product can be contracted into an FMA.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "svp_common.cuh"
+
+namespace svp {
+namespace {
+
+struct CellGrid {
+    long long nx, ny, nz, cx, cy, cz, ncell;
+    double h[3];
+};
+
+CellGrid cell_grid(const svp_grid *g) {
+    CellGrid c;
+    c.nx = g->nx; c.ny = g->ny; c.nz = g->nz;
+    c.cx = g->nx - 1; c.cy = g->ny - 1; c.cz = g->nz - 1;
+    c.ncell = c.cx * c.cy * c.cz;
+    c.h[0] = g->hx; c.h[1] = g->hy; c.h[2] = g->hz;
+    return c;
+}
+
+__device__ __forceinline__ long long cell_base(long long c, const CellGrid &g) {
+    long long x0 = c % g.cx, y0 = (c / g.cx) % g.cy, z0 = c / (g.cx * g.cy);
+    return (z0 * g.ny + y0) * g.nx + x0;
+}
+__device__ __forceinline__ long long vnode(long long base, int a, long long ny, long long nx) {
+    return base + (long long)(a >> 2) * ny * nx + (long long)((a >> 1) & 1) * nx + (a & 1);
+}
+// e-th vertex with bit j clear, in increasing vertex order (the reference's edge loop order)
+__device__ __forceinline__ int edge_start(int j, int e) {
+    int k = 0;
+    for (int a = 0; a < 8; a++) {
+        if (a & (1 << j)) continue;
+        if (k == e) return a;
+        k++;
+    }
+    return 0;
+}
+
+// ============================================================================================== 1. edge hull
+// F_rj interval: hull of the 4 edge differences (from +inf / -inf in edge order), outward, /h, outward, + identity.
+__device__ __forceinline__ bool hull_entry(const double *__restrict__ u, long long base, long long ny, long long nx,
+                                           int j, int r, double h, double &lo, double &hi) {
+    bool ok = true;
+    double lower = __longlong_as_double(0x7FF0000000000000LL), upper = -lower;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        int a = edge_start(j, e), b = a | (1 << j);
+        double d = rsub(__ldg(u + 3 * vnode(base, b, ny, nx) + r), __ldg(u + 3 * vnode(base, a, ny, nx) + r));
+        ok &= finite64(d);
+        lower = nmin(lower, d);
+        upper = nmax(upper, d);
+    }
+    double l, hh;
+    ok &= iout(lower, upper, l, hh);
+    ok &= iout(rdiv(l, h), rdiv(hh, h), l, hh);
+    double id = (r == j) ? 1.0 : 0.0;
+    ok &= iadd(l, hh, id, id, lo, hi);
+    return ok;
+}
+
+__global__ void __launch_bounds__(256) edge_hull_kernel(const double *__restrict__ u, CellGrid g, double delta,
+                                                        double *__restrict__ margin, uint8_t *__restrict__ flag) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long base = cell_base(c, g);
+        double fl[3][3], fh[3][3];
+        bool ok = true;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) ok &= hull_entry(u, base, g.ny, g.nx, j, r, g.h[j], fl[r][j], fh[r][j]);
+        double jl, jh, ml, mh;
+        ok &= idet(fl, fh, jl, jh);
+        ok &= iout(rsub(jl, delta), rsub(jh, delta), ml, mh);
+        margin[c] = ml;
+        flag[c] = ok ? 0 : 1;
+    }
+}
+
+// ============================================================================================== 2. prescreen
+struct PrescreenConst {
+    double D[3 * 27 * 8];  // closed27 Q1 derivative table (3, 27, 8), passed by value (constant bank)
+    double g12, g6, g3, sq27, eta;
+    int usable;            // 0: table not finite or has a subnormal entry -> every bound NaN
+};
+
+__device__ double prescreen_cell(const double *__restrict__ u, long long base, long long ny, long long nx,
+                                 const PrescreenConst &k) {
+    long long off[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) off[a] = (long long)(a >> 2) * ny * nx + (long long)((a >> 1) & 1) * nx + (a & 1);
+    double uv[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) uv[a][r] = __ldg(u + 3 * (base + off[a]) + r);
+    double b[27];
+    double sigma = 0., phi = 0., big = 0.;
+    bool finite = true;
+    for (int p = 0; p < 27; p++) {
+        double F[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                double acc = 0., mag = 0.;
+#pragma unroll
+                for (int a = 0; a < 8; a++) {
+                    double term = rmul(uv[a][r], k.D[(j * 27 + p) * 8 + a]);
+                    acc = radd(acc, term);
+                    mag = radd(mag, fabs(term));
+                }
+                F[r][j] = acc;
+                if (mag > sigma) sigma = mag;
+            }
+            F[r][r] = radd(F[r][r], 1.);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if (fabs(F[r][j]) > phi) phi = fabs(F[r][j]);
+        double t0 = rmul(F[0][0], rsub(rmul(F[1][1], F[2][2]), rmul(F[1][2], F[2][1])));
+        double t1 = rmul(F[0][1], rsub(rmul(F[1][2], F[2][0]), rmul(F[1][0], F[2][2])));
+        double t2 = rmul(F[0][2], rsub(rmul(F[1][0], F[2][1]), rmul(F[1][1], F[2][0])));
+        double v = radd(radd(t0, t1), t2);
+        b[p] = v;
+        if (fabs(v) > big) big = fabs(v);
+    }
+    // separable T along x, y, z: middle entry of each line -> 2 b_m - (b_l + b_r) / 2
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        int stride = s == 0 ? 1 : (s == 1 ? 3 : 9);
+#pragma unroll
+        for (int p = 0; p < 27; p++)
+            if ((p / stride) % 3 == 1) b[p] = rsub(rmul(2., b[p]), rmul(.5, radd(b[p - stride], b[p + stride])));
+    }
+    double e = radd(rmul(k.g12, radd(sigma, phi)), k.eta);
+    double P = radd(phi, e);
+    double inner = radd(radd(rmul(rmul(3., P), P), rmul(rmul(3., P), e)), rmul(e, e));
+    double ej = radd(rmul(rmul(k.sq27, e), inner), rmul(rmul(rmul(rmul(6., k.g6), P), P), P));
+    double bound = radd(rmul(1.01, radd(rmul(27., ej), rmul(rmul(135., k.g3), big))), k.eta);
+    double low = __longlong_as_double(0x7FF0000000000000LL);
+    for (int p = 0; p < 27; p++) {
+        double w = b[p];
+        if (!(w == w) || !finite64(w)) finite = false;
+        else if (w < low) low = w;
+    }
+    if (!(bound == bound) || !finite64(bound) || !(sigma == sigma) || !finite64(sigma)) finite = false;
+    return finite ? rsub(low, bound) : __longlong_as_double(0x7FF8000000000000LL);
+}
+
+__global__ void __launch_bounds__(128) prescreen_kernel(const double *__restrict__ u, CellGrid g,
+                                                        const long long *__restrict__ cells, long long n,
+                                                        const PrescreenConst k, double *__restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        out[i] = k.usable ? prescreen_cell(u, cell_base(cells[i], g), g.ny, g.nx, k)
+                          : __longlong_as_double(0x7FF8000000000000LL);
+    }
+}
+
+// ============================================================================================== 3a. fallback arrays
+__device__ __forceinline__ double edge_weight(int j, int e, int p) {
+    int a = edge_start(j, e);
+    double coord[3] = {(p % 3) * .5, ((p / 3) % 3) * .5, (p / 9) * .5};
+    double w = 1.;
+    for (int kk = 0; kk < 3; kk++) {
+        if (kk == j) continue;
+        w = rmul(w, ((a >> kk) & 1) ? coord[kk] : rsub(1., coord[kk]));
+    }
+    return w;
+}
+
+// v: 24 vertex displacements (vertex-major); outputs with stride 1 (27 entries each); returns ok
+__device__ bool fallback_cell(const double v[24], const double h[3], double delta, double *plo, double *phi,
+                              double *clo, double *chi, double *smp) {
+    bool ok = true;
+    double elo[3][4][3], ehi[3][4][3];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            int a = edge_start(j, e), b = a | (1 << j);
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                double d = rsub(v[3 * b + r], v[3 * a + r]);
+                double sl, sh;
+                ok &= iout(d, d, sl, sh);
+                double x1 = rdiv(sl, h[j]), x2 = rdiv(sh, h[j]);
+                ok &= iout(nmin(nmin(nmin(x1, x1), x2), x2), nmax(nmax(nmax(x1, x1), x2), x2), elo[j][e][r],
+                           ehi[j][e][r]);
+            }
+        }
+    double blo[27], bhi[27];
+    for (int p = 0; p < 27; p++) {
+        double fl[3][3], fh[3][3];
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                double dl = 0., dh = 0.;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    double w = edge_weight(j, e, p), wl, wh;
+                    ok &= iout(rmul(elo[j][e][r], w), rmul(ehi[j][e][r], w), wl, wh);
+                    ok &= iadd(dl, dh, wl, wh, dl, dh);
+                }
+                double c = (r == j) ? 1. : 0.;
+                ok &= iadd(dl, dh, c, c, fl[r][j], fh[r][j]);
+            }
+        double jl, jh, ml, mh;
+        ok &= idet(fl, fh, jl, jh);
+        ok &= isub(jl, jh, delta, delta, ml, mh);
+        plo[p] = ml; phi[p] = mh;
+        blo[p] = ml; bhi[p] = mh;
+    }
+    // lagrange_to_bernstein: axes x, y, z; middle <- 2 b - (a + c) * .5, all outward
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        int stride = s == 0 ? 1 : (s == 1 ? 3 : 9);
+        for (int q = 0; q < 27; q++) {
+            if ((q / stride) % 3 != 1) continue;
+            int a0 = q - stride, a2 = q + stride;
+            double ml1, mh1, sl1, sh1, hl1, hh1, nl, nh;
+            ok &= imul(blo[q], bhi[q], 2., 2., ml1, mh1);
+            ok &= iadd(blo[a0], bhi[a0], blo[a2], bhi[a2], sl1, sh1);
+            ok &= imul(sl1, sh1, .5, .5, hl1, hh1);
+            ok &= isub(ml1, mh1, hl1, hh1, nl, nh);
+            blo[q] = nl; bhi[q] = nh;
+        }
+    }
+    for (int p = 0; p < 27; p++) { clo[p] = blo[p]; chi[p] = bhi[p]; }
+    // float64 samples: F = I + sum_(j,e) ((v_b - v_a) / h) w, cofactors, ((0 + t0) + t1) + t2
+    for (int p = 0; p < 27; p++) {
+        double fs[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) fs[r][j] = (r == j) ? 1. : 0.;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                int a = edge_start(j, e), b = a | (1 << j);
+                double w = edge_weight(j, e, p);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    fs[r][j] = radd(fs[r][j], rmul(rdiv(rsub(v[3 * b + r], v[3 * a + r]), h[j]), w));
+            }
+        bool finite = true;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) finite = finite && finite64(fs[r][j]);
+        double a00 = rsub(rmul(fs[1][1], fs[2][2]), rmul(fs[1][2], fs[2][1]));
+        double a01 = rsub(rmul(fs[1][2], fs[2][0]), rmul(fs[1][0], fs[2][2]));
+        double a02 = rsub(rmul(fs[1][0], fs[2][1]), rmul(fs[1][1], fs[2][0]));
+        double a10 = rsub(rmul(fs[2][1], fs[0][2]), rmul(fs[2][2], fs[0][1]));
+        double a11 = rsub(rmul(fs[2][2], fs[0][0]), rmul(fs[2][0], fs[0][2]));
+        double a12 = rsub(rmul(fs[2][0], fs[0][1]), rmul(fs[2][1], fs[0][0]));
+        double a20 = rsub(rmul(fs[0][1], fs[1][2]), rmul(fs[0][2], fs[1][1]));
+        double a21 = rsub(rmul(fs[0][2], fs[1][0]), rmul(fs[0][0], fs[1][2]));
+        double a22 = rsub(rmul(fs[0][0], fs[1][1]), rmul(fs[0][1], fs[1][0]));
+        finite = finite && finite64(a00) && finite64(a01) && finite64(a02) && finite64(a10) && finite64(a11) &&
+                 finite64(a12) && finite64(a20) && finite64(a21) && finite64(a22);
+        double t0 = rmul(fs[0][0], a00), t1 = rmul(fs[0][1], a01), t2 = rmul(fs[0][2], a02);
+        double s = radd(radd(radd(0., t0), t1), t2);
+        finite = finite && finite64(t0) && finite64(t1) && finite64(t2) && finite64(s);
+        smp[p] = s;
+        ok = ok && finite;
+    }
+    return ok;
+}
+
+// Standalone cells: vertices (n, 8, 3)
+__global__ void __launch_bounds__(64) fallback_vertices_kernel(const double *__restrict__ vertices, long long n,
+                                                               double hx, double hy, double hz, double delta,
+                                                               double *plo, double *phi, double *clo, double *chi,
+                                                               double *smp, uint8_t *ok) {
+    const double h[3] = {hx, hy, hz};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double v[24];
+        for (int k = 0; k < 24; k++) v[k] = vertices[24 * i + k];
+        ok[i] = fallback_cell(v, h, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+    }
+}
+
+// Grid cells from a list: vertices gathered from u
+__global__ void __launch_bounds__(64) fallback_grid_kernel(const double *__restrict__ u, CellGrid g,
+                                                           const long long *__restrict__ cells, long long n,
+                                                           double delta, double *plo, double *phi, double *clo,
+                                                           double *chi, double *smp, uint8_t *ok) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long base = cell_base(cells[i], g);
+        double v[24];
+        for (int a = 0; a < 8; a++)
+            for (int r = 0; r < 3; r++) v[3 * a + r] = __ldg(u + 3 * vnode(base, a, g.ny, g.nx) + r);
+        ok[i] = fallback_cell(v, g.h, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+    }
+}
+
+// ============================================================================================== 3b. subdivision
+// Status / reason codes: see svp3d.h.
+enum { ST_FEASIBLE = 0, ST_INFEASIBLE = 1, ST_UNCERTAIN = 2 };
+enum { R_ENCLOSURE = 0, R_BERNSTEIN = 1, R_VIOLATION = 2, R_ARITH = 3, R_SUBDIV_BUDGET = 4, R_NONFINITE = 5,
+       R_BOUNDARY = 6, R_DOMAIN = 7, R_SAMPLE_WITNESS = 9, R_SUBDIV_WITNESS = 10, R_BOX_BUDGET = 11,
+       R_DEPTH_BUDGET = 12 };
+
+// Per-warp scratch layout for S slots: coefficients (S, 54) doubles, meta (S, 8) doubles (low xyz, high xyz, key),
+// serial (S) int64, depth (S) int32, heap (S) int32, free stack (S) int32.
+__host__ __device__ inline size_t warp_scratch_bytes(long long slots) {
+    return (size_t)slots * (54 * 8 + 8 * 8 + 8 + 4 + 4 + 4);
+}
+
+__device__ __forceinline__ double warp_min27(double x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        double y = __shfl_xor_sync(0xFFFFFFFFu, x, o);
+        x = y < x ? y : x;
+    }
+    return x;
+}
+
+struct WarpHeap {
+    double *coef, *meta;
+    long long *serial;
+    int *depth, *heap, *freel;
+    int size, nfree;
+    __device__ bool less(int a, int b) const {
+        double ka = meta[8 * a + 6], kb = meta[8 * b + 6];
+        return ka < kb || (ka == kb && serial[a] < serial[b]);
+    }
+    __device__ void push(int slot) {  // lane 0 only
+        int i = size++;
+        heap[i] = slot;
+        while (i > 0) {
+            int p = (i - 1) / 2;
+            if (!less(heap[i], heap[p])) break;
+            int t = heap[i]; heap[i] = heap[p]; heap[p] = t;
+            i = p;
+        }
+    }
+    __device__ int pop() {  // lane 0 only
+        int top = heap[0];
+        heap[0] = heap[--size];
+        int i = 0;
+        for (;;) {
+            int l = 2 * i + 1, r = l + 1, m = i;
+            if (l < size && less(heap[l], heap[m])) m = l;
+            if (r < size && less(heap[r], heap[m])) m = r;
+            if (m == i) break;
+            int t = heap[i]; heap[i] = heap[m]; heap[m] = t;
+            i = m;
+        }
+        return top;
+    }
+};
+
+__device__ void verdict_result(svp_cell_verdict &v, int status, double margin, long long boxes, long long depth,
+                               const double *w, int reason, double delta) {
+    v.boxes = boxes; v.depth = depth;
+    v.witness[0] = v.witness[1] = v.witness[2] = __longlong_as_double(0x7FF8000000000000LL);
+    if (delta != 0.) {
+        double l, h;
+        if (!iout(radd(margin, delta), radd(margin, delta), l, h)) {
+            v.status = ST_UNCERTAIN; v.reason = R_ARITH; v.has_margin = 0; v.has_witness = 0;
+            v.margin = __longlong_as_double(0x7FF8000000000000LL);
+            return;
+        }
+    }
+    v.status = status; v.reason = reason; v.margin = margin; v.has_margin = 1;
+    v.has_witness = w != nullptr;
+    if (w) { v.witness[0] = w[0]; v.witness[1] = w[1]; v.witness[2] = w[2]; }
+}
+
+// One warp per cell; rows[i] selects the input row (nullptr: row i).  Lanes 0..26 hold one coefficient each.
+__global__ void __launch_bounds__(128) classify_kernel(const double *__restrict__ clo, const double *__restrict__ chi,
+                                                       const double *__restrict__ phi, const long long *rows,
+                                                       long long n, double delta, long long max_depth,
+                                                       long long max_boxes, svp_cell_verdict *out, char *scratch,
+                                                       long long slots) {
+    const int lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const bool act = lane < 27;
+    const double INF = __longlong_as_double(0x7FF0000000000000LL);
+    char *base = scratch + warp_scratch_bytes(slots) * gw;
+    WarpHeap H;
+    H.coef = (double *)base;
+    H.meta = H.coef + 54 * slots;
+    H.serial = (long long *)(H.meta + 8 * slots);
+    H.depth = (int *)(H.serial + slots);
+    H.heap = H.depth + slots;
+    H.freel = H.heap + slots;
+    for (long long i = gw; i < n; i += nw) {
+        long long row = rows ? rows[i] : i;
+        double lo = act ? clo[27 * row + lane] : INF;
+        double hi = act ? chi[27 * row + lane] : INF;
+        double ph = act ? phi[27 * row + lane] : INF;
+        double root_lower = warp_min27(lo);
+        svp_cell_verdict v;
+        unsigned sw = __ballot_sync(0xFFFFFFFFu, act && ph <= 0);
+        if (sw) {
+            int q = __ffs(sw) - 1;
+            double w[3] = {(q % 3) / 2., ((q / 3) % 3) / 2., (q / 9) / 2.};
+            verdict_result(v, ST_INFEASIBLE, root_lower, 1, 0, w, R_SAMPLE_WITNESS, delta);
+            if (lane == 0) out[i] = v;
+            continue;
+        }
+        // root box in slot 0; slots 1.. free
+        if (act) { H.coef[lane] = lo; H.coef[27 + lane] = hi; }
+        if (lane == 0) {
+            for (int k = 0; k < 3; k++) { H.meta[k] = 0.; H.meta[3 + k] = 1.; }
+            H.meta[6] = root_lower;
+            H.serial[0] = 0; H.depth[0] = 0;
+            H.size = 0; H.nfree = 0;
+            for (long long s = slots - 1; s >= 1; s--) H.freel[H.nfree++] = (int)s;
+            H.push(0);
+        }
+        __syncwarp();
+        long long serial = 0, boxes = 0, depth_used = 0;
+        bool uncertain = false, done = false;
+        double cert_min = INF;
+        int size = 1;
+        while (size > 0) {
+            if (boxes >= max_boxes) {
+                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_BOX_BUDGET, delta);
+                done = true;
+                break;
+            }
+            int slot = 0;
+            if (lane == 0) slot = H.pop();
+            slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+            __syncwarp();
+            double clo_ = act ? H.coef[54 * slot + lane] : INF;
+            double chi_ = act ? H.coef[54 * slot + 27 + lane] : INF;
+            double low[3], high[3];
+            for (int k = 0; k < 3; k++) { low[k] = H.meta[8 * slot + k]; high[k] = H.meta[8 * slot + 3 + k]; }
+            int depth = H.depth[slot];
+            boxes += 1;
+            if (depth > depth_used) depth_used = depth;
+            double minimum = warp_min27(clo_);
+            __syncwarp();
+            if (minimum > 0) {
+                if (minimum < cert_min) cert_min = minimum;
+                if (lane == 0) { H.freel[H.nfree++] = slot; size = H.size; }
+                size = __shfl_sync(0xFFFFFFFFu, size, 0);
+                continue;
+            }
+            bool corner = act && ((lane % 3) % 2 == 0) && (((lane / 3) % 3) % 2 == 0) && ((lane / 9) % 2 == 0);
+            unsigned cw = __ballot_sync(0xFFFFFFFFu, corner && chi_ <= 0);
+            if (cw) {
+                int q = __ffs(cw) - 1;
+                int bits[3] = {(q % 3) / 2, ((q / 3) % 3) / 2, (q / 9) / 2};
+                double w[3];
+                for (int k = 0; k < 3; k++) w[k] = bits[k] ? high[k] : low[k];
+                verdict_result(v, ST_INFEASIBLE, root_lower, boxes, depth_used, w, R_SUBDIV_WITNESS, delta);
+                done = true;
+                break;
+            }
+            if (depth >= max_depth) {
+                uncertain = true;
+                if (lane == 0) { H.freel[H.nfree++] = slot; size = H.size; }
+                size = __shfl_sync(0xFFFFFFFFu, size, 0);
+                continue;
+            }
+            int axis = 0;
+            double best = rsub(high[0], low[0]);
+            for (int k = 1; k < 3; k++) {
+                double ext = rsub(high[k], low[k]);
+                if (ext > best) { best = ext; axis = k; }
+            }
+            int stride = axis == 0 ? 1 : (axis == 1 ? 3 : 9);
+            int t = act ? (lane / stride) % 3 : 0;
+            int la = act ? lane - t * stride : lane;
+            int lb = act ? la + stride : lane, lc = act ? la + 2 * stride : lane;
+            double al = __shfl_sync(0xFFFFFFFFu, clo_, la), ah = __shfl_sync(0xFFFFFFFFu, chi_, la);
+            double bl = __shfl_sync(0xFFFFFFFFu, clo_, lb), bh = __shfl_sync(0xFFFFFFFFu, chi_, lb);
+            double cl = __shfl_sync(0xFFFFFFFFu, clo_, lc), ch = __shfl_sync(0xFFFFFFFFu, chi_, lc);
+            double sl, sh, abl, abh, bcl, bch, ml, mh;
+            bool ok = true;
+            ok &= iadd(al, ah, bl, bh, sl, sh);
+            ok &= imul(sl, sh, .5, .5, abl, abh);
+            ok &= iadd(bl, bh, cl, ch, sl, sh);
+            ok &= imul(sl, sh, .5, .5, bcl, bch);
+            ok &= iadd(abl, abh, bcl, bch, sl, sh);
+            ok &= imul(sl, sh, .5, .5, ml, mh);
+            if (__ballot_sync(0xFFFFFFFFu, act && !ok)) {
+                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_ARITH, delta);
+                done = true;
+                break;
+            }
+            double Ll = t == 0 ? al : (t == 1 ? abl : ml), Lh = t == 0 ? ah : (t == 1 ? abh : mh);
+            double Rl = t == 0 ? ml : (t == 1 ? bcl : cl), Rh = t == 0 ? mh : (t == 1 ? bch : ch);
+            if (!act) { Ll = INF; Rl = INF; }
+            double kl = warp_min27(Ll), kr = warp_min27(Rl);
+            double mid = rmul(radd(low[axis], high[axis]), .5);
+            int rslot = 0;
+            if (lane == 0) rslot = H.freel[--H.nfree];
+            rslot = __shfl_sync(0xFFFFFFFFu, rslot, 0);
+            if (act) {
+                H.coef[54 * slot + lane] = Ll; H.coef[54 * slot + 27 + lane] = Lh;
+                H.coef[54 * rslot + lane] = Rl; H.coef[54 * rslot + 27 + lane] = Rh;
+            }
+            if (lane == 0) {
+                for (int k = 0; k < 3; k++) {
+                    H.meta[8 * slot + k] = low[k];
+                    H.meta[8 * slot + 3 + k] = k == axis ? mid : high[k];
+                    H.meta[8 * rslot + k] = k == axis ? mid : low[k];
+                    H.meta[8 * rslot + 3 + k] = high[k];
+                }
+                H.meta[8 * slot + 6] = kl; H.meta[8 * rslot + 6] = kr;
+                H.depth[slot] = depth + 1; H.depth[rslot] = depth + 1;
+                H.serial[slot] = serial + 1; H.serial[rslot] = serial + 2;
+            }
+            serial += 2;
+            __syncwarp();
+            if (lane == 0) { H.push(slot); H.push(rslot); size = H.size; }
+            size = __shfl_sync(0xFFFFFFFFu, size, 0);
+            __syncwarp();
+        }
+        if (!done) {
+            if (uncertain)
+                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_DEPTH_BUDGET, delta);
+            else
+                verdict_result(v, ST_FEASIBLE, cert_min, boxes, depth_used, nullptr, R_BERNSTEIN, delta);
+        }
+        if (lane == 0) out[i] = v;
+        __syncwarp();
+    }
+}
+
+// ============================================================================================== 4. whole map
+struct Accum {
+    unsigned long long nonfinite, boundary, invalid;   // pre-checks (nodes)
+    unsigned long long fast, prescreened, unknown, bad, boxes_extra, fallback_ok_cells;
+    long long lowest_key, sampled_key, max_depth, witness_cell;
+    int any_margin, arith, has_witness, pad;
+    double witness[3];
+};
+
+// Sampling-domain and boundary checks per node (interpolation.py:43 check_map_domain, validation zero_boundary).
+__global__ void precheck_kernel(const double *__restrict__ u, CellGrid g, double x0, double y0, double z0,
+                                Accum *acc) {
+    unsigned long long nf = 0, nb = 0, ni = 0;
+    long long nn = g.nx * g.ny * g.nz;
+    const double org[3] = {x0, y0, z0};
+    const long long len[3] = {g.nx, g.ny, g.nz};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % g.nx, y = (i / g.nx) % g.ny, z = i / (g.nx * g.ny);
+        long long idx[3] = {x, y, z};
+        double q[3] = {u[3 * i], u[3 * i + 1], u[3 * i + 2]};
+        bool nonfin = !(finite64(q[0]) && finite64(q[1]) && finite64(q[2]));
+        bool face = z == 0 || z == g.nz - 1 || y == 0 || y == g.ny - 1 || x == 0 || x == g.nx - 1;
+        bool interior = !face;
+        bool bad = false;
+        for (int j = 0; j < 3; j++) {
+            double lo = org[j], hi = radd(org[j], rmul(g.h[j], (double)(len[j] - 1)));
+            double value = radd(q[j], radd(org[j], rmul(g.h[j], (double)idx[j])));
+            if (!finite64(value) || value < lo || value > hi) bad = true;
+            if (interior && (value <= lo || value >= hi)) bad = true;
+        }
+        nf += nonfin;
+        nb += face && (q[0] != 0 || q[1] != 0 || q[2] != 0);
+        ni += bad;
+    }
+    for (int o = 16; o; o >>= 1) {
+        nf += __shfl_xor_sync(0xFFFFFFFFu, nf, o);
+        nb += __shfl_xor_sync(0xFFFFFFFFu, nb, o);
+        ni += __shfl_xor_sync(0xFFFFFFFFu, ni, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nf) atomicAdd(&acc->nonfinite, nf);
+        if (nb) atomicAdd(&acc->boundary, nb);
+        if (ni) atomicAdd(&acc->invalid, ni);
+    }
+}
+
+__global__ void tile_flag_kernel(const uint8_t *__restrict__ flag, long long ncell, long long tile,
+                                 int *__restrict__ tile_bad) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x)
+        if (flag[c]) tile_bad[c / tile] = 1;
+}
+
+__device__ __forceinline__ void warp_min_key(long long &k) {
+    for (int o = 16; o; o >>= 1) {
+        long long y = __shfl_xor_sync(0xFFFFFFFFu, k, o);
+        k = y < k ? y : k;
+    }
+}
+
+// hull-proven cells: margin > 0 in an unflagged tile; sel[c] = 1 marks the rest (prescreen/fallback candidates)
+__global__ void hull_stage_kernel(const double *__restrict__ margin, const int *__restrict__ tile_bad,
+                                  long long ncell, long long tile, uint8_t *__restrict__ sel, Accum *acc) {
+    unsigned long long nfast = 0;
+    long long key = kKeyPosInf;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        bool proven = !tile_bad[c / tile] && margin[c] > 0;
+        sel[c] = proven ? 0 : 1;
+        if (proven) {
+            nfast++;
+            long long k = order_key(margin[c]);
+            key = k < key ? k : key;
+        }
+    }
+    for (int o = 16; o; o >>= 1) nfast += __shfl_xor_sync(0xFFFFFFFFu, nfast, o);
+    warp_min_key(key);
+    if ((threadIdx.x & 31) == 0) {
+        if (nfast) {
+            atomicAdd(&acc->fast, nfast);
+            atomicMin(&acc->lowest_key, key);
+            acc->any_margin = 1;
+        }
+    }
+}
+
+// prescreen decision: margin_pre = lower (delta == 0) or nextafter(lower - delta, -inf); proven iff margin_pre > 0
+__global__ void prescreen_stage_kernel(const double *__restrict__ lower, long long n, double delta,
+                                       uint8_t *__restrict__ sel, Accum *acc) {
+    unsigned long long np = 0;
+    long long key = kKeyPosInf;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double m = delta == 0. ? lower[i] : step_down(rsub(lower[i], delta));
+        bool ok = m > 0;
+        sel[i] = ok ? 0 : 1;
+        if (ok) {
+            np++;
+            long long k = order_key(m);
+            key = k < key ? k : key;
+        }
+    }
+    for (int o = 16; o; o >>= 1) np += __shfl_xor_sync(0xFFFFFFFFu, np, o);
+    warp_min_key(key);
+    if ((threadIdx.x & 31) == 0 && np) {
+        atomicAdd(&acc->prescreened, np);
+        atomicMin(&acc->lowest_key, key);
+        acc->any_margin = 1;
+    }
+}
+
+__global__ void job_fail_kernel(const long long *__restrict__ cells, const uint8_t *__restrict__ ok, long long n,
+                                long long tile, int *__restrict__ tile_fail) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        if (!ok[i]) tile_fail[cells[i] / tile] = 1;
+}
+
+// fallback cells in successful jobs: count, sampled min, safe cells' min coefficient; sel marks cells to classify
+__global__ void fallback_stage_kernel(const long long *__restrict__ cells, const double *__restrict__ clo,
+                                      const double *__restrict__ smp, long long n, long long tile,
+                                      const int *__restrict__ tile_fail, uint8_t *__restrict__ sel, Accum *acc) {
+    unsigned long long nok = 0, nunk = 0;
+    long long key = kKeyPosInf, skey = kKeyPosInf;
+    int any_safe = 0, any_fail = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        sel[i] = 0;
+        if (tile_fail[cells[i] / tile]) { nunk++; any_fail = 1; continue; }
+        nok++;
+        double mn = clo[27 * i];
+        for (int q = 1; q < 27; q++) { double x = clo[27 * i + q]; if (x < mn) mn = x; }
+        for (int q = 0; q < 27; q++) { long long k = order_key(smp[27 * i + q]); skey = k < skey ? k : skey; }
+        if (mn > 0) {
+            any_safe = 1;
+            long long k = order_key(mn);
+            key = k < key ? k : key;
+        } else {
+            sel[i] = 1;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        nok += __shfl_xor_sync(0xFFFFFFFFu, nok, o);
+        nunk += __shfl_xor_sync(0xFFFFFFFFu, nunk, o);
+        any_safe |= __shfl_xor_sync(0xFFFFFFFFu, any_safe, o);
+        any_fail |= __shfl_xor_sync(0xFFFFFFFFu, any_fail, o);
+    }
+    warp_min_key(key);
+    warp_min_key(skey);
+    if ((threadIdx.x & 31) == 0) {
+        if (nok) atomicAdd(&acc->fallback_ok_cells, nok);
+        if (nunk) atomicAdd(&acc->unknown, nunk);
+        if (any_fail) acc->arith = 1;
+        if (skey != kKeyPosInf) atomicMin(&acc->sampled_key, skey);
+        if (any_safe) { atomicMin(&acc->lowest_key, key); acc->any_margin = 1; }
+    }
+}
+
+__global__ void verdict_stage_kernel(const svp_cell_verdict *__restrict__ v, const long long *__restrict__ rows,
+                                     const long long *__restrict__ cells, long long n, Accum *acc) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const svp_cell_verdict &r = v[i];
+        if (r.has_margin) { atomicMin(&acc->lowest_key, order_key(r.margin)); acc->any_margin = 1; }
+        if (r.reason == R_ARITH) acc->arith = 1;
+        atomicAdd(&acc->boxes_extra, (unsigned long long)(r.boxes - 1));
+        atomicMax(&acc->max_depth, r.depth);
+        if (r.status == ST_UNCERTAIN) atomicAdd(&acc->unknown, 1ULL);
+        if (r.status == ST_INFEASIBLE) {
+            atomicAdd(&acc->bad, 1ULL);
+            atomicMin(&acc->witness_cell, cells[rows[i]]);
+        }
+    }
+}
+
+__global__ void witness_kernel(const svp_cell_verdict *__restrict__ v, const long long *__restrict__ rows,
+                               const long long *__restrict__ cells, long long n, Accum *acc) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (v[i].status == ST_INFEASIBLE && cells[rows[i]] == acc->witness_cell) {
+            acc->has_witness = v[i].has_witness;
+            for (int k = 0; k < 3; k++) acc->witness[k] = v[i].witness[k];
+        }
+    }
+}
+
+__global__ void accum_init_kernel(Accum *acc) {
+    memset(acc, 0, sizeof(Accum));
+    acc->lowest_key = kKeyPosInf;
+    acc->sampled_key = kKeyPosInf;
+    acc->max_depth = 0;
+    acc->witness_cell = 0x7FFFFFFFFFFFFFFFLL;
+}
+
+// Host-side table and constants, computed with the reference's expressions (cell_q1.py:101-129,
+// certificate_prescreen.py:46-55).
+void closed27_table(const double h[3], double *D) {
+    const double nodes[3] = {0., .5, 1.};
+    for (int a = 0; a < 8; a++) {
+        int vertex[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
+        for (int p = 0; p < 27; p++) {
+            double pt[3] = {nodes[p % 3], nodes[(p / 3) % 3], nodes[p / 9]};
+            double f[3];
+            for (int j = 0; j < 3; j++) f[j] = vertex[j] ? pt[j] : 1 - pt[j];
+            for (int j = 0; j < 3; j++) {
+                int o0 = j == 0 ? 1 : 0, o1 = j == 2 ? 1 : 2;
+                D[(j * 27 + p) * 8 + a] = (vertex[j] ? 1. : -1.) / h[j] * f[o0] * f[o1];
+            }
+        }
+    }
+}
+
+PrescreenConst prescreen_const(const double h[3]) {
+    PrescreenConst k;
+    closed27_table(h, k.D);
+    const double unit = 0x1p-53;
+    auto gamma = [&](double n) { return n * unit / (1 - n * unit); };
+    k.g12 = gamma(12); k.g6 = gamma(6); k.g3 = gamma(3);
+    k.sq27 = 5.196152422706633;
+    k.eta = 1e-290;
+    k.usable = 1;
+    for (int i = 0; i < 3 * 27 * 8; i++) {
+        double x = k.D[i];
+        if (!std::isfinite(x)) k.usable = 0;
+        if (x != 0 && std::fabs(x) < 2.2250738585072014e-308) k.usable = 0;
+    }
+    return k;
+}
+
+}  // namespace
+
+// ============================================================================================== C ABI
+extern "C" int svp_edge_hull_margins(const svp_grid *g, const double *u, double delta, double *margin,
+                                     uint8_t *flag, void *stream) {
+    SVP_REQUIRE(grid_ok(g), "svp_edge_hull_margins: invalid grid");
+    SVP_REQUIRE(u && margin && flag, "svp_edge_hull_margins: null pointer");
+    CellGrid cg = cell_grid(g);
+    edge_hull_kernel<<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag);
+    SVP_LAUNCH_CHECK("edge_hull_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, const int64_t *cells, int64_t n,
+                                          double *out, void *stream) {
+    SVP_REQUIRE(grid_ok(g), "svp_prescreen_lower_bounds: invalid grid");
+    SVP_REQUIRE(n >= 0, "svp_prescreen_lower_bounds: negative count");
+    if (n == 0) return SVP_OK;
+    SVP_REQUIRE(u && cells && out, "svp_prescreen_lower_bounds: null pointer");
+    CellGrid cg = cell_grid(g);
+    PrescreenConst k = prescreen_const(cg.h);
+    prescreen_kernel<<<blocks_for(n, 128, 8), 128, 0, (cudaStream_t)stream>>>(u, cg, (const long long *)cells, n, k,
+                                                                               out);
+    SVP_LAUNCH_CHECK("prescreen_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta,
+                                   double *p_lo, double *p_hi, double *c_lo, double *c_hi, double *samples,
+                                   uint8_t *ok, void *stream) {
+    SVP_REQUIRE(n >= 0 && spacing3, "svp_fallback_arrays: invalid arguments");
+    if (n == 0) return SVP_OK;
+    SVP_REQUIRE(vertices && p_lo && p_hi && c_lo && c_hi && samples && ok, "svp_fallback_arrays: null pointer");
+    fallback_vertices_kernel<<<blocks_for(n, 64, 16), 64, 0, (cudaStream_t)stream>>>(
+        vertices, n, spacing3[0], spacing3[1], spacing3[2], delta, p_lo, p_hi, c_lo, c_hi, samples, ok);
+    SVP_LAUNCH_CHECK("fallback_vertices_kernel");
+    return SVP_OK;
+}
+
+static int classify_launch(const double *c_lo, const double *c_hi, const double *p_hi, const long long *rows,
+                           long long n, double delta, long long max_depth, long long max_boxes,
+                           svp_cell_verdict *out, char *scratch, long long warps, long long slots,
+                           cudaStream_t stream) {
+    long long threads = 128, blocks = div_up(warps * 32, threads);
+    classify_kernel<<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(c_lo, c_hi, p_hi, rows, n, delta, max_depth,
+                                                                        max_boxes, out, scratch, slots);
+    SVP_LAUNCH_CHECK("classify_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
+                                  int64_t n, double delta, int64_t max_depth, int64_t max_boxes,
+                                  svp_cell_verdict *out, void *stream) {
+    SVP_REQUIRE(n >= 0 && max_depth >= 0 && max_boxes >= 1, "svp_classify_cells: invalid arguments");
+    if (n == 0) return SVP_OK;
+    SVP_REQUIRE(c_lo && c_hi && p_lo && p_hi && out, "svp_classify_cells: null pointer");
+    SVP_REQUIRE(max_boxes <= (1LL << 24), "svp_classify_cells: max_boxes above 2^24");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long slots = max_boxes + 2;
+    long long warps = n < (long long)kSMs * 8 ? n : (long long)kSMs * 8;
+    warps = (warps + 3) / 4 * 4;  // whole blocks of 4 warps
+    char *scratch = nullptr;
+    SVP_CUDA(cudaMallocAsync((void **)&scratch, warp_scratch_bytes(slots) * warps, s));
+    int rc = classify_launch(c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, warps, slots, s);
+    cudaError_t e = cudaFreeAsync(scratch, s);
+    if (rc != SVP_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
+    return SVP_OK;
+}
+
+}  // namespace svp
+
+// ---------------------------------------------------------------------------------------------- certifier handle
+struct svp_certifier {
+    svp_grid grid;
+    svp_cert_config cfg;
+    svp::CellGrid cg;
+    long long ncell, ntiles;
+    double *margin = nullptr, *lower = nullptr;
+    uint8_t *flag = nullptr, *sel = nullptr;
+    int *tile_bad = nullptr, *tile_fail = nullptr;
+    long long *list1 = nullptr, *list2 = nullptr, *list3 = nullptr, *counts = nullptr;
+    svp::Accum *acc = nullptr;
+    void *cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    // fallback workspace (grows on demand)
+    long long fb_cap = 0;
+    double *fb = nullptr;  // 5 * 27 * cap
+    uint8_t *fb_ok = nullptr;
+    svp_cell_verdict *verdicts = nullptr;
+    char *heap = nullptr;
+    long long heap_warps = 0, heap_slots = 0;
+    svp::PrescreenConst pk;
+};
+
+namespace svp {
+namespace {
+
+int ensure_fallback(svp_certifier *c, long long n) {
+    if (n <= c->fb_cap) return SVP_OK;
+    long long cap = n < 1024 ? 1024 : n;
+    if (c->fb_cap) cap = cap < 2 * c->fb_cap ? 2 * c->fb_cap : cap;
+    cudaFree(c->fb); cudaFree(c->fb_ok); cudaFree(c->verdicts);
+    c->fb = nullptr; c->fb_ok = nullptr; c->verdicts = nullptr; c->fb_cap = 0;
+    SVP_CUDA(cudaMalloc((void **)&c->fb, sizeof(double) * 5 * 27 * cap));
+    SVP_CUDA(cudaMalloc((void **)&c->fb_ok, cap));
+    SVP_CUDA(cudaMalloc((void **)&c->verdicts, sizeof(svp_cell_verdict) * cap));
+    c->fb_cap = cap;
+    return SVP_OK;
+}
+
+template <class InIt>
+int select_flagged(svp_certifier *c, InIt in, const uint8_t *flags, long long *out, long long *count, long long n,
+                   cudaStream_t s) {
+    size_t need = 0;
+    SVP_CUDA(cub::DeviceSelect::Flagged(nullptr, need, in, flags, out, count, n, s));
+    if (need > c->cub_bytes) {
+        cudaFree(c->cub_tmp);
+        c->cub_tmp = nullptr;
+        SVP_CUDA(cudaMalloc(&c->cub_tmp, need));
+        c->cub_bytes = need;
+    }
+    SVP_CUDA(cub::DeviceSelect::Flagged(c->cub_tmp, c->cub_bytes, in, flags, out, count, n, s));
+    return SVP_OK;
+}
+
+}  // namespace
+}  // namespace svp
+
+extern "C" int svp_certifier_create(const svp_grid *g, const svp_cert_config *cfg, svp_certifier **out) {
+    using namespace svp;
+    SVP_REQUIRE(out, "svp_certifier_create: null output");
+    *out = nullptr;
+    SVP_REQUIRE(grid_ok(g) && cfg, "svp_certifier_create: invalid grid/config");
+    SVP_REQUIRE(cfg->delta >= 0 && cfg->delta < 1, "svp_certifier_create: require 0 <= delta < 1");
+    SVP_REQUIRE(cfg->max_depth >= 0 && cfg->max_boxes >= 1 && cfg->tile_size >= 1,
+                "svp_certifier_create: invalid budgets/tile size");
+    SVP_REQUIRE(cfg->max_boxes <= (1LL << 24), "svp_certifier_create: max_boxes above 2^24");
+    svp_certifier *c = new svp_certifier();
+    c->grid = *g;
+    c->cfg = *cfg;
+    if (c->cfg.delta == 0) c->cfg.delta = 0.0;  // canonical +0
+    c->cg = cell_grid(g);
+    c->ncell = c->cg.ncell;
+    c->ntiles = div_up(c->ncell, cfg->tile_size);
+    c->pk = prescreen_const(c->cg.h);
+    auto bail = [&](cudaError_t e, const char *what) {
+        svp_certifier_destroy(c);
+        return cuda_fail(e, what);
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc((void **)&c->margin, sizeof(double) * c->ncell)) != cudaSuccess) return bail(e, "margin");
+    if ((e = cudaMalloc((void **)&c->lower, sizeof(double) * c->ncell)) != cudaSuccess) return bail(e, "lower");
+    if ((e = cudaMalloc((void **)&c->flag, c->ncell)) != cudaSuccess) return bail(e, "flag");
+    if ((e = cudaMalloc((void **)&c->sel, c->ncell)) != cudaSuccess) return bail(e, "sel");
+    if ((e = cudaMalloc((void **)&c->tile_bad, sizeof(int) * c->ntiles)) != cudaSuccess) return bail(e, "tiles");
+    if ((e = cudaMalloc((void **)&c->tile_fail, sizeof(int) * c->ntiles)) != cudaSuccess) return bail(e, "tiles");
+    if ((e = cudaMalloc((void **)&c->list1, sizeof(long long) * c->ncell)) != cudaSuccess) return bail(e, "list1");
+    if ((e = cudaMalloc((void **)&c->list2, sizeof(long long) * c->ncell)) != cudaSuccess) return bail(e, "list2");
+    if ((e = cudaMalloc((void **)&c->list3, sizeof(long long) * c->ncell)) != cudaSuccess) return bail(e, "list3");
+    if ((e = cudaMalloc((void **)&c->counts, sizeof(long long) * 4)) != cudaSuccess) return bail(e, "counts");
+    if ((e = cudaMalloc((void **)&c->acc, sizeof(Accum))) != cudaSuccess) return bail(e, "accum");
+    c->heap_slots = cfg->max_boxes + 2;
+    c->heap_warps = (long long)kSMs * 8;
+    if ((e = cudaMalloc((void **)&c->heap, warp_scratch_bytes(c->heap_slots) * c->heap_warps)) != cudaSuccess)
+        return bail(e, "subdivision heap");
+    *out = c;
+    return SVP_OK;
+}
+
+extern "C" int svp_certifier_destroy(svp_certifier *c) {
+    if (!c) return SVP_OK;
+    cudaFree(c->margin); cudaFree(c->lower); cudaFree(c->flag); cudaFree(c->sel);
+    cudaFree(c->tile_bad); cudaFree(c->tile_fail); cudaFree(c->list1); cudaFree(c->list2); cudaFree(c->list3);
+    cudaFree(c->counts); cudaFree(c->acc); cudaFree(c->cub_tmp); cudaFree(c->fb); cudaFree(c->fb_ok);
+    cudaFree(c->verdicts); cudaFree(c->heap);
+    delete c;
+    return SVP_OK;
+}
+
+extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_result *out, void *stream) {
+    using namespace svp;
+    SVP_REQUIRE(c && u && out, "svp_certify_map: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = c->ncell, tile = c->cfg.tile_size;
+    const double delta = c->cfg.delta;
+    const double nan = std::nan("");
+    memset(out, 0, sizeof *out);
+    out->status = ST_UNCERTAIN;
+    out->reason = 14;  // not_checked
+    out->n_uncertain = n;
+    out->witness_cell = -1;
+    out->min_jd_lower_bound = out->min_margin_lower_bound = out->sampled_min_jd = nan;
+    out->witness_point[0] = out->witness_point[1] = out->witness_point[2] = nan;
+
+    accum_init_kernel<<<1, 1, 0, s>>>(c->acc);
+    precheck_kernel<<<blocks_for(n_nodes(&c->grid), 256, 8), 256, 0, s>>>(u, c->cg, c->grid.x0, c->grid.y0,
+                                                                            c->grid.z0, c->acc);
+    SVP_LAUNCH_CHECK("precheck_kernel");
+    edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag);
+    SVP_LAUNCH_CHECK("edge_hull_kernel");
+    SVP_CUDA(cudaMemsetAsync(c->tile_bad, 0, sizeof(int) * c->ntiles, s));
+    SVP_CUDA(cudaMemsetAsync(c->tile_fail, 0, sizeof(int) * c->ntiles, s));
+    tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad);
+    hull_stage_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->margin, c->tile_bad, n, tile, c->sel, c->acc);
+    SVP_LAUNCH_CHECK("hull stage");
+    int rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list1, c->counts, n, s);
+    if (rc) return rc;
+    Accum acc;
+    long long counts[4];
+    SVP_CUDA(cudaMemcpyAsync(&acc, c->acc, sizeof acc, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaMemcpyAsync(counts, c->counts, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    // early returns, in certify_map's order (feasibility.py:412-428)
+    if (acc.nonfinite) { out->reason = R_NONFINITE; return SVP_OK; }
+    if (acc.boundary) { out->status = ST_INFEASIBLE; out->reason = R_BOUNDARY; return SVP_OK; }
+    if (acc.invalid) { out->status = ST_INFEASIBLE; out->reason = R_DOMAIN; return SVP_OK; }
+    long long n1 = counts[0], n2 = n1;
+    const long long *list2 = c->list1;
+    if (c->cfg.prescreen && n1) {
+        prescreen_kernel<<<blocks_for(n1, 128, 8), 128, 0, s>>>(u, c->cg, c->list1, n1, c->pk, c->lower);
+        SVP_LAUNCH_CHECK("prescreen_kernel");
+        prescreen_stage_kernel<<<blocks_for(n1, 256, 8), 256, 0, s>>>(c->lower, n1, delta, c->sel, c->acc);
+        SVP_LAUNCH_CHECK("prescreen stage");
+        rc = select_flagged(c, c->list1, c->sel, c->list2, c->counts + 1, n1, s);
+        if (rc) return rc;
+        SVP_CUDA(cudaMemcpyAsync(&n2, c->counts + 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+        SVP_CUDA(cudaStreamSynchronize(s));
+        list2 = c->list2;
+    }
+    long long n3 = 0;
+    if (n2) {
+        rc = ensure_fallback(c, n2);
+        if (rc) return rc;
+        double *fb = c->fb, *plo = fb, *phi = fb + 27 * n2, *clo = fb + 2 * 27 * n2, *chi = fb + 3 * 27 * n2,
+               *smp = fb + 4 * 27 * n2;
+        fallback_grid_kernel<<<blocks_for(n2, 64, 16), 64, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
+                                                                    smp, c->fb_ok);
+        SVP_LAUNCH_CHECK("fallback_grid_kernel");
+        job_fail_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, c->fb_ok, n2, tile, c->tile_fail);
+        fallback_stage_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, clo, smp, n2, tile, c->tile_fail,
+                                                                      c->sel, c->acc);
+        SVP_LAUNCH_CHECK("fallback stage");
+        rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list3, c->counts + 2, n2, s);
+        if (rc) return rc;
+        SVP_CUDA(cudaMemcpyAsync(&n3, c->counts + 2, sizeof(long long), cudaMemcpyDeviceToHost, s));
+        SVP_CUDA(cudaStreamSynchronize(s));
+        if (n3) {
+            long long warps = n3 < c->heap_warps ? n3 : c->heap_warps;
+            warps = (warps + 3) / 4 * 4;
+            if (warps > c->heap_warps) warps = c->heap_warps;
+            rc = classify_launch(clo, chi, phi, c->list3, n3, delta, c->cfg.max_depth, c->cfg.max_boxes,
+                                 c->verdicts, c->heap, warps, c->heap_slots, s);
+            if (rc) return rc;
+            verdict_stage_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc);
+            witness_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc);
+            SVP_LAUNCH_CHECK("verdict stage");
+        }
+    }
+    SVP_CUDA(cudaMemcpyAsync(&acc, c->acc, sizeof acc, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    // the record (feasibility.py:755-771)
+    long long fallback = n2;
+    long long unknown = (long long)acc.unknown, bad = (long long)acc.bad;
+    int status = bad ? ST_INFEASIBLE : (unknown ? ST_UNCERTAIN : ST_FEASIBLE);
+    int reason = bad ? R_VIOLATION : (acc.arith ? R_ARITH : (unknown ? R_SUBDIV_BUDGET : R_BERNSTEIN));
+    long long fast = (long long)acc.fast, pre = (long long)acc.prescreened;
+    if ((fast || pre) && status == ST_FEASIBLE) reason = R_ENCLOSURE;
+    out->status = status;
+    out->reason = reason;
+    out->n_cells_checked = n;
+    out->n_uncertain = unknown;
+    out->n_infeasible = bad;
+    out->n_boxes = fast + pre + (long long)acc.fallback_ok_cells + (long long)acc.boxes_extra;
+    out->max_depth = acc.max_depth;
+    out->witness_cell = bad ? acc.witness_cell : -1;
+    out->n_fast_cells = fast;
+    out->n_fallback_cells = fallback;
+    out->n_prescreen_cells = pre;
+    if (acc.any_margin && !acc.arith) {
+        double lowest = key_value(acc.lowest_key);
+        out->min_margin_lower_bound = lowest;
+        out->min_jd_lower_bound = delta == 0. ? lowest : std::nextafter(lowest + delta, -INFINITY);
+        out->has_min_jd = 1;
+    }
+    if (!(fast || pre) && acc.sampled_key != kKeyPosInf) {
+        double sm = key_value(acc.sampled_key);
+        if (std::isfinite(sm)) { out->sampled_min_jd = sm; out->has_sampled_min = 1; }
+    }
+    if (bad && acc.has_witness)
+        for (int k = 0; k < 3; k++) out->witness_point[k] = acc.witness[k];
+    return SVP_OK;
+}

@@ -1,0 +1,54 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a); run with -m gpu")
+
+
+def same_bits(a, b):
+    """Bitwise equality of float64 arrays (NaN payloads included)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def same_bits_nan(a, b):
+    """Bitwise equality where both are not NaN, and NaN in the same places."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    na, nb = np.isnan(a), np.isnan(b)
+    return a.shape == b.shape and np.array_equal(na, nb) and same_bits(np.where(na, 0., a), np.where(nb, 0., b))
+
+
+@pytest.fixture(scope="session")
+def cert_golden():
+    return np.load(os.path.join(GOLDEN, "certificate.npz"))
+
+
+@pytest.fixture(scope="session")
+def cells_golden():
+    return np.load(os.path.join(GOLDEN, "cells.npz"))
+
+
+def cell_vertices(u, c):
+    nz, ny, nx = u.shape[:3]
+    cx, cy = nx - 1, ny - 1
+    x0, y0, z0 = c % cx, (c // cx) % cy, c // (cx * cy)
+    return np.array([u[z0 + (a >> 2), y0 + ((a >> 1) & 1), x0 + (a & 1)] for a in range(8)])
+
+
+def all_vertices(u):
+    nz, ny, nx = u.shape[:3]
+    n = (nz - 1) * (ny - 1) * (nx - 1)
+    c = np.arange(n)
+    cx, cy = nx - 1, ny - 1
+    x0, y0, z0 = c % cx, (c // cx) % cy, c // (cx * cy)
+    return np.stack([u[z0 + (a >> 2), y0 + ((a >> 1) & 1), x0 + (a & 1)] for a in range(8)], axis=1)
