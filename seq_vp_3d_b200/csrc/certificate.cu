@@ -327,9 +327,11 @@ enum { R_ENCLOSURE = 0, R_BERNSTEIN = 1, R_VIOLATION = 2, R_ARITH = 3, R_SUBDIV_
        R_DEPTH_BUDGET = 12 };
 
 // Per-warp scratch layout for S slots: coefficients (S, 54) doubles, meta (S, 8) doubles (low xyz, high xyz, key),
-// serial (S) int64, depth (S) int32, heap (S) int32, free stack (S) int32.
+// serial (S) int64, depth (S) int32, heap (S) int32, free stack (S) int32.  The per-warp stride is rounded up to
+// 256 bytes so that every warp's float64/int64 arrays stay 8-byte aligned.
 __host__ __device__ inline size_t warp_scratch_bytes(long long slots) {
-    return (size_t)slots * (54 * 8 + 8 * 8 + 8 + 4 + 4 + 4);
+    size_t b = (size_t)slots * (54 * 8 + 8 * 8 + 8 + 4 + 4 + 4);
+    return (b + 255) / 256 * 256;
 }
 
 __device__ __forceinline__ double warp_min27(double x) {
