@@ -108,6 +108,98 @@ int svp_certifier_create(const svp_grid *g, const svp_cert_config *cfg, svp_cert
 int svp_certifier_destroy(svp_certifier *c);
 int svp_certify_map(svp_certifier *c, const double *u, svp_cert_result *out, void *stream);
 
+/* ============================================================================================ registration pair
+ * One frozen subproblem's device constants: grid, fixed image, not-a-knot cubic spline of the moving image, the
+ * reference displacement u_ref of the proximal controls, the weights and the localized barrier.
+ * Replaces jd_curl/three_d/problem.py:284 Problem3D / :333 make_problem / :381 with_controls on the device side
+ * (backends/accelerated.py:363 AcceleratedHybridBackend owns the same constants). */
+typedef struct svp_weights {
+    double lam, mu, nu, kappa; /* problem.py:190 Weights3D */
+    double activation;         /* localized barrier activation a (0.05 in the reference's default route) */
+    double delta;              /* certificate delta (barrier domain J > delta) */
+} svp_weights;
+
+typedef struct svp_pair svp_pair;
+
+/* fixed, moving: (nz, ny, nx) float64; u_ref: (nz, ny, nx, 3).  The spline coefficients are computed on the device
+ * (interpolation.py:29 build_image_sampler: per-axis not-a-knot collocation, x then y then z). */
+int svp_pair_create(const svp_grid *g, const svp_weights *w, const double *fixed, const double *moving,
+                    const double *u_ref, svp_pair **out, void *stream);
+/* New proximal reference (problem.py:381 with_controls / :397 make_self_reference), copied from u_ref. */
+int svp_pair_set_reference(svp_pair *p, const double *u_ref, void *stream);
+int svp_pair_destroy(svp_pair *p);
+/* Copy of the spline coefficients (nz, ny, nx) into out (device). */
+int svp_pair_spline_coefficients(const svp_pair *p, double *out, void *stream);
+
+/* Moving image at X + u (and its physical xyz gradient when image_grad != NULL) at every node.
+ * Replaces interpolation.py:72 sample_points / :109 sample_value_gradient and backends/spline.py:81 TorchSpline.
+ * warped: (nz, ny, nx); image_grad: (nz, ny, nx, 3).  The caller certifies the sampling domain first. */
+int svp_warp(const svp_pair *p, const double *u, double *warped, double *image_grad, void *stream);
+/* Arbitrary points (n, 3) xyz inside the closed box: value (n,), gradient (n, 3) or NULL. */
+int svp_sample_points(const svp_pair *p, const double *points, int64_t n, double *value, double *gradient,
+                      void *stream);
+
+/* Energy terms (image, proximity, jd, curl, barrier) of u with its warped image, summed in double-double.
+ * Replaces residuals.py:302 _energy and backends/accelerated.py:1574 _energy.  terms5: host; barrier_violations:
+ * host count of closed27 points with J <= delta (the reference raises there).  Synchronizes. */
+int svp_energy(svp_pair *p, const double *u, const double *warped, double *terms5, int64_t *barrier_violations,
+               void *stream);
+/* Stable differences trial - base of E and of F = image + barrier, cancellation-free per residual and per
+ * barrier point (energy_comparison.py:223 _differences; backends/accelerated.py:3062 _compare).  diff2 host. */
+int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                          const double *trial_warped, double *diff2, void *stream);
+
+/* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
+#define SVP_TERM_IMAGE 1
+#define SVP_TERM_PROXIMITY 2
+#define SVP_TERM_JD 4
+#define SVP_TERM_CURL 8
+#define SVP_TERM_BARRIER 16
+#define SVP_TERM_TOTAL 31
+#define SVP_TERM_OUTER 17
+/* out: free-node vector (3 (nz-2)(ny-2)(nx-2)), component-major. */
+int svp_gradient(svp_pair *p, const double *u, const double *warped, const double *image_grad, int32_t terms,
+                 double *out, void *stream);
+/* gF (image + barrier), gD (image), gE (total) in one cell pass (linearization.py:217 outer_gradient_vectors). */
+int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, const double *image_grad, double *gF,
+                        double *gD, double *gE, void *stream);
+/* Exact diagonal of the frozen barrier GGN (linearization.py:357) and its action on a free vector p (:327). */
+int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out, void *stream);
+int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_grad, const double *pvec, double *out,
+                void *stream);
+
+/* Node JD measure J_a = min over the cells containing node a of (closed27 values and edge-quadratic minima)
+ * (solvers/jd_affine.py:205 node_min_jd without the face/interior extension).  node: (nz, ny, nx). */
+int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream);
+/* First root tau in (0, limit] of det(I + grad u + tau grad p) - delta over all closed27 points
+ * (solvers/global_jd_step.py:107 global_root_cpu; backends/torch_ops.py:636 global_jd_root).  root: host, +inf when
+ * no root; invalid: host count of points with det(I + grad u) - delta <= 0.  Synchronizes. */
+int svp_jd_root(svp_pair *p, const double *u, const double *pvec, double limit, double *root, int64_t *invalid,
+                void *stream);
+
+/* ============================================================================================ DST-I Poisson metric
+ * out = sign * s * M^-1 (s * rhs), M^-1 = DST . diag(1 / (omega (a + b lambda))) . DST per component (poisson.py:99
+ * PoissonInverse3D.apply; solvers/poisson_gradient.py:287 EquilibratedInverse; backends/hybrid.py:262
+ * apply_equilibrated).  metric: 0 = q1 spectrum, 1 = seven-point.  scale: free vector or NULL (s = 1);
+ * sign: +1 or -1 (the PG direction is -P^-1 g).  The per-axis DST-I is a dense GEMM with the orthonormal sine
+ * matrix; rhs and out may alias. */
+int svp_poisson_apply(svp_pair *p, double a, double b, int32_t metric, const double *scale, const double *rhs,
+                      double sign, double *out, void *stream);
+
+/* ============================================================================================ vector kernels
+ * Deterministic (fixed-order double-double) reductions and elementwise steps of the PG solver. */
+/* out (host) = sum a_i b_i. */
+int svp_dot(const double *a, const double *b, int64_t n, double *out, void *stream);
+/* y = x + tau p (free vectors). */
+int svp_axpy(const double *x, double tau, const double *pvec, int64_t n, double *y, void *stream);
+/* u (nz, ny, nx, 3) <- inject(theta) with exact zero faces (boundary.py:8 inject_free). */
+int svp_inject(const svp_grid *g, const double *theta, double *u, void *stream);
+/* theta <- restrict(field) (boundary.py:15 restrict_free). */
+int svp_restrict(const svp_grid *g, const double *field, double *theta, void *stream);
+/* Largest tau keeping every free node of X + u + tau p in the closed box: min of the quotients
+ * (solvers/poisson_gradient.py:993 sampling_step_bound; fast_checks.py:85 _step_bound_xu).  bound: host. */
+int svp_step_bound(const svp_grid *g, const double *u, const double *pvec, double *bound, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

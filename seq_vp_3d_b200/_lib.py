@@ -44,6 +44,10 @@ class CellVerdict(ctypes.Structure):
                 ("boxes", I64), ("depth", I64), ("margin", D), ("witness", D * 3)]
 
 
+class Weights(ctypes.Structure):
+    _fields_ = [("lam", D), ("mu", D), ("nu", D), ("kappa", D), ("activation", D), ("delta", D)]
+
+
 # name -> argtypes (restype int)
 SIGNATURES = {
     "svp_last_error": [ctypes.c_char_p, ctypes.c_size_t],
@@ -55,7 +59,30 @@ SIGNATURES = {
     "svp_certifier_create": [P, P, P],
     "svp_certifier_destroy": [P],
     "svp_certify_map": [P, P, P, P],
+    "svp_pair_create": [P, P, P, P, P, P, P],
+    "svp_pair_set_reference": [P, P, P],
+    "svp_pair_destroy": [P],
+    "svp_pair_spline_coefficients": [P, P, P],
+    "svp_warp": [P, P, P, P, P],
+    "svp_sample_points": [P, P, I64, P, P, P],
+    "svp_energy": [P, P, P, P, P, P],
+    "svp_energy_difference": [P, P, P, P, P, P, P],
+    "svp_gradient": [P, P, P, P, I32, P, P],
+    "svp_outer_gradients": [P, P, P, P, P, P, P, P],
+    "svp_ggn_diagonal": [P, P, P, P, P],
+    "svp_ggn_hvp": [P, P, P, P, P, P],
+    "svp_node_min_jd": [P, P, P, P],
+    "svp_jd_root": [P, P, P, D, P, P, P],
+    "svp_poisson_apply": [P, D, D, I32, P, P, D, P, P],
+    "svp_dot": [P, P, I64, P, P],
+    "svp_axpy": [P, D, P, I64, P, P],
+    "svp_inject": [P, P, P, P],
+    "svp_restrict": [P, P, P, P],
+    "svp_step_bound": [P, P, P, P, P],
 }
+
+TERM_IMAGE, TERM_PROXIMITY, TERM_JD, TERM_CURL, TERM_BARRIER = 1, 2, 4, 8, 16
+TERMS = {"image": 1, "proximity": 2, "jd": 4, "curl": 8, "barrier": 16, "total": 31, "outer": 17}
 
 _lib = None
 

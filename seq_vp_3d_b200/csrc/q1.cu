@@ -1,0 +1,1091 @@
+// Fused per-cell Q1 kernels of the certified-registration energy (FP64 plain form):
+//   warp_kernel        cubic B-spline value (+ gradient) at X + u, image and proximity energy sums
+//   cell_energy_kernel Gauss27 JD/curl penalties against u_ref, closed27 localized barrier
+//   cell_grad_kernel   per-cell vertex gradients (soft penalties, barrier) -> SoA locals
+//   gather_kernel      atomic-free node gather in fixed vertex order, plus the node terms
+//   ggn kernels, stable-difference kernels, node JD measure, global closed27 cubic root
+// Reference: jd_curl/three_d/{residuals.py, linearization.py, energy_comparison.py, interpolation.py,
+// solvers/jd_affine.py, solvers/global_jd_step.py}.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pair.cuh"
+
+namespace svp {
+namespace {
+
+constexpr int CT = 128;      // threads per block of the cell kernels
+constexpr int CELL_PER_SM = 8;
+
+// ============================================================================================== spline sampler
+struct SplineRef {
+    const double *c;
+    const double *t[3];  // x, y, z knots
+    long long n[3];      // nx, ny, nz coefficients per axis
+    double x0[3], h[3];
+};
+
+__device__ __forceinline__ int find_span(const double *__restrict__ t, long long n, double x, double x0, double h) {
+    long long i = (long long)floor((x - x0) / h);
+    long long s = i + 2;
+    s = s < 3 ? 3 : (s > n - 1 ? n - 1 : s);
+    while (s < n - 1 && __ldg(t + s + 1) <= x) s++;
+    while (s > 3 && __ldg(t + s) > x) s--;
+    return (int)s;
+}
+
+// backends/spline.py:12 cubic_basis: Cox-de Boor values and derivatives of the 4 B-splines on the span
+__device__ __forceinline__ void cubic_basis(const double *__restrict__ t, int s, double x, double B[4], double dB[4]) {
+    double b[4] = {1., 0., 0., 0.}, q[3];
+#pragma unroll
+    for (int degree = 1; degree <= 3; degree++) {
+        double nb[4];
+        double saved = 0.;
+#pragma unroll
+        for (int r = 0; r < degree; r++) {
+            double right = __ldg(t + s + r + 1) - x;
+            double left = x - __ldg(t + s + 1 - degree + r);
+            double temp = b[r] / (right + left);
+            nb[r] = saved + right * temp;
+            saved = left * temp;
+        }
+        nb[degree] = saved;
+#pragma unroll
+        for (int r = 0; r <= degree; r++) b[r] = nb[r];
+        if (degree == 2) { q[0] = b[0]; q[1] = b[1]; q[2] = b[2]; }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int idx = s - 3 + k;
+        double a = __ldg(t + idx + 3) - __ldg(t + idx), bb = __ldg(t + idx + 4) - __ldg(t + idx + 1);
+        double left = k == 0 ? 0. : q[k - 1], right = k == 3 ? 0. : q[k];
+        dB[k] = 3. * left / (a != 0. ? a : 1.) - 3. * right / (bb != 0. ? bb : 1.);
+        B[k] = b[k];
+    }
+}
+
+// value and (optionally) xyz gradient at physical point (x, y, z)
+template <bool GRAD>
+__device__ __forceinline__ double spline_eval(const SplineRef &S, double px, double py, double pz, double g[3]) {
+    int sx = find_span(S.t[0], S.n[0], px, S.x0[0], S.h[0]);
+    int sy = find_span(S.t[1], S.n[1], py, S.x0[1], S.h[1]);
+    int sz = find_span(S.t[2], S.n[2], pz, S.x0[2], S.h[2]);
+    double bx[4], dx[4], by[4], dy[4], bz[4], dz[4];
+    cubic_basis(S.t[0], sx, px, bx, dx);
+    cubic_basis(S.t[1], sy, py, by, dy);
+    cubic_basis(S.t[2], sz, pz, bz, dz);
+    const long long nx = S.n[0], ny = S.n[1];
+    const double *c = S.c + ((long long)(sz - 3) * ny + (sy - 3)) * nx + (sx - 3);
+    double val = 0., gx = 0., gy = 0., gz = 0.;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        double pv = 0., px_ = 0., py_ = 0.;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const double *row = c + ((long long)i * ny + j) * nx;
+            double c0 = __ldg(row), c1 = __ldg(row + 1), c2 = __ldg(row + 2), c3 = __ldg(row + 3);
+            double rv = c0 * bx[0] + c1 * bx[1] + c2 * bx[2] + c3 * bx[3];
+            pv += by[j] * rv;
+            if (GRAD) {
+                double rd = c0 * dx[0] + c1 * dx[1] + c2 * dx[2] + c3 * dx[3];
+                px_ += by[j] * rd;
+                py_ += dy[j] * rv;
+            }
+        }
+        val += bz[i] * pv;
+        if (GRAD) {
+            gx += bz[i] * px_;
+            gy += bz[i] * py_;
+            gz += dz[i] * pv;
+        }
+    }
+    if (GRAD) { g[0] = gx; g[1] = gy; g[2] = gz; }
+    return val;
+}
+
+__device__ __forceinline__ double node_weight(long long x, long long y, long long z, const Q1Const &q) {
+    double tx = (x == 0 || x == q.nx - 1) ? .5 : 1.;
+    double ty = (y == 0 || y == q.ny - 1) ? .5 : 1.;
+    double tz = (z == 0 || z == q.nz - 1) ? .5 : 1.;
+    return ((q.omega * tz) * ty) * tx;
+}
+
+// warped image at X + u (+ gradient), and the image / proximity energy sums (before the 1/2, lambda/2 factors)
+template <bool GRAD>
+__global__ void __launch_bounds__(256) warp_kernel(Q1Const q, SplineRef S, const double *__restrict__ u,
+                                                   const double *__restrict__ fixed, const double *__restrict__ uref,
+                                                   double *__restrict__ warped, double *__restrict__ image_grad,
+                                                   dd *partial) {
+    dd acc[2] = {{0., 0.}, {0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        double ux = u[3 * i], uy = u[3 * i + 1], uz = u[3 * i + 2];
+        double px = (q.x0[0] + q.h[0] * (double)x) + ux;
+        double py = (q.x0[1] + q.h[1] * (double)y) + uy;
+        double pz = (q.x0[2] + q.h[2] * (double)z) + uz;
+        double g[3];
+        double w = spline_eval<GRAD>(S, px, py, pz, g);
+        warped[i] = w;
+        if (GRAD) {
+            image_grad[3 * i] = g[0];
+            image_grad[3 * i + 1] = g[1];
+            image_grad[3 * i + 2] = g[2];
+        }
+        if (partial) {
+            double qw = node_weight(x, y, z, q);
+            double d = w - fixed[i];
+            double e0 = ux - uref[3 * i], e1 = uy - uref[3 * i + 1], e2 = uz - uref[3 * i + 2];
+            acc[0] = dd_add_d(acc[0], qw * d * d);
+            acc[1] = dd_add_d(acc[1], qw * (e0 * e0 + e1 * e1 + e2 * e2));
+        }
+    }
+    if (partial) block_reduce_dd<2>(acc, partial);
+}
+
+__global__ void __launch_bounds__(256) node_energy_kernel(Q1Const q, const double *__restrict__ u,
+                                                          const double *__restrict__ warped,
+                                                          const double *__restrict__ fixed,
+                                                          const double *__restrict__ uref, dd *partial) {
+    dd acc[2] = {{0., 0.}, {0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        double qw = node_weight(x, y, z, q);
+        double d = warped[i] - fixed[i];
+        double e0 = u[3 * i] - uref[3 * i], e1 = u[3 * i + 1] - uref[3 * i + 1], e2 = u[3 * i + 2] - uref[3 * i + 2];
+        acc[0] = dd_add_d(acc[0], qw * d * d);
+        acc[1] = dd_add_d(acc[1], qw * (e0 * e0 + e1 * e1 + e2 * e2));
+    }
+    block_reduce_dd<2>(acc, partial);
+}
+
+__global__ void __launch_bounds__(256) sample_points_kernel(SplineRef S, const double *__restrict__ pts, long long n,
+                                                            double *__restrict__ value, double *__restrict__ grad) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double g[3];
+        if (grad) {
+            value[i] = spline_eval<true>(S, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], g);
+            grad[3 * i] = g[0]; grad[3 * i + 1] = g[1]; grad[3 * i + 2] = g[2];
+        } else {
+            value[i] = spline_eval<false>(S, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], g);
+        }
+    }
+}
+
+// ============================================================================================== cell energy
+__device__ __forceinline__ void gauss_tables(const double v[8][3], const Q1Const &q, double G[3][3][3][3]) {
+    double E[3][4][3];
+    cell_edges(v, E);
+    point_derivatives(E, q.gn, q.gm, q.ih, G);
+}
+__device__ __forceinline__ void closed_tables(const double v[8][3], const Q1Const &q, double G[3][3][3][3]) {
+    const double n[3] = {0., .5, 1.}, m[3] = {1., .5, 0.};
+    double E[3][4][3];
+    cell_edges(v, E);
+    point_derivatives(E, n, m, q.ih, G);
+}
+
+// partial[block][0..2] = sum w (J - Jr)^2, sum w |C - Cr|^2, sum barrier; violations counted in *bad
+__global__ void __launch_bounds__(CT) cell_energy_kernel(Q1Const q, const double *__restrict__ u,
+                                                         const double *__restrict__ uref, dd *partial,
+                                                         unsigned long long *bad) {
+    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    unsigned long long nbad = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double v[8][3], G[3][3][3][3], Gr[3][3][3][3];
+        load_cell(u, n0, q, v);
+        gauss_tables(v, q, G);
+        {
+            double vr[8][3];
+            load_cell(uref, n0, q, vr);
+            gauss_tables(vr, q, Gr);
+        }
+        double sj = 0., sc = 0.;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], Vr[3][3], C[3], Cr[3];
+            grad_at(G, ix, iy, iz, V);
+            grad_at(Gr, ix, iy, iz, Vr);
+            double dj = det_only(V) - det_only(Vr);
+            curl_of(V, C);
+            curl_of(Vr, Cr);
+            double c0 = C[0] - Cr[0], c1 = C[1] - Cr[1], c2 = C[2] - Cr[2];
+            sj += q.gw[p] * dj * dj;
+            sc += q.gw[p] * (c0 * c0 + c1 * c1 + c2 * c2);
+        }
+        double Gc[3][3][3][3];
+        closed_tables(v, q, Gc);
+        double sb = 0.;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            double V[3][3];
+            grad_at(Gc, p % 3, (p / 3) % 3, p / 9, V);
+            double J = det_only(V);
+            if (!(J > q.delta)) { nbad++; continue; }
+            double b, b1, b2;
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+            sb += b;
+        }
+        acc[0] = dd_add_d(acc[0], sj);
+        acc[1] = dd_add_d(acc[1], sc);
+        acc[2] = dd_add_d(acc[2], sb);
+    }
+    block_reduce_dd<3>(acc, partial);
+    for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
+}
+
+// ============================================================================================== cell gradients
+// Per-cell vertex values -> SoA locals L[(a * 3 + r) * ncell + c].
+__device__ __forceinline__ void store_locals(double *__restrict__ L, long long c, long long ncell,
+                                             const double v[8][3]) {
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) L[(long long)(a * 3 + r) * ncell + c] = v[a][r];
+}
+
+// soft (JD + curl penalty) gradient of one cell into Ls; barrier gradient into Lb (zero if inactive)
+__device__ __forceinline__ void cell_soft_grad(const double v[8][3], const double vr[8][3], const Q1Const &q,
+                                               double Ls[8][3]) {
+    double G[3][3][3][3], Gr[3][3][3][3], S[3][3][3][3];
+    gauss_tables(v, q, G);
+    gauss_tables(vr, q, Gr);
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int s = 0; s < 3; s++)
+#pragma unroll
+            for (int t = 0; t < 3; t++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+#pragma unroll 1
+    for (int p = 0; p < 27; p++) {
+        int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+        double V[3][3], Vr[3][3], A[3][3], J, C[3], Cr[3];
+        grad_at(G, ix, iy, iz, V);
+        grad_at(Gr, ix, iy, iz, Vr);
+        cofactor_det(V, A, J);
+        double Jr = det_only(Vr);
+        curl_of(V, C);
+        curl_of(Vr, Cr);
+        double jd = q.mu * q.gw[p] * (J - Jr);
+        double k0 = q.nu * q.gw[p] * (C[0] - Cr[0]), k1 = q.nu * q.gw[p] * (C[1] - Cr[1]),
+               k2 = q.nu * q.gw[p] * (C[2] - Cr[2]);
+        double f[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * jd;
+        f[2][1] += k0; f[1][2] -= k0;
+        f[0][2] += k1; f[2][0] -= k1;
+        f[1][0] += k2; f[0][1] -= k2;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            S[0][iy][iz][r] += f[r][0];
+            S[1][ix][iz][r] += f[r][1];
+            S[2][ix][iy][r] += f[r][2];
+        }
+    }
+    scatter_edges(S, q.gn, q.gm, q.ih, Ls);
+}
+
+__device__ __forceinline__ bool cell_barrier_grad(const double v[8][3], const Q1Const &q, double Lb[8][3]) {
+    const double n[3] = {0., .5, 1.}, m[3] = {1., .5, 0.};
+    double G[3][3][3][3];
+    closed_tables(v, q, G);
+    double S[3][3][3][3];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int s = 0; s < 3; s++)
+#pragma unroll
+            for (int t = 0; t < 3; t++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+#pragma unroll 1
+    for (int p = 0; p < 27; p++) {
+        int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+        double V[3][3], A[3][3], J;
+        grad_at(G, ix, iy, iz, V);
+        cofactor_det(V, A, J);
+        if (!(J < q.act)) continue;
+        double b, b1, b2;
+        barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+        any = true;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            S[0][iy][iz][r] += A[r][0] * b1;
+            S[1][ix][iz][r] += A[r][1] * b1;
+            S[2][ix][iy][r] += A[r][2] * b1;
+        }
+    }
+    if (any) scatter_edges(S, n, m, q.ih, Lb);
+    return any;
+}
+
+// mode bit 0: soft penalties (jd, curl per the masks), bit 1: barrier.  Output layout:
+//   split = false: L1 = soft + barrier;  split = true: L1 = soft + barrier, L2 = barrier alone.
+__global__ void __launch_bounds__(CT) cell_grad_kernel(Q1Const q, const double *__restrict__ u,
+                                                       const double *__restrict__ uref, double mu_scale,
+                                                       double nu_scale, bool barrier, bool split,
+                                                       double *__restrict__ L1, double *__restrict__ L2) {
+    Q1Const qq = q;
+    qq.mu = q.mu * mu_scale;
+    qq.nu = q.nu * nu_scale;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double v[8][3], L[8][3], Lb[8][3];
+        load_cell(u, n0, q, v);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) { L[a][r] = 0.; Lb[a][r] = 0.; }
+        if (qq.mu != 0. || qq.nu != 0.) {
+            double vr[8][3];
+            load_cell(uref, n0, q, vr);
+            cell_soft_grad(v, vr, qq, L);
+        }
+        if (barrier) cell_barrier_grad(v, q, Lb);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) L[a][r] += Lb[a][r];
+        store_locals(L1, c, q.ncell, L);
+        if (split) store_locals(L2, c, q.ncell, Lb);
+    }
+}
+
+// ============================================================================================== gather
+struct GatherSpec {
+    int nout;
+    double ci[3], cp[3], c1[3], c2[3];  // coefficients of image, proximity, L1, L2 per output
+    double *out[3];
+};
+
+// Free node (z, y, x): sum of the 8 cells' vertex values in fixed order a = 0..7, plus node terms.
+__global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, const double *__restrict__ L1,
+                                                     const double *__restrict__ L2, const double *__restrict__ u,
+                                                     const double *__restrict__ uref,
+                                                     const double *__restrict__ warped,
+                                                     const double *__restrict__ fixed,
+                                                     const double *__restrict__ image_grad) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long node = (z * q.ny + y) * q.nx + x;
+        double qw = node_weight(x, y, z, q);
+        double dimg = warped ? qw * (warped[node] - fixed[node]) : 0.;
+        double s1[3] = {0., 0., 0.}, s2[3] = {0., 0., 0.};
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            long long c = ((z - (a >> 2)) * q.cy + (y - ((a >> 1) & 1))) * q.cx + (x - (a & 1));
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                if (L1) s1[r] += L1[(long long)(a * 3 + r) * q.ncell + c];
+                if (L2) s2[r] += L2[(long long)(a * 3 + r) * q.ncell + c];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double img = image_grad ? dimg * image_grad[3 * node + r] : 0.;
+            double prox = uref ? q.lam * qw * (u[3 * node + r] - uref[3 * node + r]) : 0.;
+            for (int k = 0; k < g.nout; k++)
+                g.out[k][r * q.nfree + i] = ((g.ci[k] * img + g.cp[k] * prox) + g.c1[k] * s1[r]) + g.c2[k] * s2[r];
+        }
+    }
+}
+
+// ============================================================================================== GGN
+// Per-cell diagonal contributions: sum_p w (mu lj^2 + nu cs) + sum_closed27 b'' lc^2, lj = sum_j A_rj D_jpa.
+__global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const double *__restrict__ u,
+                                                           double *__restrict__ L) {
+    const double cn[3] = {0., .5, 1.}, cm[3] = {1., .5, 0.};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double v[8][3], G[3][3][3][3], out[8][3];
+        load_cell(u, n0, q, v);
+        gauss_tables(v, q, G);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] = 0.;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], A[3][3], J;
+            grad_at(G, ix, iy, iz, V);
+            cofactor_det(V, A, J);
+            int id[3] = {ix, iy, iz};
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                int bits[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
+                double f[3], D[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) f[k] = bits[k] ? q.gn[id[k]] : q.gm[id[k]];
+                D[0] = (bits[0] ? q.ih[0] : -q.ih[0]) * f[1] * f[2];
+                D[1] = (bits[1] ? q.ih[1] : -q.ih[1]) * f[0] * f[2];
+                D[2] = (bits[2] ? q.ih[2] : -q.ih[2]) * f[0] * f[1];
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    double lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
+                    double cs = 0.;
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        if (j != r) cs += D[j] * D[j];
+                    out[a][r] += q.gw[p] * (q.mu * lj * lj + q.nu * cs);
+                }
+            }
+        }
+        double Gc[3][3][3][3];
+        closed_tables(v, q, Gc);
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], A[3][3], J;
+            grad_at(Gc, ix, iy, iz, V);
+            cofactor_det(V, A, J);
+            if (!(J < q.act)) continue;
+            double b, b1, b2;
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+            int id[3] = {ix, iy, iz};
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                int bits[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
+                double f[3], D[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) f[k] = bits[k] ? cn[id[k]] : cm[id[k]];
+                D[0] = (bits[0] ? q.ih[0] : -q.ih[0]) * f[1] * f[2];
+                D[1] = (bits[1] ? q.ih[1] : -q.ih[1]) * f[0] * f[2];
+                D[2] = (bits[2] ? q.ih[2] : -q.ih[2]) * f[0] * f[1];
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    double lc = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
+                    out[a][r] += b2 * lc * lc;
+                }
+            }
+        }
+        store_locals(L, c, q.ncell, out);
+    }
+}
+
+// GGN action on a node field vv (zero faces): Gauss JD/curl linearization + closed27 barrier curvature.
+__global__ void __launch_bounds__(CT) cell_ggn_hvp_kernel(Q1Const q, const double *__restrict__ u,
+                                                          const double *__restrict__ vv, double *__restrict__ L) {
+    const double cn[3] = {0., .5, 1.}, cm[3] = {1., .5, 0.};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double v[8][3], w[8][3], G[3][3][3][3], Gv[3][3][3][3], S[3][3][3][3], out[8][3];
+        load_cell(u, n0, q, v);
+        load_cell(vv, n0, q, w);
+        gauss_tables(v, q, G);
+        gauss_tables(w, q, Gv);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] = 0.;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int s = 0; s < 3; s++)
+#pragma unroll
+                for (int t = 0; t < 3; t++)
+#pragma unroll
+                    for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], W[3][3], A[3][3], J, K[3];
+            grad_at(G, ix, iy, iz, V);
+            grad_at(Gv, ix, iy, iz, W);
+            cofactor_det(V, A, J);
+            double jd = 0.;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) jd += A[r][jj] * W[r][jj];
+            curl_of(W, K);
+            jd *= q.mu * q.gw[p];
+            double k0 = q.nu * q.gw[p] * K[0], k1 = q.nu * q.gw[p] * K[1], k2 = q.nu * q.gw[p] * K[2];
+            double f[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * jd;
+            f[2][1] += k0; f[1][2] -= k0;
+            f[0][2] += k1; f[2][0] -= k1;
+            f[1][0] += k2; f[0][1] -= k2;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                S[0][iy][iz][r] += f[r][0];
+                S[1][ix][iz][r] += f[r][1];
+                S[2][ix][iy][r] += f[r][2];
+            }
+        }
+        scatter_edges(S, q.gn, q.gm, q.ih, out);
+        double Gc[3][3][3][3], Gcv[3][3][3][3];
+        closed_tables(v, q, Gc);
+        closed_tables(w, q, Gcv);
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int s = 0; s < 3; s++)
+#pragma unroll
+                for (int t = 0; t < 3; t++)
+#pragma unroll
+                    for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+        bool any = false;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], W[3][3], A[3][3], J;
+            grad_at(Gc, ix, iy, iz, V);
+            cofactor_det(V, A, J);
+            if (!(J < q.act)) continue;
+            grad_at(Gcv, ix, iy, iz, W);
+            double b, b1, b2;
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+            double lj = 0.;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) lj += A[r][jj] * W[r][jj];
+            lj *= b2;
+            any = true;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                S[0][iy][iz][r] += A[r][0] * lj;
+                S[1][ix][iz][r] += A[r][1] * lj;
+                S[2][ix][iy][r] += A[r][2] * lj;
+            }
+        }
+        if (any) scatter_edges(S, cn, cm, q.ih, out);
+        store_locals(L, c, q.ncell, out);
+    }
+}
+
+// node part of the GGN: q |b|^2 + lambda q (diagonal) or q b (b . v) + lambda q v (action)
+__global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const double *__restrict__ L,
+                                                       const double *__restrict__ image_grad,
+                                                       const double *__restrict__ vv, double *__restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long node = (z * q.ny + y) * q.nx + x;
+        double qw = node_weight(x, y, z, q);
+        double s[3] = {0., 0., 0.};
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            long long c = ((z - (a >> 2)) * q.cy + (y - ((a >> 1) & 1))) * q.cx + (x - (a & 1));
+#pragma unroll
+            for (int r = 0; r < 3; r++) s[r] += L[(long long)(a * 3 + r) * q.ncell + c];
+        }
+        const double *b = image_grad + 3 * node;
+        if (vv) {
+            const double *v = vv + 3 * node;
+            double bv = b[0] * v[0] + b[1] * v[1] + b[2] * v[2];
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[r * q.nfree + i] = (qw * b[r] * bv + q.lam * qw * v[r]) + s[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[r * q.nfree + i] = (qw * b[r] * b[r] + q.lam * qw) + s[r];
+        }
+    }
+}
+
+// ============================================================================================== stable differences
+// One residual pair: (b - a)(b + a) / 2 accumulated exactly enough in double-double.
+__device__ __forceinline__ dd sq_change(double a, double b) {
+    dd d = two_sum(b, -a), s = two_sum(b, a);
+    dd p = two_prod(d.hi, s.hi);
+    p.lo += d.hi * s.lo + d.lo * s.hi;
+    return {p.hi * .5, p.lo * .5};
+}
+
+// energy_comparison.py:145 localized branch (double precision), unweighted
+__device__ __forceinline__ double barrier_difference(double ja, double jb, double act, double d) {
+    double a = ja < act ? ja : act, b = jb < act ? jb : act;
+    double scale = act - d;
+    double ra = (act - a) / scale, rb = (act - b) / scale;
+    double h = (b - a) / scale;
+    double loga = ra < .5 ? log1p(-ra) : log((a - d) / scale);
+    double x = (b - a) / (a - d);
+    double ratio = x >= -.5 ? log1p(x) : log((b - d) / (a - d));
+    return h * (ra + rb) * loga - rb * rb * ratio;
+}
+
+__global__ void __launch_bounds__(256) node_diff_kernel(Q1Const q, const double *__restrict__ ua,
+                                                        const double *__restrict__ wa,
+                                                        const double *__restrict__ ub,
+                                                        const double *__restrict__ wb,
+                                                        const double *__restrict__ fixed,
+                                                        const double *__restrict__ uref, dd *partial) {
+    dd acc[2] = {{0., 0.}, {0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        double qw = node_weight(x, y, z, q);
+        double sq = sqrt(qw), sl = sqrt(q.lam * qw);
+        acc[0] = dd_add(acc[0], sq_change(sq * (wa[i] - fixed[i]), sq * (wb[i] - fixed[i])));
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            acc[1] = dd_add(acc[1], sq_change(sl * (ua[3 * i + r] - uref[3 * i + r]),
+                                              sl * (ub[3 * i + r] - uref[3 * i + r])));
+    }
+    block_reduce_dd<2>(acc, partial);
+}
+
+__global__ void __launch_bounds__(CT) cell_diff_kernel(Q1Const q, const double *__restrict__ ua,
+                                                       const double *__restrict__ ub,
+                                                       const double *__restrict__ uref, dd *partial) {
+    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double va[8][3], vb[8][3], vr[8][3];
+        double Ga[3][3][3][3], Gb[3][3][3][3], Gr[3][3][3][3];
+        load_cell(ua, n0, q, va);
+        load_cell(ub, n0, q, vb);
+        load_cell(uref, n0, q, vr);
+        gauss_tables(va, q, Ga);
+        gauss_tables(vb, q, Gb);
+        gauss_tables(vr, q, Gr);
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double Va[3][3], Vb[3][3], Vr[3][3], Ca[3], Cb[3], Cr[3];
+            grad_at(Ga, ix, iy, iz, Va);
+            grad_at(Gb, ix, iy, iz, Vb);
+            grad_at(Gr, ix, iy, iz, Vr);
+            double jr = det_only(Vr);
+            double smu = sqrt(q.mu * q.gw[p]), snu = sqrt(q.nu * q.gw[p]);
+            acc[0] = dd_add(acc[0], sq_change(smu * (det_only(Va) - jr), smu * (det_only(Vb) - jr)));
+            curl_of(Va, Ca);
+            curl_of(Vb, Cb);
+            curl_of(Vr, Cr);
+#pragma unroll
+            for (int r = 0; r < 3; r++) acc[1] = dd_add(acc[1], sq_change(snu * (Ca[r] - Cr[r]), snu * (Cb[r] - Cr[r])));
+        }
+        closed_tables(va, q, Ga);
+        closed_tables(vb, q, Gb);
+        double sb = 0.;
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double Va[3][3], Vb[3][3];
+            grad_at(Ga, ix, iy, iz, Va);
+            grad_at(Gb, ix, iy, iz, Vb);
+            double ja = det_only(Va), jb = det_only(Vb);
+            if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
+        }
+        acc[2] = dd_add_d(acc[2], q.bw * sb);
+    }
+    block_reduce_dd<3>(acc, partial);
+}
+
+// ============================================================================================== node JD measure
+__global__ void __launch_bounds__(CT) cell_min_jd_kernel(Q1Const q, const double *__restrict__ u,
+                                                         double *__restrict__ m) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        double v[8][3], G[3][3][3][3], J[27];
+        load_cell(u, cell_node0(c, q), q, v);
+        closed_tables(v, q, G);
+        double mn = __longlong_as_double(0x7FF0000000000000LL);
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            double V[3][3];
+            grad_at(G, p % 3, (p / 3) % 3, p / 9, V);
+            J[p] = det_only(V);
+            mn = fmin(mn, J[p]);
+        }
+        // exact interior minima of the edge quadratics through t = 0, 1/2, 1 (solvers/jd_affine.py:24)
+#pragma unroll 1
+        for (int e = 0; e < 12; e++) {
+            int f0, f1, f2;
+            if (e < 4) {            // x edges: iz, iy in {0, 2}
+                int iz = (e >> 1) * 2, iy = (e & 1) * 2;
+                f0 = 9 * iz + 3 * iy; f1 = f0 + 1; f2 = f0 + 2;
+            } else if (e < 8) {     // y edges: iz, ix in {0, 2}
+                int k = e - 4, iz = (k >> 1) * 2, ix = (k & 1) * 2;
+                f0 = 9 * iz + ix; f1 = f0 + 3; f2 = f0 + 6;
+            } else {                // z edges: iy, ix in {0, 2}
+                int k = e - 8, iy = (k >> 1) * 2, ix = (k & 1) * 2;
+                f0 = 3 * iy + ix; f1 = f0 + 9; f2 = f0 + 18;
+            }
+            double a = 2 * (J[f0] - 2 * J[f1] + J[f2]);
+            double b = -3 * J[f0] + 4 * J[f1] - J[f2];
+            if (a > 0 && b < 0 && -b < 2 * a) mn = fmin(mn, J[f0] - b * b / (4 * a));
+        }
+        m[c] = mn;
+    }
+}
+
+__global__ void __launch_bounds__(256) node_min_kernel(Q1Const q, const double *__restrict__ m,
+                                                       double *__restrict__ node) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        double mn = __longlong_as_double(0x7FF0000000000000LL);
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            long long cz = z - (a >> 2), cy = y - ((a >> 1) & 1), cx = x - (a & 1);
+            if (cz < 0 || cy < 0 || cx < 0 || cz >= q.cz || cy >= q.cy || cx >= q.cx) continue;
+            mn = fmin(mn, m[(cz * q.cy + cy) * q.cx + cx]);
+        }
+        node[i] = mn;
+    }
+}
+
+// ============================================================================================== global JD root
+// solvers/global_jd_step.py:52 first_roots for one point (b0 > 0), normalized s in (0, 1]; +inf if none
+__device__ double first_root(double b0, double b1, double b2, double b3) {
+    const double INF = __longlong_as_double(0x7FF0000000000000LL);
+    if (b0 > fabs(b1) + fabs(b2) + fabs(b3)) return INF;
+    const double nan = __longlong_as_double(0x7FF8000000000000LL);
+    double a = 3 * b3, b = 2 * b2, c = b1;
+    bool linear = a == 0;
+    double r_lin = (linear && b != 0) ? -c / b : nan;
+    double disc = b * b - 4 * a * c;
+    double sq = sqrt(disc >= 0 ? disc : 0.);
+    double qq = -(b + (b >= 0 ? sq : -sq)) / 2;
+    double r1 = (!linear && disc >= 0 && a != 0) ? qq / a : nan;
+    double r2 = (!linear && disc >= 0 && qq != 0) ? c / qq : nan;
+    if (linear) { r1 = r_lin; r2 = nan; }
+    r1 = (r1 > 0 && r1 < 1) ? r1 : 1.;
+    r2 = (r2 > 0 && r2 < 1) ? r2 : 1.;
+    double t1 = fmin(r1, r2), t2 = fmax(r1, r2);
+    auto qv = [&](double s) { return b0 + s * (b1 + s * (b2 + s * b3)); };
+    const double eps4 = 4 * 2.220446049250313e-16;
+    auto touch = [&](double s) { return eps4 * (fabs(b0) + s * (fabs(b1) + s * (fabs(b2) + s * fabs(b3)))); };
+    double lo, hi;
+    if (qv(t1) <= touch(t1)) { lo = 0.; hi = t1; }
+    else if (qv(t2) <= touch(t2)) { lo = t1; hi = t2; }
+    else if (qv(1.) <= 0) { lo = t2; hi = 1.; }
+    else return INF;
+    for (int k = 0; k < 50; k++) {
+        double mid = .5 * (lo + hi);
+        if (qv(mid) <= 0) hi = mid;
+        else lo = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(CT) jd_root_kernel(Q1Const q, const double *__restrict__ u,
+                                                     const double *__restrict__ pv, double limit,
+                                                     long long *__restrict__ best_key,
+                                                     unsigned long long *__restrict__ invalid) {
+    long long key = kKeyPosInf;
+    unsigned long long nbad = 0;
+    const double L2 = limit * limit, L3 = limit * limit * limit;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        double v[8][3], w[8][3], G[3][3][3][3], Gp[3][3][3][3];
+        load_cell(u, n0, q, v);
+        load_cell(pv, n0, q, w);
+        closed_tables(v, q, G);
+        closed_tables(w, q, Gp);
+#pragma unroll 1
+        for (int p = 0; p < 27; p++) {
+            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            double V[3][3], W[3][3], AF[3][3], AV[3][3], J, JV;
+            grad_at(G, ix, iy, iz, V);
+            grad_at(Gp, ix, iy, iz, W);
+            cofactor_det(V, AF, J);
+            // cofactor of V alone (no identity)
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                int j = (r + 1) % 3, k = (r + 2) % 3;
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++) {
+                    int l = (cc + 1) % 3, mm = (cc + 2) % 3;
+                    AV[r][cc] = W[j][l] * W[k][mm] - W[j][mm] * W[k][l];
+                }
+            }
+            JV = (W[0][0] * AV[0][0] + W[0][1] * AV[0][1]) + W[0][2] * AV[0][2];
+            double c0 = J - q.delta, c1 = 0., c2 = 0.;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++) {
+                    c1 += AF[r][cc] * W[r][cc];
+                    c2 += (V[r][cc] + (r == cc ? 1. : 0.)) * AV[r][cc];
+                }
+            if (!(c0 > 0)) { nbad++; continue; }
+            double s = first_root(c0, c1 * limit, c2 * L2, JV * L3);
+            long long k = order_key(s);
+            key = k < key ? k : key;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        long long y = __shfl_xor_sync(0xFFFFFFFFu, key, o);
+        key = y < key ? y : key;
+        nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(best_key, key);
+        if (nbad) atomicAdd(invalid, nbad);
+    }
+}
+
+// ============================================================================================== final reduction
+__global__ void final_reduce_kernel(const dd *__restrict__ partial, long long blocks, int K, double *out) {
+    // one block; thread t reduces blocks t, t + 256, ... in order, then a fixed tree
+    __shared__ dd sh[256];
+    for (int k = 0; k < K; k++) {
+        dd acc = {0., 0.};
+        for (long long b = threadIdx.x; b < blocks; b += blockDim.x) acc = dd_add(acc, partial[b * K + k]);
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s; s >>= 1) {
+            if ((int)threadIdx.x < s) sh[threadIdx.x] = dd_add(sh[threadIdx.x], sh[threadIdx.x + s]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) { out[2 * k] = sh[0].hi; out[2 * k + 1] = sh[0].lo; }
+        __syncthreads();
+    }
+}
+
+SplineRef spline_ref(const svp_pair *p) {
+    SplineRef S;
+    S.c = p->coeff;
+    for (int k = 0; k < 3; k++) {
+        S.t[k] = p->knots[k];
+        S.x0[k] = p->q.x0[k];
+        S.h[k] = p->q.h[k];
+    }
+    S.n[0] = p->q.nx; S.n[1] = p->q.ny; S.n[2] = p->q.nz;
+    return S;
+}
+
+unsigned cell_blocks(const svp_pair *p) { return blocks_for(p->q.ncell, CT, CELL_PER_SM); }
+unsigned node_blocks(long long n) { return blocks_for(n, 256, 8); }
+
+}  // namespace
+
+int pair_partials(svp_pair *p, long long blocks, int k) {
+    long long need = blocks * k;
+    if (need <= p->partial_cap) return SVP_OK;
+    cudaFree(p->partial);
+    p->partial = nullptr;
+    p->partial_cap = 0;
+    SVP_CUDA(cudaMalloc((void **)&p->partial, sizeof(dd) * need));
+    p->partial_cap = need;
+    return SVP_OK;
+}
+
+int pair_locals(svp_pair *p, int n) {
+    size_t bytes = sizeof(double) * 24 * (size_t)p->q.ncell;
+    if (n >= 1 && !p->loc1) SVP_CUDA(cudaMalloc((void **)&p->loc1, bytes));
+    if (n >= 2 && !p->loc2) SVP_CUDA(cudaMalloc((void **)&p->loc2, bytes));
+    return SVP_OK;
+}
+
+}  // namespace svp
+
+using namespace svp;
+
+extern "C" int svp_warp(const svp_pair *p, const double *u, double *warped, double *image_grad, void *stream) {
+    SVP_REQUIRE(p && u && warped, "svp_warp: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    SplineRef S = spline_ref(p);
+    unsigned nb = node_blocks(p->q.nnode);
+    if (image_grad)
+        warp_kernel<true><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, image_grad, nullptr);
+    else
+        warp_kernel<false><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, nullptr, nullptr);
+    SVP_LAUNCH_CHECK("warp_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_sample_points(const svp_pair *p, const double *points, int64_t n, double *value,
+                                 double *gradient, void *stream) {
+    SVP_REQUIRE(p && n >= 0, "svp_sample_points: invalid arguments");
+    if (!n) return SVP_OK;
+    SVP_REQUIRE(points && value, "svp_sample_points: null pointer");
+    sample_points_kernel<<<node_blocks(n), 256, 0, (cudaStream_t)stream>>>(spline_ref(p), points, n, value,
+                                                                           gradient);
+    SVP_LAUNCH_CHECK("sample_points_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_energy(svp_pair *p, const double *u, const double *warped, double *terms5,
+                          int64_t *barrier_violations, void *stream) {
+    SVP_REQUIRE(p && u && warped && terms5, "svp_energy: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = node_blocks(p->q.nnode), cb = cell_blocks(p);
+    int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
+    if (rc) return rc;
+    SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
+    node_energy_kernel<<<nb, 256, 0, s>>>(p->q, u, warped, p->fixed, p->u_ref, p->partial);
+    SVP_LAUNCH_CHECK("node_energy_kernel");
+    dd *pc = p->partial + (long long)nb * 2;
+    cell_energy_kernel<<<cb, CT, 0, s>>>(p->q, u, p->u_ref, pc, (unsigned long long *)p->counter);
+    SVP_LAUNCH_CHECK("cell_energy_kernel");
+    double node2[2], cell3[3];
+    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result);
+    final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4);
+    SVP_LAUNCH_CHECK("final_reduce_kernel");
+    double tmp[10];
+    long long bad = 0;
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaMemcpyAsync(&bad, p->counter, sizeof bad, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 2; k++) node2[k] = tmp[2 * k] + tmp[2 * k + 1];
+    for (int k = 0; k < 3; k++) cell3[k] = tmp[4 + 2 * k] + tmp[4 + 2 * k + 1];
+    terms5[0] = .5 * node2[0];
+    terms5[1] = .5 * p->q.lam * node2[1];
+    terms5[2] = .5 * p->q.mu * cell3[0];
+    terms5[3] = .5 * p->q.nu * cell3[1];
+    terms5[4] = cell3[2];
+    if (barrier_violations) *barrier_violations = bad;
+    return SVP_OK;
+}
+
+extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped,
+                                     const double *trial_u, const double *trial_warped, double *diff2,
+                                     void *stream) {
+    SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && diff2, "svp_energy_difference: null");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = node_blocks(p->q.nnode), cb = cell_blocks(p);
+    int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
+    if (rc) return rc;
+    node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
+                                        p->partial);
+    dd *pc = p->partial + (long long)nb * 2;
+    cell_diff_kernel<<<cb, CT, 0, s>>>(p->q, base_u, trial_u, p->u_ref, pc);
+    SVP_LAUNCH_CHECK("difference kernels");
+    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result);
+    final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4);
+    SVP_LAUNCH_CHECK("final_reduce_kernel");
+    double tmp[10];
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    // E = image + proximity + jd + curl + barrier; F = image + barrier (sums of double-double pieces)
+    double img = tmp[0] + tmp[1], prox = tmp[2] + tmp[3];
+    double jd = tmp[4] + tmp[5], curl = tmp[6] + tmp[7], bar = tmp[8] + tmp[9];
+    diff2[0] = (((img + prox) + jd) + curl) + bar;
+    diff2[1] = img + bar;
+    return SVP_OK;
+}
+
+static int run_gather(svp_pair *p, const GatherSpec &g, const double *L1, const double *L2, const double *u,
+                      const double *uref, const double *warped, const double *image_grad, cudaStream_t s) {
+    gather_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, g, L1, L2, u, uref, warped, p->fixed, image_grad);
+    SVP_LAUNCH_CHECK("gather_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                            int32_t terms, double *out, void *stream) {
+    SVP_REQUIRE(p && u && out, "svp_gradient: null argument");
+    SVP_REQUIRE((terms & ~SVP_TERM_TOTAL) == 0 && terms, "svp_gradient: invalid term mask");
+    bool img = terms & SVP_TERM_IMAGE;
+    SVP_REQUIRE(!img || (warped && image_grad), "svp_gradient: the image term needs warped and image_grad");
+    cudaStream_t s = (cudaStream_t)stream;
+    bool cellwork = terms & (SVP_TERM_JD | SVP_TERM_CURL | SVP_TERM_BARRIER);
+    if (cellwork) {
+        int rc = pair_locals(p, 1);
+        if (rc) return rc;
+        cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
+                                                       (terms & SVP_TERM_CURL) ? 1. : 0.,
+                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr);
+        SVP_LAUNCH_CHECK("cell_grad_kernel");
+    }
+    GatherSpec g{};
+    g.nout = 1;
+    g.ci[0] = img ? 1. : 0.;
+    g.cp[0] = (terms & SVP_TERM_PROXIMITY) ? 1. : 0.;
+    g.c1[0] = cellwork ? 1. : 0.;
+    g.out[0] = out;
+    return run_gather(p, g, cellwork ? p->loc1 : nullptr, nullptr, u, p->u_ref, img ? warped : nullptr,
+                      img ? image_grad : nullptr, s);
+}
+
+extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                                   double *gF, double *gD, double *gE, void *stream) {
+    SVP_REQUIRE(p && u && warped && image_grad && gF && gD && gE, "svp_outer_gradients: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = pair_locals(p, 2);
+    if (rc) return rc;
+    cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2);
+    SVP_LAUNCH_CHECK("cell_grad_kernel");
+    GatherSpec g{};
+    g.nout = 3;
+    // gF = image + barrier; gD = image; gE = image + proximity + soft + barrier
+    g.ci[0] = 1.; g.cp[0] = 0.; g.c1[0] = 0.; g.c2[0] = 1.; g.out[0] = gF;
+    g.ci[1] = 1.; g.cp[1] = 0.; g.c1[1] = 0.; g.c2[1] = 0.; g.out[1] = gD;
+    g.ci[2] = 1.; g.cp[2] = 1.; g.c1[2] = 1.; g.c2[2] = 0.; g.out[2] = gE;
+    return run_gather(p, g, p->loc1, p->loc2, u, p->u_ref, warped, image_grad, s);
+}
+
+extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out,
+                                void *stream) {
+    SVP_REQUIRE(p && u && image_grad && out, "svp_ggn_diagonal: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = pair_locals(p, 1);
+    if (rc) return rc;
+    cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1);
+    ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out);
+    SVP_LAUNCH_CHECK("ggn diagonal");
+    return SVP_OK;
+}
+
+extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_grad, const double *pvec,
+                           double *out, void *stream) {
+    SVP_REQUIRE(p && u && image_grad && pvec && out, "svp_ggn_hvp: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = pair_locals(p, 2);
+    if (rc) return rc;
+    // inject p into a node field (zero faces) held in loc2's storage
+    double *vv = p->loc2;
+    rc = svp_inject(&p->grid, pvec, vv, stream);
+    if (rc) return rc;
+    cell_ggn_hvp_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, p->loc1);
+    ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out);
+    SVP_LAUNCH_CHECK("ggn hvp");
+    return SVP_OK;
+}
+
+extern "C" int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream) {
+    SVP_REQUIRE(p && u && node, "svp_node_min_jd: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    cell_min_jd_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->cellbuf);
+    node_min_kernel<<<node_blocks(p->q.nnode), 256, 0, s>>>(p->q, p->cellbuf, node);
+    SVP_LAUNCH_CHECK("node_min_jd");
+    return SVP_OK;
+}
+
+extern "C" int svp_jd_root(svp_pair *p, const double *u, const double *pvec, double limit, double *root,
+                           int64_t *invalid, void *stream) {
+    SVP_REQUIRE(p && u && pvec && root && limit > 0, "svp_jd_root: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = pair_locals(p, 2);
+    if (rc) return rc;
+    double *vv = p->loc2;
+    rc = svp_inject(&p->grid, pvec, vv, stream);
+    if (rc) return rc;
+    long long init[2] = {kKeyPosInf, 0};
+    SVP_CUDA(cudaMemcpyAsync(p->counter, init, sizeof init, cudaMemcpyHostToDevice, s));
+    jd_root_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, limit, p->counter,
+                                                 (unsigned long long *)(p->counter + 1));
+    SVP_LAUNCH_CHECK("jd_root_kernel");
+    long long out[2];
+    SVP_CUDA(cudaMemcpyAsync(out, p->counter, sizeof out, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    double sv = key_value(out[0]);
+    *root = std::isfinite(sv) ? sv * limit : INFINITY;
+    if (invalid) *invalid = out[1];
+    return SVP_OK;
+}

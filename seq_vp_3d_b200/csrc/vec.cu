@@ -1,0 +1,167 @@
+// Vector kernels of the PG solver on free-node vectors: deterministic dot products, the trial axpy with the
+// reference's two roundings, inject/restrict between node fields and free vectors, and the domain step bound.
+#include <cmath>
+
+#include "pair.cuh"
+
+namespace svp {
+namespace {
+
+__global__ void __launch_bounds__(256) dot_kernel(const double *__restrict__ a, const double *__restrict__ b,
+                                                  long long n, dd *partial) {
+    dd acc[1] = {{0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        acc[0] = dd_add(acc[0], two_prod(a[i], b[i]));
+    block_reduce_dd<1>(acc, partial);
+}
+
+__global__ void dot_final_kernel(const dd *__restrict__ partial, long long blocks, double *out) {
+    __shared__ dd sh[256];
+    dd acc = {0., 0.};
+    for (long long b = threadIdx.x; b < blocks; b += blockDim.x) acc = dd_add(acc, partial[b]);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] = dd_add(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0].hi + sh[0].lo;
+}
+
+// y = fl(x + fl(tau * p)): the trial step's two roundings (no FMA), as base.theta + tau * direction
+__global__ void axpy_kernel(const double *__restrict__ x, double tau, const double *__restrict__ p, long long n,
+                            double *__restrict__ y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        y[i] = __dadd_rn(x[i], __dmul_rn(tau, p[i]));
+}
+
+__global__ void inject_kernel(long long nx, long long ny, long long nz, const double *__restrict__ theta,
+                              double *__restrict__ u) {
+    const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz, nn = nx * ny * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
+        long long f = ((z - 1) * fy + (y - 1)) * fx + (x - 1);
+#pragma unroll
+        for (int r = 0; r < 3; r++) u[3 * i + r] = face ? 0. : theta[r * nf + f];
+    }
+}
+
+__global__ void restrict_kernel(long long nx, long long ny, long long nz, const double *__restrict__ u,
+                                double *__restrict__ theta) {
+    const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz;
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
+         f += (long long)gridDim.x * blockDim.x) {
+        long long x = f % fx + 1, y = (f / fx) % fy + 1, z = f / (fx * fy) + 1;
+        long long i = (z * ny + y) * nx + x;
+#pragma unroll
+        for (int r = 0; r < 3; r++) theta[r * nf + f] = u[3 * i + r];
+    }
+}
+
+// fast_checks.py:85 _step_bound_xu: min over free nodes and components with d != 0 of
+// ((d > 0 ? top : bottom) - fl(axis + u)) / d; order-independent min via integer keys
+__global__ void step_bound_kernel(long long nx, long long ny, long long nz, double hx, double hy, double hz,
+                                  double x0, double y0, double z0, const double *__restrict__ u,
+                                  const double *__restrict__ p, long long *best) {
+    const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz;
+    const double h[3] = {hx, hy, hz}, o[3] = {x0, y0, z0};
+    const long long len[3] = {nx, ny, nz};
+    long long key = kKeyPosInf;
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
+         f += (long long)gridDim.x * blockDim.x) {
+        long long x = f % fx + 1, y = (f / fx) % fy + 1, z = f / (fx * fy) + 1;
+        long long idx[3] = {x, y, z};
+        long long i = (z * ny + y) * nx + x;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double d = p[r * nf + f];
+            if (d > 0 || d < 0) {
+                double base = __dadd_rn(o[r], __dmul_rn(h[r], (double)idx[r]));
+                double pt = __dadd_rn(base, u[3 * i + r]);
+                double lim = d > 0 ? __dadd_rn(o[r], __dmul_rn(h[r], (double)(len[r] - 1))) : o[r];
+                double qv = __ddiv_rn(__dsub_rn(lim, pt), d);
+                long long k = order_key(qv);
+                key = k < key ? k : key;
+            }
+        }
+    }
+    for (int s = 16; s; s >>= 1) {
+        long long y = __shfl_xor_sync(0xFFFFFFFFu, key, s);
+        key = y < key ? y : key;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMin(best, key);
+}
+
+}  // namespace
+}  // namespace svp
+
+using namespace svp;
+
+extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out, void *stream) {
+    SVP_REQUIRE(a && b && out && n >= 0, "svp_dot: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = blocks_for(n, 256, 4);
+    dd *part = nullptr;
+    SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * nb + sizeof(double), s));
+    double *res = (double *)(part + nb);
+    dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part);
+    dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res);
+    cudaError_t le = cudaGetLastError();
+    double host = 0.;
+    cudaError_t ce = cudaMemcpyAsync(&host, res, sizeof host, cudaMemcpyDeviceToHost, s);
+    cudaError_t fe = cudaFreeAsync(part, s);
+    if (le != cudaSuccess) return cuda_fail(le, "dot kernels");
+    if (ce != cudaSuccess) return cuda_fail(ce, "dot copy");
+    if (fe != cudaSuccess) return cuda_fail(fe, "dot free");
+    SVP_CUDA(cudaStreamSynchronize(s));
+    *out = host;
+    return SVP_OK;
+}
+
+extern "C" int svp_axpy(const double *x, double tau, const double *pvec, int64_t n, double *y, void *stream) {
+    SVP_REQUIRE(x && pvec && y && n >= 0, "svp_axpy: invalid argument");
+    if (!n) return SVP_OK;
+    axpy_kernel<<<blocks_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(x, tau, pvec, n, y);
+    SVP_LAUNCH_CHECK("axpy_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_inject(const svp_grid *g, const double *theta, double *u, void *stream) {
+    SVP_REQUIRE(grid_ok(g) && theta && u, "svp_inject: invalid argument");
+    inject_kernel<<<blocks_for(n_nodes(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, theta, u);
+    SVP_LAUNCH_CHECK("inject_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_restrict(const svp_grid *g, const double *field, double *theta, void *stream) {
+    SVP_REQUIRE(grid_ok(g) && field && theta, "svp_restrict: invalid argument");
+    restrict_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, field,
+                                                                                      theta);
+    SVP_LAUNCH_CHECK("restrict_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_step_bound(const svp_grid *g, const double *u, const double *pvec, double *bound, void *stream) {
+    SVP_REQUIRE(grid_ok(g) && u && pvec && bound, "svp_step_bound: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long *best = nullptr;
+    SVP_CUDA(cudaMallocAsync((void **)&best, sizeof(long long), s));
+    long long init = kKeyPosInf, host = 0;
+    cudaError_t e1 = cudaMemcpyAsync(best, &init, sizeof init, cudaMemcpyHostToDevice, s);
+    step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
+                                                                    g->y0, g->z0, u, pvec, best);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t e2 = cudaMemcpyAsync(&host, best, sizeof host, cudaMemcpyDeviceToHost, s);
+    cudaError_t e3 = cudaFreeAsync(best, s);
+    if (e1 != cudaSuccess) return cuda_fail(e1, "step bound init");
+    if (le != cudaSuccess) return cuda_fail(le, "step_bound_kernel");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "step bound copy");
+    if (e3 != cudaSuccess) return cuda_fail(e3, "step bound free");
+    SVP_CUDA(cudaStreamSynchronize(s));
+    *bound = key_value(host);
+    return SVP_OK;
+}

@@ -1,0 +1,159 @@
+"""Device registration pair: the Q1 energy/gradient/metric kernels of libsvp3d behind a small Python class.
+
+A DevicePair owns the frozen device constants of one subproblem (grid, fixed image, spline of the moving image,
+u_ref, weights) -- the device half of jd_curl/three_d/problem.py:284 Problem3D.  Every method takes and returns
+CUDA tensors (node fields (nz, ny, nx[, 3]) float64, free vectors (3 * n_free,) component-major).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import grid_struct, ptr, require_cuda, stream_ptr, to_device
+
+F64 = torch.float64
+
+
+class DevicePair:
+    def __init__(self, grid, fixed, moving, u_ref, *, lam, mu, nu, kappa, activation=.05, delta=0., stream=None):
+        require_cuda()
+        self.grid = grid
+        self.weights = (float(lam), float(mu), float(nu), float(kappa), float(activation), float(delta))
+        self._g = grid_struct(grid)
+        self._w = _lib.Weights(*self.weights)
+        f, m, r = to_device(fixed), to_device(moving), to_device(u_ref)
+        if tuple(f.shape) != grid.shape or tuple(m.shape) != grid.shape or tuple(r.shape) != grid.shape + (3,):
+            raise ValueError("fixed/moving (nz, ny, nx) and u_ref (nz, ny, nx, 3) required")
+        h = ctypes.c_void_p()
+        _lib.call("svp_pair_create", ctypes.byref(self._g), ctypes.byref(self._w), ptr(f), ptr(m), ptr(r),
+                  ctypes.byref(h), stream_ptr(stream))
+        self._h = h
+        self.device = f.device
+        nz, ny, nx = grid.shape
+        self.nnode, self.nfree = nz * ny * nx, (nz - 2) * (ny - 2) * (nx - 2)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().svp_pair_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------------ allocation helpers
+    def node(self, comps=0):
+        shape = self.grid.shape + ((comps,) if comps else ())
+        return torch.empty(shape, dtype=F64, device=self.device)
+
+    def free(self):
+        return torch.empty(3 * self.nfree, dtype=F64, device=self.device)
+
+    # ------------------------------------------------------------------ kernels
+    def set_reference(self, u_ref, stream=None):
+        r = to_device(u_ref)
+        _lib.call("svp_pair_set_reference", self._h, ptr(r), stream_ptr(stream))
+
+    def spline_coefficients(self, stream=None):
+        out = self.node()
+        _lib.call("svp_pair_spline_coefficients", self._h, ptr(out), stream_ptr(stream))
+        return out
+
+    def warp(self, u, with_gradient=False, stream=None):
+        w = self.node()
+        g = self.node(3) if with_gradient else None
+        _lib.call("svp_warp", self._h, ptr(u), ptr(w), ptr(g), stream_ptr(stream))
+        return w, g
+
+    def sample_points(self, points, with_gradient=True, stream=None):
+        pts = to_device(points).reshape(-1, 3).contiguous()
+        n = pts.shape[0]
+        v = torch.empty(n, dtype=F64, device=self.device)
+        g = torch.empty((n, 3), dtype=F64, device=self.device) if with_gradient else None
+        _lib.call("svp_sample_points", self._h, ptr(pts), n, ptr(v), ptr(g), stream_ptr(stream))
+        return v, g
+
+    def energy(self, u, warped, stream=None):
+        """(terms[5] image, proximity, jd, curl, barrier; number of barrier points with J <= delta)."""
+        t = (ctypes.c_double * 5)()
+        bad = ctypes.c_int64()
+        _lib.call("svp_energy", self._h, ptr(u), ptr(warped), t, ctypes.byref(bad), stream_ptr(stream))
+        return np.array(t[:]), int(bad.value)
+
+    def energy_difference(self, base_u, base_w, trial_u, trial_w, stream=None):
+        """(E(trial) - E(base), F(trial) - F(base)), cancellation-free."""
+        d = (ctypes.c_double * 2)()
+        _lib.call("svp_energy_difference", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(trial_w), d,
+                  stream_ptr(stream))
+        return d[0], d[1]
+
+    def gradient(self, u, warped, image_grad, term="total", out=None, stream=None):
+        out = self.free() if out is None else out
+        _lib.call("svp_gradient", self._h, ptr(u), ptr(warped), ptr(image_grad), _lib.TERMS[term], ptr(out),
+                  stream_ptr(stream))
+        return out
+
+    def outer_gradients(self, u, warped, image_grad, stream=None):
+        gF, gD, gE = self.free(), self.free(), self.free()
+        _lib.call("svp_outer_gradients", self._h, ptr(u), ptr(warped), ptr(image_grad), ptr(gF), ptr(gD), ptr(gE),
+                  stream_ptr(stream))
+        return gF, gD, gE
+
+    def ggn_diagonal(self, u, image_grad, stream=None):
+        out = self.free()
+        _lib.call("svp_ggn_diagonal", self._h, ptr(u), ptr(image_grad), ptr(out), stream_ptr(stream))
+        return out
+
+    def ggn_hvp(self, u, image_grad, p, stream=None):
+        out = self.free()
+        _lib.call("svp_ggn_hvp", self._h, ptr(u), ptr(image_grad), ptr(to_device(p)), ptr(out), stream_ptr(stream))
+        return out
+
+    def node_min_jd(self, u, stream=None):
+        out = self.node()
+        _lib.call("svp_node_min_jd", self._h, ptr(u), ptr(out), stream_ptr(stream))
+        return out
+
+    def jd_root(self, u, p, limit, stream=None):
+        """(tau of the first closed27 root in (0, limit] or None, invalid base points)."""
+        root = ctypes.c_double()
+        bad = ctypes.c_int64()
+        _lib.call("svp_jd_root", self._h, ptr(u), ptr(p), float(limit), ctypes.byref(root), ctypes.byref(bad),
+                  stream_ptr(stream))
+        r = root.value
+        return (None if not np.isfinite(r) else r), int(bad.value)
+
+    def poisson_apply(self, a, b, rhs, *, metric="q1", scale=None, sign=1., out=None, stream=None):
+        out = self.free() if out is None else out
+        _lib.call("svp_poisson_apply", self._h, float(a), float(b), 0 if metric == "q1" else 1, ptr(scale),
+                  ptr(rhs), float(sign), ptr(out), stream_ptr(stream))
+        return out
+
+    # ------------------------------------------------------------------ vector helpers
+    def inject(self, theta, out=None, stream=None):
+        out = self.node(3) if out is None else out
+        _lib.call("svp_inject", ctypes.byref(self._g), ptr(theta), ptr(out), stream_ptr(stream))
+        return out
+
+    def restrict(self, field, out=None, stream=None):
+        out = self.free() if out is None else out
+        _lib.call("svp_restrict", ctypes.byref(self._g), ptr(field), ptr(out), stream_ptr(stream))
+        return out
+
+    def step_bound(self, u, p, stream=None):
+        b = ctypes.c_double()
+        _lib.call("svp_step_bound", ctypes.byref(self._g), ptr(u), ptr(p), ctypes.byref(b), stream_ptr(stream))
+        return b.value
+
+
+def dot(a, b, stream=None):
+    out = ctypes.c_double()
+    _lib.call("svp_dot", ptr(a), ptr(b), a.numel(), ctypes.byref(out), stream_ptr(stream))
+    return out.value
+
+
+def axpy(x, tau, p, out=None, stream=None):
+    out = torch.empty_like(x) if out is None else out
+    _lib.call("svp_axpy", ptr(x), float(tau), ptr(p), x.numel(), ptr(out), stream_ptr(stream))
+    return out
