@@ -122,7 +122,7 @@ typedef struct svp_weights {
 typedef struct svp_pair svp_pair;
 
 /* fixed, moving: (nz, ny, nx) float64; u_ref: (nz, ny, nx, 3).  The spline coefficients are computed on the device
- * (interpolation.py:29 build_image_sampler: per-axis not-a-knot collocation, x then y then z). */
+ * (interpolation.py:29 build_image_sampler: per-axis not-a-knot collocation, z then y then x). */
 int svp_pair_create(const svp_grid *g, const svp_weights *w, const double *fixed, const double *moving,
                     const double *u_ref, svp_pair **out, void *stream);
 /* New proximal reference (problem.py:381 with_controls / :397 make_self_reference), copied from u_ref. */
@@ -199,6 +199,24 @@ int svp_restrict(const svp_grid *g, const double *field, double *theta, void *st
 /* Largest tau keeping every free node of X + u + tau p in the closed box: min of the quotients
  * (solvers/poisson_gradient.py:993 sampling_step_bound; fast_checks.py:85 _step_bound_xu).  bound: host. */
 int svp_step_bound(const svp_grid *g, const double *u, const double *pvec, double *bound, void *stream);
+
+/* BB2 secant products of the PG step (solvers/poisson_gradient.py:785 _step_proposal_fast): with s = theta -
+ * theta_old, y = g - g_old, iy = p_old - p, out4 (host) = (s.y, s.s, y.y, y.iy). */
+int svp_bb2_dots(const double *theta, const double *theta_old, const double *g, const double *g_old,
+                 const double *p_old, const double *pvec, int64_t n, double *out4, void *stream);
+/* out2 (host) = (max |a - b|, max |b|), NaN-propagating (fast_checks.py:120 _max_abs_diff, :111 _max_abs):
+ * the inputs of the relative step max|candidate - theta| / max(L, max|theta|) (solvers/common.py:70 step_ratio). */
+int svp_max_abs_diff(const double *a, const double *b, int64_t n, double *out2, void *stream);
+
+/* Image-curvature shift alpha = factor * mean over free nodes of (q/omega) |grad I(X+u)|^2 / 3
+ * (solvers/poisson_gradient.py:269 image_curvature_shift).  alpha: host. */
+int svp_image_shift(svp_pair *p, const double *image_grad, double factor, double *alpha, void *stream);
+/* Equilibrated, JD-affine damped PG scale S~ = sqrt(m) / sqrt(d) * r with r = min(1, max(J_a, floor) / activation)
+ * on the free nodes (solvers/poisson_gradient.py:473-533; solvers/jd_affine.py:228 affine_factors).
+ * diag: GGN diagonal (free vector), node_jd: (nz, ny, nx); scale: free vector out.  bad (host): number of entries
+ * where d <= 0 or the scale is not finite and positive (the reference raises there).  Synchronizes. */
+int svp_pg_scale(svp_pair *p, const double *diag, const double *node_jd, double m, double activation, double floor_,
+                 double *scale, int64_t *bad, void *stream);
 
 #ifdef __cplusplus
 }

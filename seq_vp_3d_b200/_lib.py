@@ -79,6 +79,10 @@ SIGNATURES = {
     "svp_inject": [P, P, P, P],
     "svp_restrict": [P, P, P, P],
     "svp_step_bound": [P, P, P, P, P],
+    "svp_bb2_dots": [P, P, P, P, P, P, I64, P, P],
+    "svp_max_abs_diff": [P, P, I64, P, P],
+    "svp_image_shift": [P, P, D, P, P],
+    "svp_pg_scale": [P, P, P, D, D, D, P, P, P],
 }
 
 TERM_IMAGE, TERM_PROXIMITY, TERM_JD, TERM_CURL, TERM_BARRIER = 1, 2, 4, 8, 16

@@ -839,6 +839,42 @@ __global__ void __launch_bounds__(CT) jd_root_kernel(Q1Const q, const double *__
     }
 }
 
+// ============================================================================================== PG metric pieces
+__global__ void __launch_bounds__(256) shift_kernel(Q1Const q, const double *__restrict__ image_grad, dd *partial) {
+    dd acc[1] = {{0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        const double *b = image_grad + 3 * ((z * q.ny + y) * q.nx + x);
+        double qo = node_weight(x, y, z, q) / q.omega;
+        acc[0] = dd_add_d(acc[0], qo * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2]));
+    }
+    block_reduce_dd<1>(acc, partial);
+}
+
+__global__ void __launch_bounds__(256) pg_scale_kernel(Q1Const q, const double *__restrict__ diag,
+                                                       const double *__restrict__ node, double sm, double act,
+                                                       double floor_, double *__restrict__ scale,
+                                                       unsigned long long *bad) {
+    unsigned long long nb = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        double ja = node[(z * q.ny + y) * q.nx + x];
+        double r = fmin(1., fmax(ja, floor_) / act);
+        if (!(ja == ja) || !(ja < INFINITY) || !(ja > -INFINITY)) nb++;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double d = diag[c * q.nfree + i];
+            double s = (sm / sqrt(d)) * r;
+            if (!(d > 0) || !(s > 0) || !(s < INFINITY)) nb++;
+            scale[c * q.nfree + i] = s;
+        }
+    }
+    for (int o = 16; o; o >>= 1) nb += __shfl_xor_sync(0xFFFFFFFFu, nb, o);
+    if ((threadIdx.x & 31) == 0 && nb) atomicAdd(bad, nb);
+}
+
 // ============================================================================================== final reduction
 __global__ void final_reduce_kernel(const dd *__restrict__ partial, long long blocks, int K, double *out) {
     // one block; thread t reduces blocks t, t + 256, ... in order, then a fixed tree
@@ -1087,5 +1123,36 @@ extern "C" int svp_jd_root(svp_pair *p, const double *u, const double *pvec, dou
     double sv = key_value(out[0]);
     *root = std::isfinite(sv) ? sv * limit : INFINITY;
     if (invalid) *invalid = out[1];
+    return SVP_OK;
+}
+
+extern "C" int svp_image_shift(svp_pair *p, const double *image_grad, double factor, double *alpha, void *stream) {
+    SVP_REQUIRE(p && image_grad && alpha, "svp_image_shift: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = node_blocks(p->q.nfree);
+    int rc = pair_partials(p, nb, 1);
+    if (rc) return rc;
+    shift_kernel<<<nb, 256, 0, s>>>(p->q, image_grad, p->partial);
+    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 1, p->result);
+    SVP_LAUNCH_CHECK("shift kernels");
+    double tmp[2];
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    *alpha = factor * ((tmp[0] + tmp[1]) / (double)p->q.nfree) / 3;
+    return SVP_OK;
+}
+
+extern "C" int svp_pg_scale(svp_pair *p, const double *diag, const double *node_jd, double m, double activation,
+                            double floor_, double *scale, int64_t *bad, void *stream) {
+    SVP_REQUIRE(p && diag && node_jd && scale && m > 0 && activation > 0, "svp_pg_scale: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long), s));
+    pg_scale_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, diag, node_jd, std::sqrt(m), activation, floor_,
+                                                            scale, (unsigned long long *)p->counter);
+    SVP_LAUNCH_CHECK("pg_scale_kernel");
+    long long host = 0;
+    SVP_CUDA(cudaMemcpyAsync(&host, p->counter, sizeof host, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    if (bad) *bad = host;
     return SVP_OK;
 }

@@ -1,6 +1,7 @@
 // Vector kernels of the PG solver on free-node vectors: deterministic dot products, the trial axpy with the
 // reference's two roundings, inject/restrict between node fields and free vectors, and the domain step bound.
 #include <cmath>
+#include <cstring>
 
 #include "pair.cuh"
 
@@ -96,10 +97,107 @@ __global__ void step_bound_kernel(long long nx, long long ny, long long nz, doub
     if ((threadIdx.x & 31) == 0) atomicMin(best, key);
 }
 
+__global__ void __launch_bounds__(256) bb2_kernel(const double *__restrict__ th, const double *__restrict__ th0,
+                                                  const double *__restrict__ g, const double *__restrict__ g0,
+                                                  const double *__restrict__ p0, const double *__restrict__ p,
+                                                  long long n, dd *partial) {
+    dd acc[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = th[i] - th0[i], y = g[i] - g0[i], iy = p0[i] - p[i];
+        acc[0] = dd_add(acc[0], two_prod(s, y));
+        acc[1] = dd_add(acc[1], two_prod(s, s));
+        acc[2] = dd_add(acc[2], two_prod(y, y));
+        acc[3] = dd_add(acc[3], two_prod(y, iy));
+    }
+    block_reduce_dd<4>(acc, partial);
+}
+
+__global__ void multi_final_kernel(const dd *__restrict__ partial, long long blocks, int K, double *out) {
+    __shared__ dd sh[256];
+    for (int k = 0; k < K; k++) {
+        dd acc = {0., 0.};
+        for (long long b = threadIdx.x; b < blocks; b += blockDim.x) acc = dd_add(acc, partial[b * K + k]);
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s; s >>= 1) {
+            if ((int)threadIdx.x < s) sh[threadIdx.x] = dd_add(sh[threadIdx.x], sh[threadIdx.x + s]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[k] = sh[0].hi + sh[0].lo;
+        __syncthreads();
+    }
+}
+
+// max |a - b| and max |b| as order keys of non-negative values; a NaN maps above +inf (propagates)
+__global__ void max_abs_diff_kernel(const double *__restrict__ a, const double *__restrict__ b, long long n,
+                                    long long *keys) {
+    long long k0 = 0, k1 = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double d = fabs(a[i] - b[i]), m = fabs(b[i]);
+        long long x = d != d ? 0x7FF8000000000000LL : __double_as_longlong(d);
+        long long y = m != m ? 0x7FF8000000000000LL : __double_as_longlong(m);
+        k0 = x > k0 ? x : k0;
+        k1 = y > k1 ? y : k1;
+    }
+    for (int s = 16; s; s >>= 1) {
+        long long x = __shfl_xor_sync(0xFFFFFFFFu, k0, s), y = __shfl_xor_sync(0xFFFFFFFFu, k1, s);
+        k0 = x > k0 ? x : k0;
+        k1 = y > k1 ? y : k1;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(keys, k0);
+        atomicMax(keys + 1, k1);
+    }
+}
+
 }  // namespace
 }  // namespace svp
 
 using namespace svp;
+
+extern "C" int svp_bb2_dots(const double *theta, const double *theta_old, const double *g, const double *g_old,
+                            const double *p_old, const double *pvec, int64_t n, double *out4, void *stream) {
+    SVP_REQUIRE(theta && theta_old && g && g_old && p_old && pvec && out4 && n >= 0, "svp_bb2_dots: invalid");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = blocks_for(n, 256, 4);
+    dd *part = nullptr;
+    SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * 4 * nb + 4 * sizeof(double), s));
+    double *res = (double *)(part + 4 * nb);
+    bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part);
+    multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res);
+    cudaError_t le = cudaGetLastError();
+    double host[4];
+    cudaError_t ce = cudaMemcpyAsync(host, res, sizeof host, cudaMemcpyDeviceToHost, s);
+    cudaError_t fe = cudaFreeAsync(part, s);
+    if (le != cudaSuccess) return cuda_fail(le, "bb2 kernels");
+    if (ce != cudaSuccess) return cuda_fail(ce, "bb2 copy");
+    if (fe != cudaSuccess) return cuda_fail(fe, "bb2 free");
+    SVP_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 4; k++) out4[k] = host[k];
+    return SVP_OK;
+}
+
+extern "C" int svp_max_abs_diff(const double *a, const double *b, int64_t n, double *out2, void *stream) {
+    SVP_REQUIRE(a && b && out2 && n >= 0, "svp_max_abs_diff: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long *keys = nullptr;
+    SVP_CUDA(cudaMallocAsync((void **)&keys, 2 * sizeof(long long), s));
+    cudaError_t e0 = cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s);
+    max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys);
+    cudaError_t le = cudaGetLastError();
+    long long host[2] = {0, 0};
+    cudaError_t ce = cudaMemcpyAsync(host, keys, sizeof host, cudaMemcpyDeviceToHost, s);
+    cudaError_t fe = cudaFreeAsync(keys, s);
+    if (e0 != cudaSuccess) return cuda_fail(e0, "max abs init");
+    if (le != cudaSuccess) return cuda_fail(le, "max_abs_diff_kernel");
+    if (ce != cudaSuccess) return cuda_fail(ce, "max abs copy");
+    if (fe != cudaSuccess) return cuda_fail(fe, "max abs free");
+    SVP_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 2; k++) memcpy(&out2[k], &host[k], sizeof(double));
+    return SVP_OK;
+}
 
 extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out, void *stream) {
     SVP_REQUIRE(a && b && out && n >= 0, "svp_dot: invalid argument");

@@ -13,6 +13,7 @@ certificate.npz   per-cell edge-hull margins/flags, float Bernstein prescreen bo
                   arrays and certify_map records on several grids/fields (feasibility.py, compiled_enclosure.py,
                   certificate_prescreen.py, compiled_fallback.py).
 cells.npz         standalone cells through fallback_arrays + _classify (subdivision verdicts, witnesses, budgets).
+seq.npz           the reference's solve_sequential (default PG route, T62 metric) on a small seeded pair.
 q1.npz            spline coefficients/samples, energy terms, gradients, GGN diagonal, GGN HVP, DST-I Poisson apply,
                   stable energy reductions of a small problem (residuals.py, linearization.py, poisson.py,
                   energy_comparison.py).
@@ -333,7 +334,7 @@ def make_cells(out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default="certificate,cells,q1")
+    ap.add_argument("--only", default="certificate,cells,q1,seq")
     args = ap.parse_args()
     import_reference(args.reference)
     only = set(args.only.split(","))
@@ -344,6 +345,9 @@ def main():
     if "q1" in only:
         from q1_golden import make_q1      # second half of this generator (energy, gradient, DST)
         make_q1(HERE)
+    if "seq" in only:
+        from q1_golden import make_seq     # the full certified proximal loop on a small pair
+        make_seq(HERE)
 
 
 if __name__ == "__main__":

@@ -135,3 +135,52 @@ def make_q1(out):
     np.savez_compressed(os.path.join(out, "q1.npz"), **data)
     print("q1.npz: energy", data["t1/energy"], "node73 min", node73[1:-1, 1:-1, 1:-1].min(),
           "roots", data["jd_root0"], data["jd_root1"])
+
+
+def make_seq(out):
+    """The reference's full certified proximal loop (CPU, default PG route with the T62 metric) on a small pair."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from seq_vp_3d_b200.synthetic import blob_pair, default_weights
+    from jd_curl.three_d.grid import make_grid_3d
+    from jd_curl.three_d.problem import Weights3D, make_problem
+    from jd_curl.three_d.feasibility import PrescreenCertificateConfig
+    from jd_curl.three_d.sequential import solve_sequential, SequentialReuseConfig3D
+    from jd_curl.three_d.solvers.poisson_gradient import ConservativePGConfig3D
+    shape, spacing = (14, 13, 12), (1.0, 1.0, 1.0)
+    fixed, moving, u_gt = blob_pair(shape, spacing, seed=3)
+    nz, ny, nx = shape
+    grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=1., hy=1., hz=1., unit="mm")
+    w = default_weights(shape, spacing)
+    weights = Weights3D(lam=w["lam"], mu=w["mu"], nu=w["nu"], kappa=w["kappa"])
+    config = PrescreenCertificateConfig(delta=0., max_depth=48, max_boxes=255, tile_size=65536, fallback_workers=2)
+    problem = make_problem(grid=grid, fixed_image=fixed, moving_image=moving, u_ref=np.zeros(grid.shape + (3,)),
+                           weights=weights, certificate_config=config, barrier_location="closed27_uniform",
+                           barrier_activation=.05)
+    inner = ConservativePGConfig3D(max_iterations=5, metric_policy="image_shift_ggn_equilibrated_jd_affine_v1",
+                                   resolution_exit=True)
+    outer = SequentialReuseConfig3D(max_iterations=6, eta0=.01)
+    res = solve_sequential(problem, np.zeros(3 * grid.n_free_scalar), solver="pg", inner_config=inner, config=outer)
+    rows = []
+    attempts = []
+    for k, row in enumerate(res.history):
+        rows.append([k, row["outer_accepted"], row["inner_accepted_steps"], row["E_start"],
+                     np.nan if row["E_candidate"] is None else row["E_candidate"], row["GF_before"],
+                     np.nan if row["GF_candidate"] is None else row["GF_candidate"], row["forcing_target"]])
+        for a in row["inner_history"]:
+            attempts.append([k, a["iteration"], a["attempt"], a["tau"], a["accepted"],
+                             np.nan if a["actual_reduction"] is None else a["actual_reduction"],
+                             a["energy_base"], a["gradient_norm"]])
+    e = res.final_state.energy
+    np.savez_compressed(os.path.join(out, "seq.npz"), fixed=fixed, moving=moving, spacing=np.array(spacing),
+                        weights=np.array([w["lam"], w["mu"], w["nu"], w["kappa"]]),
+                        status=np.array(res.status), reason=np.array(res.reason),
+                        theta=res.final_state.theta, rows=np.array(rows, dtype=np.float64),
+                        attempts=np.array(attempts, dtype=np.float64),
+                        inner_status=np.array([r["inner_status"] for r in res.history]),
+                        attempt_reasons=np.array([a["reason"] for r in res.history for a in r["inner_history"]]),
+                        final_energy=np.array([e.image, e.proximity, e.jd, e.curl, e.barrier]),
+                        gf=np.array([res.GF_initial, res.GF_final, res.GF_threshold]),
+                        counts=np.array([res.counts["outer_accepted"], res.counts["inner_calls"]]))
+    print("seq.npz:", res.status, res.reason, "outer", res.counts["outer_accepted"], "rows", len(rows),
+          "attempts", len(attempts), "final E", e.total)

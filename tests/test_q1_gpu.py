@@ -79,7 +79,9 @@ def test_stable_difference(gold):
     w2, _ = P.warp(u2)
     dE, dF = P.energy_difference(u1, w1, u2, w2)
     red = d["reduction"]            # actual = -(trial - base), resolution = 16 eps max(E)
-    assert abs(-dE - red[0]) <= red[1] / 64 and abs(-dF - red[2]) <= red[3] / 64, (dE, dF, red)
+    # within 1e-12 relative and within 1/8 of the reference's own comparison resolution
+    for got, ref, res in ((-dE, red[0], red[1]), (-dF, red[2], red[3])):
+        assert abs(got - ref) <= min(TOL * abs(ref), res / 8), (dE, dF, red)
 
 
 def test_poisson_metric_direction(gold):
@@ -121,10 +123,10 @@ def seeded_problem(shape, spacing, seed):
         moving += a * np.exp(-((zz - c[0] - d[0]) ** 2 + (yy - c[1] - d[1]) ** 2 + (xx - c[2] - d[2]) ** 2) / (2 * s * s))
     h = np.array(spacing)
     taper = (np.sin(np.pi * zz / (nz - 1)) * np.sin(np.pi * yy / (ny - 1)) * np.sin(np.pi * xx / (nx - 1)))
-    u = np.stack([taper * np.sin(2 * np.pi * (k + 1) * (xx + yy + zz) / 23 + k) for k in range(3)], -1) * 0.9 * h
+    u = np.stack([taper * np.sin(2 * np.pi * (k + 1) * (xx + yy + zz) / 23 + k) for k in range(3)], -1) * 0.15 * h
     # a local compression that activates the barrier
     g = np.exp(-((zz - nz // 2) ** 2 + (yy - ny // 2) ** 2) / 4.)
-    u[..., 0] += -0.96 * np.clip(xx - nx // 2, -1, 1) * h[0] * g
+    u[..., 0] += -0.94 * np.clip(xx - nx // 2, -1, 1) * h[0] * g
     u[[0, -1]] = 0.; u[:, [0, -1]] = 0.; u[:, :, [0, -1]] = 0.
     u_ref = 0.5 * u
     return fixed, moving, np.ascontiguousarray(u), np.ascontiguousarray(u_ref)
