@@ -42,6 +42,14 @@ typedef struct svp_grid {
 int svp_last_error(char *buf, size_t len);
 /* Library ABI version (major * 10000 + minor * 100 + patch). */
 int svp_version(void);
+/* Number of kernel launches this library made in the process so far (host counter).  No reference counterpart:
+ * the launch accounting of the measurement harness. */
+int svp_counters(int64_t *launches);
+/* Opt-in CUDA-event timing of the named hot kernels on their launch streams (resets the totals).  No reference
+ * counterpart (the reference times its backend methods with device syncs, backends/hybrid.py:23 timed). */
+int svp_timers_enable(int on);
+/* Launch count and summed device time (ms) of one named kernel since svp_timers_enable; synchronizes its events. */
+int svp_timer_read(const char *name, int64_t *count, double *total_ms);
 
 /* ============================================================================================ certificate
  * Status codes: 0 certified_feasible, 1 infeasible, 2 uncertain.  Reason codes (index into this list):

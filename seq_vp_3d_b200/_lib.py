@@ -52,6 +52,9 @@ class Weights(ctypes.Structure):
 SIGNATURES = {
     "svp_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "svp_version": [],
+    "svp_counters": [P],
+    "svp_timers_enable": [ctypes.c_int],
+    "svp_timer_read": [ctypes.c_char_p, P, P],
     "svp_edge_hull_margins": [P, P, D, P, P, P],
     "svp_prescreen_lower_bounds": [P, P, P, I64, P, P],
     "svp_fallback_arrays": [P, I64, P, D, P, P, P, P, P, P, P],

@@ -790,7 +790,7 @@ extern "C" int svp_edge_hull_margins(const svp_grid *g, const double *u, double 
     SVP_REQUIRE(grid_ok(g), "svp_edge_hull_margins: invalid grid");
     SVP_REQUIRE(u && margin && flag, "svp_edge_hull_margins: null pointer");
     CellGrid cg = cell_grid(g);
-    edge_hull_kernel<<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag);
+    { svp::KernelTimer _t("edge_hull_kernel", (cudaStream_t)stream); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag)); }
     SVP_LAUNCH_CHECK("edge_hull_kernel");
     return SVP_OK;
 }
@@ -803,8 +803,8 @@ extern "C" int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, co
     SVP_REQUIRE(u && cells && out, "svp_prescreen_lower_bounds: null pointer");
     CellGrid cg = cell_grid(g);
     PrescreenConst k = prescreen_const(cg.h);
-    prescreen_kernel<<<blocks_for(n, 128, 8), 128, 0, (cudaStream_t)stream>>>(u, cg, (const long long *)cells, n, k,
-                                                                               out);
+    { svp::KernelTimer _t("prescreen_kernel", (cudaStream_t)stream); SVP_LAUNCH(prescreen_kernel<<<blocks_for(n, 128, 8), 128, 0, (cudaStream_t)stream>>>(u, cg, (const long long *)cells, n, k,
+                                                                               out)); }
     SVP_LAUNCH_CHECK("prescreen_kernel");
     return SVP_OK;
 }
@@ -815,8 +815,8 @@ extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const doub
     SVP_REQUIRE(n >= 0 && spacing3, "svp_fallback_arrays: invalid arguments");
     if (n == 0) return SVP_OK;
     SVP_REQUIRE(vertices && p_lo && p_hi && c_lo && c_hi && samples && ok, "svp_fallback_arrays: null pointer");
-    fallback_vertices_kernel<<<blocks_for(n, 64, 16), 64, 0, (cudaStream_t)stream>>>(
-        vertices, n, spacing3[0], spacing3[1], spacing3[2], delta, p_lo, p_hi, c_lo, c_hi, samples, ok);
+    SVP_LAUNCH(fallback_vertices_kernel<<<blocks_for(n, 64, 16), 64, 0, (cudaStream_t)stream>>>(
+        vertices, n, spacing3[0], spacing3[1], spacing3[2], delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
     SVP_LAUNCH_CHECK("fallback_vertices_kernel");
     return SVP_OK;
 }
@@ -826,8 +826,8 @@ static int classify_launch(const double *c_lo, const double *c_hi, const double 
                            svp_cell_verdict *out, char *scratch, long long warps, long long slots,
                            cudaStream_t stream) {
     long long threads = 128, blocks = div_up(warps * 32, threads);
-    classify_kernel<<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(c_lo, c_hi, p_hi, rows, n, delta, max_depth,
-                                                                        max_boxes, out, scratch, slots);
+    { svp::KernelTimer _t("classify_kernel", stream); SVP_LAUNCH(classify_kernel<<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(c_lo, c_hi, p_hi, rows, n, delta, max_depth,
+                                                                        max_boxes, out, scratch, slots)); }
     SVP_LAUNCH_CHECK("classify_kernel");
     return SVP_OK;
 }
@@ -977,16 +977,16 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     out->min_jd_lower_bound = out->min_margin_lower_bound = out->sampled_min_jd = nan;
     out->witness_point[0] = out->witness_point[1] = out->witness_point[2] = nan;
 
-    accum_init_kernel<<<1, 1, 0, s>>>(c->acc);
-    precheck_kernel<<<blocks_for(n_nodes(&c->grid), 256, 8), 256, 0, s>>>(u, c->cg, c->grid.x0, c->grid.y0,
-                                                                            c->grid.z0, c->acc);
+    SVP_LAUNCH(accum_init_kernel<<<1, 1, 0, s>>>(c->acc));
+    { svp::KernelTimer _t("precheck_kernel", s); SVP_LAUNCH(precheck_kernel<<<blocks_for(n_nodes(&c->grid), 256, 8), 256, 0, s>>>(u, c->cg, c->grid.x0, c->grid.y0,
+                                                                            c->grid.z0, c->acc)); }
     SVP_LAUNCH_CHECK("precheck_kernel");
-    edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag);
+    { svp::KernelTimer _t("edge_hull_kernel", s); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag)); }
     SVP_LAUNCH_CHECK("edge_hull_kernel");
     SVP_CUDA(cudaMemsetAsync(c->tile_bad, 0, sizeof(int) * c->ntiles, s));
     SVP_CUDA(cudaMemsetAsync(c->tile_fail, 0, sizeof(int) * c->ntiles, s));
-    tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad);
-    hull_stage_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->margin, c->tile_bad, n, tile, c->sel, c->acc);
+    SVP_LAUNCH(tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad));
+    SVP_LAUNCH(hull_stage_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->margin, c->tile_bad, n, tile, c->sel, c->acc));
     SVP_LAUNCH_CHECK("hull stage");
     int rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list1, c->counts, n, s);
     if (rc) return rc;
@@ -1002,9 +1002,9 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     long long n1 = counts[0], n2 = n1;
     const long long *list2 = c->list1;
     if (c->cfg.prescreen && n1) {
-        prescreen_kernel<<<blocks_for(n1, 128, 8), 128, 0, s>>>(u, c->cg, c->list1, n1, c->pk, c->lower);
+        { svp::KernelTimer _t("prescreen_kernel", s); SVP_LAUNCH(prescreen_kernel<<<blocks_for(n1, 128, 8), 128, 0, s>>>(u, c->cg, c->list1, n1, c->pk, c->lower)); }
         SVP_LAUNCH_CHECK("prescreen_kernel");
-        prescreen_stage_kernel<<<blocks_for(n1, 256, 8), 256, 0, s>>>(c->lower, n1, delta, c->sel, c->acc);
+        SVP_LAUNCH(prescreen_stage_kernel<<<blocks_for(n1, 256, 8), 256, 0, s>>>(c->lower, n1, delta, c->sel, c->acc));
         SVP_LAUNCH_CHECK("prescreen stage");
         rc = select_flagged(c, c->list1, c->sel, c->list2, c->counts + 1, n1, s);
         if (rc) return rc;
@@ -1018,12 +1018,12 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
         if (rc) return rc;
         double *fb = c->fb, *plo = fb, *phi = fb + 27 * n2, *clo = fb + 2 * 27 * n2, *chi = fb + 3 * 27 * n2,
                *smp = fb + 4 * 27 * n2;
-        fallback_grid_kernel<<<blocks_for(n2, 64, 16), 64, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
-                                                                    smp, c->fb_ok);
+        { svp::KernelTimer _t("fallback_grid_kernel", s); SVP_LAUNCH(fallback_grid_kernel<<<blocks_for(n2, 64, 16), 64, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
+                                                                    smp, c->fb_ok)); }
         SVP_LAUNCH_CHECK("fallback_grid_kernel");
-        job_fail_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, c->fb_ok, n2, tile, c->tile_fail);
-        fallback_stage_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, clo, smp, n2, tile, c->tile_fail,
-                                                                      c->sel, c->acc);
+        SVP_LAUNCH(job_fail_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, c->fb_ok, n2, tile, c->tile_fail));
+        SVP_LAUNCH(fallback_stage_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, clo, smp, n2, tile, c->tile_fail,
+                                                                      c->sel, c->acc));
         SVP_LAUNCH_CHECK("fallback stage");
         rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list3, c->counts + 2, n2, s);
         if (rc) return rc;
@@ -1036,8 +1036,8 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
             rc = classify_launch(clo, chi, phi, c->list3, n3, delta, c->cfg.max_depth, c->cfg.max_boxes,
                                  c->verdicts, c->heap, warps, c->heap_slots, s);
             if (rc) return rc;
-            verdict_stage_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc);
-            witness_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc);
+            SVP_LAUNCH(verdict_stage_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
+            SVP_LAUNCH(witness_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
             SVP_LAUNCH_CHECK("verdict stage");
         }
     }

@@ -147,13 +147,13 @@ int apply_axis(const double *M, int axis, long long batch, long long n2, long lo
     if (axis == 0) {
         long long R = batch * n2 * n1;
         dim3 grid((unsigned)div_up(R, TM), (unsigned)div_up(n0, TN));
-        gemm_right_kernel<<<grid, 256, 0, s>>>(M, (int)n0, in, R, out);
+        { svp::KernelTimer _t("gemm_right_kernel", s); SVP_LAUNCH(gemm_right_kernel<<<grid, 256, 0, s>>>(M, (int)n0, in, R, out)); }
     } else if (axis == 1) {
         dim3 grid((unsigned)div_up(n0, TN), (unsigned)div_up(n1, TM), (unsigned)(batch * n2));
-        gemm_left_kernel<<<grid, 256, 0, s>>>(M, (int)n1, in, n0, n0, n1 * n0, out);
+        { svp::KernelTimer _t("gemm_left_kernel", s); SVP_LAUNCH(gemm_left_kernel<<<grid, 256, 0, s>>>(M, (int)n1, in, n0, n0, n1 * n0, out)); }
     } else {
         dim3 grid((unsigned)div_up(n1 * n0, TN), (unsigned)div_up(n2, TM), (unsigned)batch);
-        gemm_left_kernel<<<grid, 256, 0, s>>>(M, (int)n2, in, n1 * n0, n1 * n0, n2 * n1 * n0, out);
+        { svp::KernelTimer _t("gemm_left_kernel", s); SVP_LAUNCH(gemm_left_kernel<<<grid, 256, 0, s>>>(M, (int)n2, in, n1 * n0, n1 * n0, n2 * n1 * n0, out)); }
     }
     SVP_LAUNCH_CHECK("axis GEMM");
     return SVP_OK;
@@ -207,9 +207,9 @@ static int set_denominator(svp_pair *p, double a, double b, int metric, cudaStre
     double *dev = nullptr;
     SVP_CUDA(cudaMallocAsync((void **)&dev, sizeof(double) * host.size(), s));
     SVP_CUDA(cudaMemcpyAsync(dev, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice, s));
-    den_kernel<<<blocks_for(p->q.nfree, 256, 8), 256, 0, s>>>(p->den, p->q.fx, p->q.fy, p->q.fz, dev + off[0],
+    SVP_LAUNCH(den_kernel<<<blocks_for(p->q.nfree, 256, 8), 256, 0, s>>>(p->den, p->q.fx, p->q.fy, p->q.fz, dev + off[0],
                                                               dev + off[1], dev + off[2], dev + off[3], dev + off[4],
-                                                              dev + off[5], p->q.omega, a, b, metric);
+                                                              dev + off[5], p->q.omega, a, b, metric));
     SVP_LAUNCH_CHECK("den_kernel");
     SVP_CUDA(cudaFreeAsync(dev, s));
     p->den_a = a;
@@ -234,16 +234,16 @@ extern "C" int svp_poisson_apply(svp_pair *p, double a, double b, int32_t metric
     const long long f0 = p->q.fx, f1 = p->q.fy, f2 = p->q.fz;
     double *t0 = p->dst_tmp, *t1 = p->dst_tmp + n3;
     unsigned eb = blocks_for(n3, 256, 8);
-    scale_kernel<<<eb, 256, 0, s>>>(rhs, scale, 1., n3, t0);
+    SVP_LAUNCH(scale_kernel<<<eb, 256, 0, s>>>(rhs, scale, 1., n3, t0));
     SVP_LAUNCH_CHECK("scale_kernel");
     if ((rc = apply_axis(p->dst_mat[0], 0, 3, f2, f1, f0, t0, t1, s))) return rc;
     if ((rc = apply_axis(p->dst_mat[1], 1, 3, f2, f1, f0, t1, t0, s))) return rc;
     if ((rc = apply_axis(p->dst_mat[2], 2, 3, f2, f1, f0, t0, t1, s))) return rc;
-    divide_kernel<<<eb, 256, 0, s>>>(t1, p->den, nf, n3);
+    SVP_LAUNCH(divide_kernel<<<eb, 256, 0, s>>>(t1, p->den, nf, n3));
     if ((rc = apply_axis(p->dst_mat[0], 0, 3, f2, f1, f0, t1, t0, s))) return rc;
     if ((rc = apply_axis(p->dst_mat[1], 1, 3, f2, f1, f0, t0, t1, s))) return rc;
     if ((rc = apply_axis(p->dst_mat[2], 2, 3, f2, f1, f0, t1, t0, s))) return rc;
-    scale_kernel<<<eb, 256, 0, s>>>(t0, scale, sign, n3, out);
+    SVP_LAUNCH(scale_kernel<<<eb, 256, 0, s>>>(t0, scale, sign, n3, out));
     SVP_LAUNCH_CHECK("scale_kernel");
     return SVP_OK;
 }

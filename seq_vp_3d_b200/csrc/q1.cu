@@ -938,9 +938,9 @@ extern "C" int svp_warp(const svp_pair *p, const double *u, double *warped, doub
     SplineRef S = spline_ref(p);
     unsigned nb = node_blocks(p->q.nnode);
     if (image_grad)
-        warp_kernel<true><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, image_grad, nullptr);
+        { svp::KernelTimer _t("warp_kernel_grad", s); SVP_LAUNCH(warp_kernel<true><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, image_grad, nullptr)); }
     else
-        warp_kernel<false><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, nullptr, nullptr);
+        { svp::KernelTimer _t("warp_kernel", s); SVP_LAUNCH(warp_kernel<false><<<nb, 256, 0, s>>>(p->q, S, u, p->fixed, p->u_ref, warped, nullptr, nullptr)); }
     SVP_LAUNCH_CHECK("warp_kernel");
     return SVP_OK;
 }
@@ -950,8 +950,8 @@ extern "C" int svp_sample_points(const svp_pair *p, const double *points, int64_
     SVP_REQUIRE(p && n >= 0, "svp_sample_points: invalid arguments");
     if (!n) return SVP_OK;
     SVP_REQUIRE(points && value, "svp_sample_points: null pointer");
-    sample_points_kernel<<<node_blocks(n), 256, 0, (cudaStream_t)stream>>>(spline_ref(p), points, n, value,
-                                                                           gradient);
+    SVP_LAUNCH(sample_points_kernel<<<node_blocks(n), 256, 0, (cudaStream_t)stream>>>(spline_ref(p), points, n, value,
+                                                                           gradient));
     SVP_LAUNCH_CHECK("sample_points_kernel");
     return SVP_OK;
 }
@@ -964,14 +964,14 @@ extern "C" int svp_energy(svp_pair *p, const double *u, const double *warped, do
     int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
     if (rc) return rc;
     SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
-    node_energy_kernel<<<nb, 256, 0, s>>>(p->q, u, warped, p->fixed, p->u_ref, p->partial);
+    { svp::KernelTimer _t("node_energy_kernel", s); SVP_LAUNCH(node_energy_kernel<<<nb, 256, 0, s>>>(p->q, u, warped, p->fixed, p->u_ref, p->partial)); }
     SVP_LAUNCH_CHECK("node_energy_kernel");
     dd *pc = p->partial + (long long)nb * 2;
-    cell_energy_kernel<<<cb, CT, 0, s>>>(p->q, u, p->u_ref, pc, (unsigned long long *)p->counter);
+    { svp::KernelTimer _t("cell_energy_kernel", s); SVP_LAUNCH(cell_energy_kernel<<<cb, CT, 0, s>>>(p->q, u, p->u_ref, pc, (unsigned long long *)p->counter)); }
     SVP_LAUNCH_CHECK("cell_energy_kernel");
     double node2[2], cell3[3];
-    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result);
-    final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4);
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4));
     SVP_LAUNCH_CHECK("final_reduce_kernel");
     double tmp[10];
     long long bad = 0;
@@ -997,13 +997,13 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
     unsigned nb = node_blocks(p->q.nnode), cb = cell_blocks(p);
     int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
     if (rc) return rc;
-    node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
-                                        p->partial);
+    { svp::KernelTimer _t("node_diff_kernel", s); SVP_LAUNCH(node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
+                                        p->partial)); }
     dd *pc = p->partial + (long long)nb * 2;
-    cell_diff_kernel<<<cb, CT, 0, s>>>(p->q, base_u, trial_u, p->u_ref, pc);
+    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CT, 0, s>>>(p->q, base_u, trial_u, p->u_ref, pc)); }
     SVP_LAUNCH_CHECK("difference kernels");
-    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result);
-    final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4);
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4));
     SVP_LAUNCH_CHECK("final_reduce_kernel");
     double tmp[10];
     SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
@@ -1018,7 +1018,7 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
 
 static int run_gather(svp_pair *p, const GatherSpec &g, const double *L1, const double *L2, const double *u,
                       const double *uref, const double *warped, const double *image_grad, cudaStream_t s) {
-    gather_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, g, L1, L2, u, uref, warped, p->fixed, image_grad);
+    { svp::KernelTimer _t("gather_kernel", s); SVP_LAUNCH(gather_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, g, L1, L2, u, uref, warped, p->fixed, image_grad)); }
     SVP_LAUNCH_CHECK("gather_kernel");
     return SVP_OK;
 }
@@ -1034,9 +1034,9 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
     if (cellwork) {
         int rc = pair_locals(p, 1);
         if (rc) return rc;
-        cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
+        { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
-                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr);
+                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr)); }
         SVP_LAUNCH_CHECK("cell_grad_kernel");
     }
     GatherSpec g{};
@@ -1055,7 +1055,7 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 2);
     if (rc) return rc;
-    cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2);
+    { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
     GatherSpec g{};
     g.nout = 3;
@@ -1072,8 +1072,8 @@ extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *imag
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 1);
     if (rc) return rc;
-    cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1);
-    ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out);
+    { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1)); }
+    SVP_LAUNCH(ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out));
     SVP_LAUNCH_CHECK("ggn diagonal");
     return SVP_OK;
 }
@@ -1088,8 +1088,8 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
     double *vv = p->loc2;
     rc = svp_inject(&p->grid, pvec, vv, stream);
     if (rc) return rc;
-    cell_ggn_hvp_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, p->loc1);
-    ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out);
+    { svp::KernelTimer _t("cell_ggn_hvp_kernel", s); SVP_LAUNCH(cell_ggn_hvp_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, p->loc1)); }
+    SVP_LAUNCH(ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out));
     SVP_LAUNCH_CHECK("ggn hvp");
     return SVP_OK;
 }
@@ -1097,8 +1097,8 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
 extern "C" int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream) {
     SVP_REQUIRE(p && u && node, "svp_node_min_jd: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    cell_min_jd_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->cellbuf);
-    node_min_kernel<<<node_blocks(p->q.nnode), 256, 0, s>>>(p->q, p->cellbuf, node);
+    { svp::KernelTimer _t("cell_min_jd_kernel", s); SVP_LAUNCH(cell_min_jd_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->cellbuf)); }
+    SVP_LAUNCH(node_min_kernel<<<node_blocks(p->q.nnode), 256, 0, s>>>(p->q, p->cellbuf, node));
     SVP_LAUNCH_CHECK("node_min_jd");
     return SVP_OK;
 }
@@ -1114,8 +1114,8 @@ extern "C" int svp_jd_root(svp_pair *p, const double *u, const double *pvec, dou
     if (rc) return rc;
     long long init[2] = {kKeyPosInf, 0};
     SVP_CUDA(cudaMemcpyAsync(p->counter, init, sizeof init, cudaMemcpyHostToDevice, s));
-    jd_root_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, limit, p->counter,
-                                                 (unsigned long long *)(p->counter + 1));
+    { svp::KernelTimer _t("jd_root_kernel", s); SVP_LAUNCH(jd_root_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, limit, p->counter,
+                                                 (unsigned long long *)(p->counter + 1))); }
     SVP_LAUNCH_CHECK("jd_root_kernel");
     long long out[2];
     SVP_CUDA(cudaMemcpyAsync(out, p->counter, sizeof out, cudaMemcpyDeviceToHost, s));
@@ -1132,8 +1132,8 @@ extern "C" int svp_image_shift(svp_pair *p, const double *image_grad, double fac
     unsigned nb = node_blocks(p->q.nfree);
     int rc = pair_partials(p, nb, 1);
     if (rc) return rc;
-    shift_kernel<<<nb, 256, 0, s>>>(p->q, image_grad, p->partial);
-    final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 1, p->result);
+    SVP_LAUNCH(shift_kernel<<<nb, 256, 0, s>>>(p->q, image_grad, p->partial));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 1, p->result));
     SVP_LAUNCH_CHECK("shift kernels");
     double tmp[2];
     SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
@@ -1147,8 +1147,8 @@ extern "C" int svp_pg_scale(svp_pair *p, const double *diag, const double *node_
     SVP_REQUIRE(p && diag && node_jd && scale && m > 0 && activation > 0, "svp_pg_scale: invalid argument");
     cudaStream_t s = (cudaStream_t)stream;
     SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long), s));
-    pg_scale_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, diag, node_jd, std::sqrt(m), activation, floor_,
-                                                            scale, (unsigned long long *)p->counter);
+    SVP_LAUNCH(pg_scale_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, diag, node_jd, std::sqrt(m), activation, floor_,
+                                                            scale, (unsigned long long *)p->counter));
     SVP_LAUNCH_CHECK("pg_scale_kernel");
     long long host = 0;
     SVP_CUDA(cudaMemcpyAsync(&host, p->counter, sizeof host, cudaMemcpyDeviceToHost, s));

@@ -11,6 +11,18 @@ namespace svp {
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t err, const char *what);
+void count_launch();
+
+// Opt-in per-kernel CUDA-event timing (svp_timers_enable): a scope records an event pair on its stream around the
+// launches inside it; svp_timer_read resolves and sums them.
+class KernelTimer {
+  public:
+    KernelTimer(const char *name, cudaStream_t stream);
+    ~KernelTimer();
+  private:
+    int slot_;
+    cudaStream_t stream_;
+};
 }  // namespace svp
 
 #define SVP_CUDA(call)                                                                       \
@@ -23,6 +35,16 @@ int cuda_fail(cudaError_t err, const char *what);
     do {                                                                                     \
         cudaError_t _e = cudaGetLastError();                                                 \
         if (_e != cudaSuccess) return svp::cuda_fail(_e, what);                              \
+    } while (0)
+
+// Every kernel launch of the library goes through SVP_LAUNCH: it is counted (svp_counters) and its launch error
+// returned as an SVP status.
+#define SVP_LAUNCH(...)                                                                      \
+    do {                                                                                     \
+        __VA_ARGS__;                                                                         \
+        svp::count_launch();                                                                 \
+        cudaError_t _e = cudaGetLastError();                                                 \
+        if (_e != cudaSuccess) return svp::cuda_fail(_e, #__VA_ARGS__);                      \
     } while (0)
 
 #define SVP_REQUIRE(cond, msg)                                                               \

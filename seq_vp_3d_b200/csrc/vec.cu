@@ -165,8 +165,8 @@ extern "C" int svp_bb2_dots(const double *theta, const double *theta_old, const 
     dd *part = nullptr;
     SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * 4 * nb + 4 * sizeof(double), s));
     double *res = (double *)(part + 4 * nb);
-    bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part);
-    multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res);
+    SVP_LAUNCH(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
+    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res));
     cudaError_t le = cudaGetLastError();
     double host[4];
     cudaError_t ce = cudaMemcpyAsync(host, res, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -185,7 +185,7 @@ extern "C" int svp_max_abs_diff(const double *a, const double *b, int64_t n, dou
     long long *keys = nullptr;
     SVP_CUDA(cudaMallocAsync((void **)&keys, 2 * sizeof(long long), s));
     cudaError_t e0 = cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s);
-    max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys);
+    SVP_LAUNCH(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
     cudaError_t le = cudaGetLastError();
     long long host[2] = {0, 0};
     cudaError_t ce = cudaMemcpyAsync(host, keys, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -206,8 +206,8 @@ extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out,
     dd *part = nullptr;
     SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * nb + sizeof(double), s));
     double *res = (double *)(part + nb);
-    dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part);
-    dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res);
+    SVP_LAUNCH(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
+    SVP_LAUNCH(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res));
     cudaError_t le = cudaGetLastError();
     double host = 0.;
     cudaError_t ce = cudaMemcpyAsync(&host, res, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -223,22 +223,22 @@ extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out,
 extern "C" int svp_axpy(const double *x, double tau, const double *pvec, int64_t n, double *y, void *stream) {
     SVP_REQUIRE(x && pvec && y && n >= 0, "svp_axpy: invalid argument");
     if (!n) return SVP_OK;
-    axpy_kernel<<<blocks_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(x, tau, pvec, n, y);
+    SVP_LAUNCH(axpy_kernel<<<blocks_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(x, tau, pvec, n, y));
     SVP_LAUNCH_CHECK("axpy_kernel");
     return SVP_OK;
 }
 
 extern "C" int svp_inject(const svp_grid *g, const double *theta, double *u, void *stream) {
     SVP_REQUIRE(grid_ok(g) && theta && u, "svp_inject: invalid argument");
-    inject_kernel<<<blocks_for(n_nodes(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, theta, u);
+    SVP_LAUNCH(inject_kernel<<<blocks_for(n_nodes(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, theta, u));
     SVP_LAUNCH_CHECK("inject_kernel");
     return SVP_OK;
 }
 
 extern "C" int svp_restrict(const svp_grid *g, const double *field, double *theta, void *stream) {
     SVP_REQUIRE(grid_ok(g) && field && theta, "svp_restrict: invalid argument");
-    restrict_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, field,
-                                                                                      theta);
+    SVP_LAUNCH(restrict_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, (cudaStream_t)stream>>>(g->nx, g->ny, g->nz, field,
+                                                                                      theta));
     SVP_LAUNCH_CHECK("restrict_kernel");
     return SVP_OK;
 }
@@ -250,8 +250,8 @@ extern "C" int svp_step_bound(const svp_grid *g, const double *u, const double *
     SVP_CUDA(cudaMallocAsync((void **)&best, sizeof(long long), s));
     long long init = kKeyPosInf, host = 0;
     cudaError_t e1 = cudaMemcpyAsync(best, &init, sizeof init, cudaMemcpyHostToDevice, s);
-    step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
-                                                                    g->y0, g->z0, u, pvec, best);
+    SVP_LAUNCH(step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
+                                                                    g->y0, g->z0, u, pvec, best));
     cudaError_t le = cudaGetLastError();
     cudaError_t e2 = cudaMemcpyAsync(&host, best, sizeof host, cudaMemcpyDeviceToHost, s);
     cudaError_t e3 = cudaFreeAsync(best, s);
