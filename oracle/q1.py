@@ -113,6 +113,14 @@ def local(u, grid, cells=None):
     return u.reshape(-1, 3)[cell_nodes(grid, cells)]          # (ncell, 8, 3)
 
 
+TILE = 8192       # cells per tile (the reference's MemoryConfig.cell_tile_size)
+
+
+def tiles(grid):
+    for start in range(0, grid.n_cells, TILE):
+        yield np.arange(start, min(start + TILE, grid.n_cells))
+
+
 # ----------------------------------------------------------------------------------------------- geometry
 def cofactor(F):
     out = np.empty(F.shape)
@@ -122,9 +130,21 @@ def cofactor(F):
     return out
 
 
+def grad_points(loc, op):
+    """V[n, p, r, j] = sum_a loc[n, a, r] D[j, p, a]: per component/axis (cells, 8) @ (8, P) products, as
+    geometry.py:268-272 forms them."""
+    n, P = loc.shape[0], op.D.shape[1]
+    V = np.empty((n, P, 3, 3))
+    for r in range(3):
+        v = np.ascontiguousarray(loc[:, :, r])
+        for j in range(3):
+            V[..., r, j] = v @ op.D[j].T
+    return V
+
+
 def geometry(loc, op):
     """F (n,P,3,3), A, J (n,P), curl (n,P,3) from local vertex displacements (n,8,3)."""
-    V = np.einsum("nar,jpa->nprj", loc, op.D)
+    V = grad_points(loc, op)
     F = V + np.eye(3)
     A = cofactor(F)
     J = np.sum(F[..., 0, :] * A[..., 0, :], axis=-1)
@@ -250,18 +270,21 @@ def warp(problem, u, with_gradient=False):
 
 
 def cell_terms(problem, u):
-    """(jd, curl, barrier) longdouble sums over all cells (residuals.py:279 _cell_energy)."""
+    """(jd, curl, barrier) longdouble sums over all cells, tile by tile (residuals.py:279 _cell_energy)."""
     g = problem.grid
     G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
-    _, _, J, curl = geometry(local(u, g), G)
-    _, _, Jr, curlr = geometry(local(problem.u_ref, g), G)
-    jd = .5 * problem.mu * np.sum(G.weights * (J - Jr) ** 2, dtype=np.longdouble)
-    cu = .5 * problem.nu * np.sum(G.weights[None, :, None] * (curl - curlr) ** 2, dtype=np.longdouble)
-    _, _, Jc, _ = geometry(local(u, g), C)
-    if np.any(Jc <= problem.delta):
-        raise FloatingPointError("barrier point J <= delta")
-    b, _, _ = barrier_terms(Jc, problem.delta, problem.barrier_weight, problem.activation)
-    return jd, cu, np.sum(b, dtype=np.longdouble)
+    jd = cu = bar = np.longdouble(0)
+    for t in tiles(g):
+        _, _, J, curl = geometry(local(u, g, t), G)
+        _, _, Jr, curlr = geometry(local(problem.u_ref, g, t), G)
+        jd += .5 * problem.mu * np.sum(G.weights * (J - Jr) ** 2, dtype=np.longdouble)
+        cu += .5 * problem.nu * np.sum(G.weights[None, :, None] * (curl - curlr) ** 2, dtype=np.longdouble)
+        _, _, Jc, _ = geometry(local(u, g, t), C)
+        if np.any(Jc <= problem.delta):
+            raise FloatingPointError("barrier point J <= delta")
+        b, _, _ = barrier_terms(Jc, problem.delta, problem.barrier_weight, problem.activation)
+        bar += np.sum(b, dtype=np.longdouble)
+    return jd, cu, bar
 
 
 def energy(problem, u, warped=None):
@@ -275,14 +298,13 @@ def energy(problem, u, warped=None):
     return np.array([float(image), float(prox), float(jd), float(cu), float(bar)])
 
 
-def _scatter(grid, op, flux, out):
-    """out (3, nz, ny, nx) += D^T flux (flux (n,P,3,3) [r, j])."""
-    loc = np.einsum("nprj,jpa->nar", flux, op.D)              # (n, 8, 3)
-    nodes = cell_nodes(grid)
+def _scatter(grid, op, flux, out, cells=None):
+    """out (3, nz, ny, nx) += D^T flux (flux (n,P,3,3) [r, j]) (cell_q1.py:186 _transpose_add)."""
+    nodes = cell_nodes(grid, cells)
+    size = out[0].size
     for r in range(3):
-        flat = out[r].ravel()
-        for a in range(8):
-            np.add.at(flat, nodes[:, a], loc[:, a, r])
+        loc = sum(np.ascontiguousarray(flux[..., r, j]) @ op.D[j] for j in range(3))   # (n, 8)
+        out[r] += np.bincount(nodes.ravel(), weights=loc.ravel(), minlength=size).reshape(out[r].shape)
 
 
 def _flux(A, jd, curl):
@@ -316,18 +338,18 @@ def gradient(problem, u, warped, image_grad, term="total"):
         out += np.moveaxis(q[..., None] * (warped - problem.fixed)[..., None] * image_grad, -1, 0)
     if term in ("total", "proximity"):
         out += np.moveaxis(problem.lam * q[..., None] * (u - problem.u_ref), -1, 0)
-    if term in ("total", "jd", "curl"):
-        G = ops(g, "gauss27")
-        _, A, J, curl = geometry(local(u, g), G)
-        _, _, Jr, curlr = geometry(local(problem.u_ref, g), G)
-        jd = problem.mu * G.weights * (J - Jr) if term != "curl" else np.zeros_like(J)
-        cu = problem.nu * G.weights[None, :, None] * (curl - curlr) if term != "jd" else None
-        _scatter(g, G, _flux(A, jd, cu), out)
-    if term in ("total", "outer", "barrier"):
-        C = ops(g, "closed27_uniform")
-        _, A, J, _ = geometry(local(u, g), C)
-        _, first, _ = barrier_terms(J, problem.delta, problem.barrier_weight, problem.activation)
-        _scatter(g, C, _flux(A, first, None), out)
+    G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
+    for t in tiles(g):
+        if term in ("total", "jd", "curl"):
+            _, A, J, curl = geometry(local(u, g, t), G)
+            _, _, Jr, curlr = geometry(local(problem.u_ref, g, t), G)
+            jd = problem.mu * G.weights * (J - Jr) if term != "curl" else np.zeros_like(J)
+            cu = problem.nu * G.weights[None, :, None] * (curl - curlr) if term != "jd" else None
+            _scatter(g, G, _flux(A, jd, cu), out, t)
+        if term in ("total", "outer", "barrier"):
+            _, A, J, _ = geometry(local(u, g, t), C)
+            _, first, _ = barrier_terms(J, problem.delta, problem.barrier_weight, problem.activation)
+            _scatter(g, C, _flux(A, first, None), out, t)
     return restrict(out)
 
 
@@ -337,20 +359,21 @@ def ggn_diagonal(problem, u, image_grad):
     q = g.node_weights()
     out = np.moveaxis(q[..., None] * image_grad ** 2 + problem.lam * q[..., None], -1, 0).copy()
     G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
-    _, A, _, _ = geometry(local(u, g), G)
-    _, Ac, Jc, _ = geometry(local(u, g), C)
-    _, _, curv = barrier_terms(Jc, problem.delta, problem.barrier_weight, problem.activation)
-    nodes = cell_nodes(g)
     D, Dc = G.D, C.D
-    for r in range(3):
-        flat = out[r].ravel()
-        for a in range(8):
-            lj = sum(A[..., r, j] * D[j, :, a] for j in range(3))
-            lc = sum(Ac[..., r, j] * Dc[j, :, a] for j in range(3))
-            cs = sum(D[j, :, a] ** 2 for j in range(3) if j != r)
-            value = np.sum(G.weights * (problem.mu * lj ** 2 + problem.nu * cs), axis=-1)
-            value += np.sum(curv * lc ** 2, axis=-1)
-            np.add.at(flat, nodes[:, a], value)
+    for t in tiles(g):
+        _, A, _, _ = geometry(local(u, g, t), G)
+        _, Ac, Jc, _ = geometry(local(u, g, t), C)
+        _, _, curv = barrier_terms(Jc, problem.delta, problem.barrier_weight, problem.activation)
+        nodes = cell_nodes(g, t)
+        for r in range(3):
+            flat = out[r].ravel()
+            for a in range(8):
+                lj = sum(A[..., r, j] * D[j, :, a] for j in range(3))
+                lc = sum(Ac[..., r, j] * Dc[j, :, a] for j in range(3))
+                cs = sum(D[j, :, a] ** 2 for j in range(3) if j != r)
+                value = np.sum(G.weights * (problem.mu * lj ** 2 + problem.nu * cs), axis=-1)
+                value += np.sum(curv * lc ** 2, axis=-1)
+                flat += np.bincount(nodes[:, a], weights=value, minlength=flat.size)
     return restrict(out)
 
 
@@ -363,13 +386,13 @@ def ggn_hvp(problem, u, image_grad, p):
     out = np.moveaxis(node, -1, 0).copy()
     G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
     _, A, _, _ = geometry(local(u, g), G)
-    V = np.einsum("nar,jpa->nprj", local(v, g), G.D)
+    V = grad_points(local(v, g), G)
     jd = np.sum(A * V, axis=(-2, -1))
     curl = np.stack((V[..., 2, 1] - V[..., 1, 2], V[..., 0, 2] - V[..., 2, 0], V[..., 1, 0] - V[..., 0, 1]), -1)
     _scatter(g, G, _flux(A, problem.mu * G.weights * jd, problem.nu * G.weights[None, :, None] * curl), out)
     _, Ac, Jc, _ = geometry(local(u, g), C)
     _, _, curv = barrier_terms(Jc, problem.delta, problem.barrier_weight, problem.activation)
-    Vc = np.einsum("nar,jpa->nprj", local(v, g), C.D)
+    Vc = grad_points(local(v, g), C)
     lj = np.sum(Ac * Vc, axis=(-2, -1))
     _scatter(g, C, _flux(Ac, curv * lj, None), out)
     return restrict(out)
@@ -408,19 +431,20 @@ def differences(problem, base_u, base_w, trial_u, trial_w):
     prox = lambda u: np.sqrt(problem.lam * q)[..., None] * (u - problem.u_ref)
     image = _sq(img(base_w), img(trial_w))
     total = image + _sq(prox(base_u), prox(trial_u))
-    G = ops(g, "gauss27")
-    _, _, Jr, curlr = geometry(local(problem.u_ref, g), G)
-    blocks = []
-    for u in (base_u, trial_u):
-        _, _, J, curl = geometry(local(u, g), G)
-        blocks.append((np.sqrt(problem.mu * G.weights) * (J - Jr),
-                       np.sqrt(problem.nu * G.weights)[None, :, None] * (curl - curlr)))
-    total += _sq(blocks[0][0], blocks[1][0]) + _sq(blocks[0][1], blocks[1][1])
-    C = ops(g, "closed27_uniform")
-    Ja = geometry(local(base_u, g), C)[2]
-    Jb = geometry(local(trial_u, g), C)[2]
+    G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
     w = np.longdouble(problem.kappa) * np.longdouble(g.omega) / 27
-    bar = w * np.sum(barrier_difference(Ja, Jb, problem.delta, problem.activation), dtype=np.longdouble)
+    bar = np.longdouble(0)
+    for t in tiles(g):
+        _, _, Jr, curlr = geometry(local(problem.u_ref, g, t), G)
+        blocks = []
+        for u in (base_u, trial_u):
+            _, _, J, curl = geometry(local(u, g, t), G)
+            blocks.append((np.sqrt(problem.mu * G.weights) * (J - Jr),
+                           np.sqrt(problem.nu * G.weights)[None, :, None] * (curl - curlr)))
+        total += _sq(blocks[0][0], blocks[1][0]) + _sq(blocks[0][1], blocks[1][1])
+        Ja = geometry(local(base_u, g, t), C)[2]
+        Jb = geometry(local(trial_u, g, t), C)[2]
+        bar += w * np.sum(barrier_difference(Ja, Jb, problem.delta, problem.activation), dtype=np.longdouble)
     return total + bar, image + bar
 
 
@@ -551,7 +575,7 @@ def global_jd_root(problem, u, direction, limit):
     g = problem.grid
     C = ops(g, "closed27_uniform")
     F = geometry(local(u, g), C)[0]
-    V = np.einsum("nar,jpa->nprj", local(inject(direction, g), g), C.D)
+    V = grad_points(local(inject(direction, g), g), C)
     AF, AV = cofactor(F), cofactor(V)
     c0 = np.sum(F[..., 0, :] * AF[..., 0, :], -1) - problem.delta
     c1 = np.sum(AF * V, axis=(-2, -1))
