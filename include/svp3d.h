@@ -109,6 +109,20 @@ int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing
 int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi, int64_t n,
                        double delta, int64_t max_depth, int64_t max_boxes, svp_cell_verdict *out, void *stream);
 
+/* svp_classify_cells without any device allocation.  No counterpart in the reference (whose subdivision runs in
+ * Python on the host): it is for callers that cannot allocate device memory once they are running -- a host whose
+ * device memory is owned by another allocator (a framework's caching pool, a fixed budget set at start-up) or a
+ * latency-critical loop where an allocation's implicit synchronisation or pool growth is not acceptable.  The box
+ * heaps live in one file-scope device array of 4,317,184 bytes (32 cells in flight x 257 heap slots), which every
+ * device that loads the library keeps until process exit.  Limit: max_boxes <= 255 (larger is rejected with
+ * SVP_EINVAL); n is unbounded (cells are processed 32 at a time).  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (concurrent streams) race and must be serialised by the caller.  Results equal
+ * svp_classify_cells' bit for bit. */
+int svp_classify_cells_noalloc(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
+                               int64_t n, double delta, int64_t max_depth, int64_t max_boxes, svp_cell_verdict *out,
+                               void *stream);
+
 /* Whole-map certificate with owned workspace.  svp_certify_map replaces feasibility.py:393 certify_map and :558
  * certify_map_owned (PrescreenCertificateConfig execution) and synchronizes; out is a host struct. */
 typedef struct svp_certifier svp_certifier;

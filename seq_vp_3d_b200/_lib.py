@@ -59,6 +59,7 @@ SIGNATURES = {
     "svp_prescreen_lower_bounds": [P, P, P, I64, P, P],
     "svp_fallback_arrays": [P, I64, P, D, P, P, P, P, P, P, P],
     "svp_classify_cells": [P, P, P, P, I64, D, I64, I64, P, P],
+    "svp_classify_cells_noalloc": [P, P, P, P, I64, D, I64, I64, P, P],
     "svp_certifier_create": [P, P, P],
     "svp_certifier_destroy": [P],
     "svp_certify_map": [P, P, P, P],

@@ -14,6 +14,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "svp_common.cuh"
@@ -1073,5 +1074,62 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     }
     if (bad && acc.has_witness)
         for (int k = 0; k < 3; k++) out->witness_point[k] = acc.witness[k];
+    return SVP_OK;
+}
+
+// ---------------------------------------------------------------------------------------------- allocation-free
+// svp_classify_cells_noalloc: the subdivision of svp_classify_cells with its box heaps in a fixed, file-scope device
+// array instead of a stream-ordered allocation, for callers that may not allocate device memory after start-up.
+// Capacity: 32 warps (cells in flight) with max_boxes <= 255; each warp's region is rewritten from scratch for every
+// cell it takes, so nothing carries over between calls.  Every loaded device holds the array until process exit.
+namespace svp {
+namespace {
+constexpr long long kNoAllocWarps = 32;
+constexpr long long kNoAllocMaxBoxes = 255;
+constexpr size_t kNoAllocWarpBytes = ((size_t)(kNoAllocMaxBoxes + 2) * (54 * 8 + 8 * 8 + 8 + 4 + 4 + 4) + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes = (size_t)kNoAllocWarps * kNoAllocWarpBytes;  // 4,317,184 bytes
+
+static __device__ __align__(256) char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[256] = {};
+
+// Device address of the scratch array on the current device; the first call on a device looks it up.
+int noalloc_scratch(char **out) {
+    int dev = -1;
+    SVP_CUDA(cudaGetDevice(&dev));
+    SVP_REQUIRE(dev >= 0 && dev < 256, "svp_classify_cells_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(svp classify scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = (char *)g_noalloc_ptr[dev];
+    return SVP_OK;
+}
+}  // namespace
+}  // namespace svp
+
+extern "C" int svp_classify_cells_noalloc(const double *c_lo, const double *c_hi, const double *p_lo,
+                                          const double *p_hi, int64_t n, double delta, int64_t max_depth,
+                                          int64_t max_boxes, svp_cell_verdict *out, void *stream) {
+    using namespace svp;
+    SVP_REQUIRE(n >= 0 && max_depth >= 0 && max_boxes >= 1, "svp_classify_cells_noalloc: invalid arguments");
+    SVP_REQUIRE(max_boxes <= kNoAllocMaxBoxes,
+                "svp_classify_cells_noalloc: max_boxes above the static scratch limit of 255 boxes per cell");
+    if (n == 0) return SVP_OK;
+    SVP_REQUIRE(c_lo && c_hi && p_lo && p_hi && out, "svp_classify_cells_noalloc: null pointer");
+    char *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    const long long slots = max_boxes + 2;
+    long long warps = n < kNoAllocWarps ? n : kNoAllocWarps;
+    warps = (warps + 3) / 4 * 4;
+    SVP_REQUIRE(warp_scratch_bytes(slots) * (size_t)warps <= kNoAllocBytes,
+                "svp_classify_cells_noalloc: scratch capacity exceeded");
+    SVP_LAUNCH(classify_kernel<<<(unsigned)(warps * 32 / 128), 128, 0, (cudaStream_t)stream>>>(
+        c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, slots));
     return SVP_OK;
 }
