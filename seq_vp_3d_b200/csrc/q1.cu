@@ -176,16 +176,54 @@ __global__ void __launch_bounds__(256) sample_points_kernel(SplineRef S, const d
 }
 
 // ============================================================================================== cell energy
-__device__ __forceinline__ void gauss_tables(const double v[8][3], const Q1Const &q, double G[3][3][3][3]) {
-    double E[3][4][3];
-    cell_edges(v, E);
-    point_derivatives(E, q.gn, q.gm, q.ih, G);
+
+// Gauss27 sums of one cell, fully unrolled from the edges of u and u_ref (registers only, no tables)
+__device__ __forceinline__ void gauss_penalty_sums(const double E[3][4][3], const double Er[3][4][3], const Q1Const &q,
+                                                   double &sj, double &sc) {
+#pragma unroll 1
+    for (int p = 0; p < 27; p++) {
+        const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+        const double mx = q.gm[ix], nx = q.gn[ix], my = q.gm[iy], ny = q.gn[iy], mz = q.gm[iz], nz = q.gn[iz];
+        double X[3], Y[3], Z[3], Xr[3], Yr[3], Zr[3];
+        column<0>(E, my, ny, mz, nz, q.ih[0], X);
+        column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
+        column<2>(E, mx, nx, my, ny, q.ih[2], Z);
+        column<0>(Er, my, ny, mz, nz, q.ih[0], Xr);
+        column<1>(Er, mx, nx, mz, nz, q.ih[1], Yr);
+        column<2>(Er, mx, nx, my, ny, q.ih[2], Zr);
+        double V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
+        double Vr[3][3] = {{Xr[0], Yr[0], Zr[0]}, {Xr[1], Yr[1], Zr[1]}, {Xr[2], Yr[2], Zr[2]}};
+        double dj = det_only(V) - det_only(Vr);
+        double C[3], Cr[3];
+        curl_of(V, C);
+        curl_of(Vr, Cr);
+        double c0 = C[0] - Cr[0], c1 = C[1] - Cr[1], c2 = C[2] - Cr[2];
+        const double w = q.gw[p];
+        sj += w * dj * dj;
+        sc += w * (c0 * c0 + c1 * c1 + c2 * c2);
+    }
 }
-__device__ __forceinline__ void closed_tables(const double v[8][3], const Q1Const &q, double G[3][3][3][3]) {
-    const double n[3] = {0., .5, 1.}, m[3] = {1., .5, 0.};
-    double E[3][4][3];
-    cell_edges(v, E);
-    point_derivatives(E, n, m, q.ih, G);
+
+// closed27 localized barrier of one cell from the edges of u; violations (J <= delta) counted
+__device__ __forceinline__ void closed_barrier_sum(const double E[3][4][3], const Q1Const &q, double &sb,
+                                                   unsigned long long &nbad) {
+#pragma unroll 1
+    for (int p = 0; p < 27; p++) {
+        const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+        const double nx = .5 * ix, ny = .5 * iy, nz = .5 * iz, mx = 1. - nx, my = 1. - ny, mz = 1. - nz;
+        double X[3], Y[3], Z[3];
+        column<0>(E, my, ny, mz, nz, q.ih[0], X);
+        column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
+        column<2>(E, mx, nx, my, ny, q.ih[2], Z);
+        double V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
+        double J = det_only(V);
+        if (!(J > q.delta)) { nbad++; continue; }
+        if (J < q.act) {
+            double b, b1, b2;
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+            sb += b;
+        }
+    }
 }
 
 // partial[block][0..2] = sum w (J - Jr)^2, sum w |C - Cr|^2, sum barrier; violations counted in *bad
@@ -197,41 +235,17 @@ __global__ void __launch_bounds__(CT) cell_energy_kernel(Q1Const q, const double
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        double v[8][3], G[3][3][3][3], Gr[3][3][3][3];
-        load_cell(u, n0, q, v);
-        gauss_tables(v, q, G);
+        double E[3][4][3], Er[3][4][3];
         {
-            double vr[8][3];
-            load_cell(uref, n0, q, vr);
-            gauss_tables(vr, q, Gr);
+            double v[8][3];
+            load_cell(u, n0, q, v);
+            cell_edges(v, E);
+            load_cell(uref, n0, q, v);
+            cell_edges(v, Er);
         }
-        double sj = 0., sc = 0.;
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-            double V[3][3], Vr[3][3], C[3], Cr[3];
-            grad_at(G, ix, iy, iz, V);
-            grad_at(Gr, ix, iy, iz, Vr);
-            double dj = det_only(V) - det_only(Vr);
-            curl_of(V, C);
-            curl_of(Vr, Cr);
-            double c0 = C[0] - Cr[0], c1 = C[1] - Cr[1], c2 = C[2] - Cr[2];
-            sj += q.gw[p] * dj * dj;
-            sc += q.gw[p] * (c0 * c0 + c1 * c1 + c2 * c2);
-        }
-        double Gc[3][3][3][3];
-        closed_tables(v, q, Gc);
-        double sb = 0.;
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            double V[3][3];
-            grad_at(Gc, p % 3, (p / 3) % 3, p / 9, V);
-            double J = det_only(V);
-            if (!(J > q.delta)) { nbad++; continue; }
-            double b, b1, b2;
-            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-            sb += b;
-        }
+        double sj = 0., sc = 0., sb = 0.;
+        gauss_penalty_sums(E, Er, q, sj, sc);
+        closed_barrier_sum(E, q, sb, nbad);
         acc[0] = dd_add_d(acc[0], sj);
         acc[1] = dd_add_d(acc[1], sc);
         acc[2] = dd_add_d(acc[2], sb);
@@ -242,6 +256,84 @@ __global__ void __launch_bounds__(CT) cell_energy_kernel(Q1Const q, const double
 }
 
 // ============================================================================================== cell gradients
+// Kernels with 27-point tables keep them in a per-thread slice of dynamic shared memory (slice k at
+// smem[k * blockDim.x + threadIdx.x]: bank-conflict free); the edges of the fields stay in registers and the
+// point loops stay rolled, so no kernel touches local memory.
+constexpr int CS = 64;     // threads per block of the shared-memory cell kernels
+
+struct PointW {
+    double mx, nx, my, ny, mz, nz;
+};
+__device__ __forceinline__ PointW gauss_w(const Q1Const &q, int p) {
+    const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+    return {q.gm[ix], q.gn[ix], q.gm[iy], q.gn[iy], q.gm[iz], q.gn[iz]};
+}
+__device__ __forceinline__ PointW closed_w(int p) {
+    const double nx = .5 * (p % 3), ny = .5 * ((p / 3) % 3), nz = .5 * (p / 9);
+    return {1. - nx, nx, 1. - ny, ny, 1. - nz, nz};
+}
+__device__ __forceinline__ void grad_point(const double E[3][4][3], const PointW &w, const Q1Const &q, double V[3][3]) {
+    double X[3], Y[3], Z[3];
+    column<0>(E, w.my, w.ny, w.mz, w.nz, q.ih[0], X);
+    column<1>(E, w.mx, w.nx, w.mz, w.nz, q.ih[1], Y);
+    column<2>(E, w.mx, w.nx, w.my, w.ny, q.ih[2], Z);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        V[r][0] = X[r];
+        V[r][1] = Y[r];
+        V[r][2] = Z[r];
+    }
+}
+__device__ __forceinline__ void load_edges(const double *__restrict__ u, long long n0, const Q1Const &q,
+                                           double E[3][4][3]) {
+    double v[8][3];
+    load_cell(u, n0, q, v);
+    cell_edges(v, E);
+}
+__device__ __forceinline__ void zero_slice(double *sl, int T, int n) {
+    for (int k = 0; k < n; k++) sl[k * T] = 0.;
+}
+// S[j][s][t][r] += f[r][j] at point (ix, iy, iz): j = 0 -> (iy, iz), j = 1 -> (ix, iz), j = 2 -> (ix, iy)
+__device__ __forceinline__ void add_flux(double *sl, int T, int ix, int iy, int iz, const double f[3][3]) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        sl[((iy * 3 + iz) * 3 + r) * T] += f[r][0];
+        sl[(27 + (ix * 3 + iz) * 3 + r) * T] += f[r][1];
+        sl[(54 + (ix * 3 + iy) * 3 + r) * T] += f[r][2];
+    }
+}
+// adjoint of the edge interpolation (scatter_edges) reading S from the slice
+__device__ __forceinline__ void scatter_slice(const double *sl, int T, const double n[3], const double m[3],
+                                              const double ih[3], double L[8][3]) {
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double e[4] = {0., 0., 0., 0.};
+#pragma unroll
+            for (int s = 0; s < 3; s++) {
+                double t0 = 0., t1 = 0.;
+#pragma unroll
+                for (int t = 0; t < 3; t++) {
+                    double v = sl[(27 * j + (s * 3 + t) * 3 + r) * T] * ih[j];
+                    t0 += m[t] * v;
+                    t1 += n[t] * v;
+                }
+                e[0] += m[s] * t0;
+                e[1] += n[s] * t0;
+                e[2] += m[s] * t1;
+                e[3] += n[s] * t1;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                int lo = k & 1, hi = k >> 1;
+                int a = j == 0 ? 2 * lo + 4 * hi : (j == 1 ? lo + 4 * hi : lo + 2 * hi);
+                L[a | (1 << j)][r] += e[k];
+                L[a][r] -= e[k];
+            }
+        }
+}
+
 // Per-cell vertex values -> SoA locals L[(a * 3 + r) * ncell + c].
 __device__ __forceinline__ void store_locals(double *__restrict__ L, long long c, long long ncell,
                                              const double v[8][3]) {
@@ -251,110 +343,80 @@ __device__ __forceinline__ void store_locals(double *__restrict__ L, long long c
         for (int r = 0; r < 3; r++) L[(long long)(a * 3 + r) * ncell + c] = v[a][r];
 }
 
-// soft (JD + curl penalty) gradient of one cell into Ls; barrier gradient into Lb (zero if inactive)
-__device__ __forceinline__ void cell_soft_grad(const double v[8][3], const double vr[8][3], const Q1Const &q,
-                                               double Ls[8][3]) {
-    double G[3][3][3][3], Gr[3][3][3][3], S[3][3][3][3];
-    gauss_tables(v, q, G);
-    gauss_tables(vr, q, Gr);
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-#pragma unroll
-        for (int s = 0; s < 3; s++)
-#pragma unroll
-            for (int t = 0; t < 3; t++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
-#pragma unroll 1
-    for (int p = 0; p < 27; p++) {
-        int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-        double V[3][3], Vr[3][3], A[3][3], J, C[3], Cr[3];
-        grad_at(G, ix, iy, iz, V);
-        grad_at(Gr, ix, iy, iz, Vr);
-        cofactor_det(V, A, J);
-        double Jr = det_only(Vr);
-        curl_of(V, C);
-        curl_of(Vr, Cr);
-        double jd = q.mu * q.gw[p] * (J - Jr);
-        double k0 = q.nu * q.gw[p] * (C[0] - Cr[0]), k1 = q.nu * q.gw[p] * (C[1] - Cr[1]),
-               k2 = q.nu * q.gw[p] * (C[2] - Cr[2]);
-        double f[3][3];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * jd;
-        f[2][1] += k0; f[1][2] -= k0;
-        f[0][2] += k1; f[2][0] -= k1;
-        f[1][0] += k2; f[0][1] -= k2;
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            S[0][iy][iz][r] += f[r][0];
-            S[1][ix][iz][r] += f[r][1];
-            S[2][ix][iy][r] += f[r][2];
-        }
-    }
-    scatter_edges(S, q.gn, q.gm, q.ih, Ls);
-}
-
-__device__ __forceinline__ bool cell_barrier_grad(const double v[8][3], const Q1Const &q, double Lb[8][3]) {
-    const double n[3] = {0., .5, 1.}, m[3] = {1., .5, 0.};
-    double G[3][3][3][3];
-    closed_tables(v, q, G);
-    double S[3][3][3][3];
-    bool any = false;
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-#pragma unroll
-        for (int s = 0; s < 3; s++)
-#pragma unroll
-            for (int t = 0; t < 3; t++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
-#pragma unroll 1
-    for (int p = 0; p < 27; p++) {
-        int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-        double V[3][3], A[3][3], J;
-        grad_at(G, ix, iy, iz, V);
-        cofactor_det(V, A, J);
-        if (!(J < q.act)) continue;
-        double b, b1, b2;
-        barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-        any = true;
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            S[0][iy][iz][r] += A[r][0] * b1;
-            S[1][ix][iz][r] += A[r][1] * b1;
-            S[2][ix][iy][r] += A[r][2] * b1;
-        }
-    }
-    if (any) scatter_edges(S, n, m, q.ih, Lb);
-    return any;
-}
-
-// mode bit 0: soft penalties (jd, curl per the masks), bit 1: barrier.  Output layout:
-//   split = false: L1 = soft + barrier;  split = true: L1 = soft + barrier, L2 = barrier alone.
-__global__ void __launch_bounds__(CT) cell_grad_kernel(Q1Const q, const double *__restrict__ u,
+// L1 = soft (JD, curl penalties scaled by mu_scale, nu_scale) + barrier; with split, L2 = barrier alone.
+__global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *__restrict__ u,
                                                        const double *__restrict__ uref, double mu_scale,
                                                        double nu_scale, bool barrier, bool split,
                                                        double *__restrict__ L1, double *__restrict__ L2) {
-    Q1Const qq = q;
-    qq.mu = q.mu * mu_scale;
-    qq.nu = q.nu * nu_scale;
+    extern __shared__ double smem[];
+    double *sl = smem + threadIdx.x;
+    const int T = blockDim.x;
+    const double cn[3] = {0., .5, 1.}, cm[3] = {1., .5, 0.};
+    const double mu = q.mu * mu_scale, nu = q.nu * nu_scale;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        double v[8][3], L[8][3], Lb[8][3];
-        load_cell(u, n0, q, v);
+        double E[3][4][3], L[8][3];
+        load_edges(u, n0, q, E);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) { L[a][r] = 0.; Lb[a][r] = 0.; }
-        if (qq.mu != 0. || qq.nu != 0.) {
-            double vr[8][3];
-            load_cell(uref, n0, q, vr);
-            cell_soft_grad(v, vr, qq, L);
+            for (int r = 0; r < 3; r++) L[a][r] = 0.;
+        if (mu != 0. || nu != 0.) {
+            double Er[3][4][3];
+            load_edges(uref, n0, q, Er);
+            zero_slice(sl, T, 81);
+#pragma unroll 1
+            for (int p = 0; p < 27; p++) {
+                const PointW w = gauss_w(q, p);
+                double V[3][3], Vr[3][3], A[3][3], J, C[3], Cr[3];
+                grad_point(E, w, q, V);
+                grad_point(Er, w, q, Vr);
+                cofactor_det(V, A, J);
+                double Jr = det_only(Vr);
+                curl_of(V, C);
+                curl_of(Vr, Cr);
+                const double gw = q.gw[p];
+                double jd = mu * gw * (J - Jr);
+                double k0 = nu * gw * (C[0] - Cr[0]), k1 = nu * gw * (C[1] - Cr[1]), k2 = nu * gw * (C[2] - Cr[2]);
+                double f[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * jd;
+                f[2][1] += k0; f[1][2] -= k0;
+                f[0][2] += k1; f[2][0] -= k1;
+                f[1][0] += k2; f[0][1] -= k2;
+                add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
+            }
+            scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
         }
-        if (barrier) cell_barrier_grad(v, q, Lb);
+        bool any = false;
+        if (barrier) {
+            zero_slice(sl, T, 81);
+#pragma unroll 1
+            for (int p = 0; p < 27; p++) {
+                double V[3][3];
+                grad_point(E, closed_w(p), q, V);
+                if (!(det_only(V) < q.act)) continue;
+                double A[3][3], J, b, b1, b2;
+                cofactor_det(V, A, J);
+                barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+                double f[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * b1;
+                add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
+                any = true;
+            }
+        }
+        double Lb[8][3];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) Lb[a][r] = 0.;
+        if (any) scatter_slice(sl, T, cn, cm, q.ih, Lb);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
@@ -398,43 +460,45 @@ __global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, co
         for (int r = 0; r < 3; r++) {
             double img = image_grad ? dimg * image_grad[3 * node + r] : 0.;
             double prox = uref ? q.lam * qw * (u[3 * node + r] - uref[3 * node + r]) : 0.;
-            for (int k = 0; k < g.nout; k++)
-                g.out[k][r * q.nfree + i] = ((g.ci[k] * img + g.cp[k] * prox) + g.c1[k] * s1[r]) + g.c2[k] * s2[r];
+#pragma unroll
+            for (int k = 0; k < 3; k++)     // constant indices keep the spec in the parameter bank
+                if (k < g.nout)
+                    g.out[k][r * q.nfree + i] = ((g.ci[k] * img + g.cp[k] * prox) + g.c1[k] * s1[r]) + g.c2[k] * s2[r];
         }
     }
 }
 
 // ============================================================================================== GGN
 // Per-cell diagonal contributions: sum_p w (mu lj^2 + nu cs) + sum_closed27 b'' lc^2, lj = sum_j A_rj D_jpa.
+__device__ __forceinline__ void point_D(const PointW &w, int a, const double ih[3], double D[3]) {
+    const int bx = a & 1, by = (a >> 1) & 1, bz = (a >> 2) & 1;
+    const double fx = bx ? w.nx : w.mx, fy = by ? w.ny : w.my, fz = bz ? w.nz : w.mz;
+    D[0] = (bx ? ih[0] : -ih[0]) * fy * fz;
+    D[1] = (by ? ih[1] : -ih[1]) * fx * fz;
+    D[2] = (bz ? ih[2] : -ih[2]) * fx * fy;
+}
+
 __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const double *__restrict__ u,
                                                            double *__restrict__ L) {
-    const double cn[3] = {0., .5, 1.}, cm[3] = {1., .5, 0.};
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
-        long long n0 = cell_node0(c, q);
-        double v[8][3], G[3][3][3][3], out[8][3];
-        load_cell(u, n0, q, v);
-        gauss_tables(v, q, G);
+        double E[3][4][3], out[8][3];
+        load_edges(u, cell_node0(c, q), q, E);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] = 0.;
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            const PointW w = gauss_w(q, p);
             double V[3][3], A[3][3], J;
-            grad_at(G, ix, iy, iz, V);
+            grad_point(E, w, q, V);
             cofactor_det(V, A, J);
-            int id[3] = {ix, iy, iz};
+            const double gw = q.gw[p];
 #pragma unroll
             for (int a = 0; a < 8; a++) {
-                int bits[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
-                double f[3], D[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) f[k] = bits[k] ? q.gn[id[k]] : q.gm[id[k]];
-                D[0] = (bits[0] ? q.ih[0] : -q.ih[0]) * f[1] * f[2];
-                D[1] = (bits[1] ? q.ih[1] : -q.ih[1]) * f[0] * f[2];
-                D[2] = (bits[2] ? q.ih[2] : -q.ih[2]) * f[0] * f[1];
+                double D[3];
+                point_D(w, a, q.ih, D);
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
@@ -442,31 +506,23 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
 #pragma unroll
                     for (int j = 0; j < 3; j++)
                         if (j != r) cs += D[j] * D[j];
-                    out[a][r] += q.gw[p] * (q.mu * lj * lj + q.nu * cs);
+                    out[a][r] += gw * (q.mu * lj * lj + q.nu * cs);
                 }
             }
         }
-        double Gc[3][3][3][3];
-        closed_tables(v, q, Gc);
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-            double V[3][3], A[3][3], J;
-            grad_at(Gc, ix, iy, iz, V);
+            const PointW w = closed_w(p);
+            double V[3][3];
+            grad_point(E, w, q, V);
+            if (!(det_only(V) < q.act)) continue;
+            double A[3][3], J, b, b1, b2;
             cofactor_det(V, A, J);
-            if (!(J < q.act)) continue;
-            double b, b1, b2;
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-            int id[3] = {ix, iy, iz};
 #pragma unroll
             for (int a = 0; a < 8; a++) {
-                int bits[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
-                double f[3], D[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) f[k] = bits[k] ? cn[id[k]] : cm[id[k]];
-                D[0] = (bits[0] ? q.ih[0] : -q.ih[0]) * f[1] * f[2];
-                D[1] = (bits[1] ? q.ih[1] : -q.ih[1]) * f[0] * f[2];
-                D[2] = (bits[2] ? q.ih[2] : -q.ih[2]) * f[0] * f[1];
+                double D[3];
+                point_D(w, a, q.ih, D);
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lc = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
@@ -479,35 +535,29 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
 }
 
 // GGN action on a node field vv (zero faces): Gauss JD/curl linearization + closed27 barrier curvature.
-__global__ void __launch_bounds__(CT) cell_ggn_hvp_kernel(Q1Const q, const double *__restrict__ u,
+__global__ void __launch_bounds__(CS) cell_ggn_hvp_kernel(Q1Const q, const double *__restrict__ u,
                                                           const double *__restrict__ vv, double *__restrict__ L) {
+    extern __shared__ double smem[];
+    double *sl = smem + threadIdx.x;
+    const int T = blockDim.x;
     const double cn[3] = {0., .5, 1.}, cm[3] = {1., .5, 0.};
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        double v[8][3], w[8][3], G[3][3][3][3], Gv[3][3][3][3], S[3][3][3][3], out[8][3];
-        load_cell(u, n0, q, v);
-        load_cell(vv, n0, q, w);
-        gauss_tables(v, q, G);
-        gauss_tables(w, q, Gv);
+        double E[3][4][3], Ev[3][4][3], out[8][3];
+        load_edges(u, n0, q, E);
+        load_edges(vv, n0, q, Ev);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] = 0.;
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-#pragma unroll
-            for (int s = 0; s < 3; s++)
-#pragma unroll
-                for (int t = 0; t < 3; t++)
-#pragma unroll
-                    for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+        zero_slice(sl, T, 81);
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            const PointW w = gauss_w(q, p);
             double V[3][3], W[3][3], A[3][3], J, K[3];
-            grad_at(G, ix, iy, iz, V);
-            grad_at(Gv, ix, iy, iz, W);
+            grad_point(E, w, q, V);
+            grad_point(Ev, w, q, W);
             cofactor_det(V, A, J);
             double jd = 0.;
 #pragma unroll
@@ -515,8 +565,9 @@ __global__ void __launch_bounds__(CT) cell_ggn_hvp_kernel(Q1Const q, const doubl
 #pragma unroll
                 for (int jj = 0; jj < 3; jj++) jd += A[r][jj] * W[r][jj];
             curl_of(W, K);
-            jd *= q.mu * q.gw[p];
-            double k0 = q.nu * q.gw[p] * K[0], k1 = q.nu * q.gw[p] * K[1], k2 = q.nu * q.gw[p] * K[2];
+            const double gw = q.gw[p];
+            jd *= q.mu * gw;
+            double k0 = q.nu * gw * K[0], k1 = q.nu * gw * K[1], k2 = q.nu * gw * K[2];
             double f[3][3];
 #pragma unroll
             for (int r = 0; r < 3; r++)
@@ -525,35 +576,20 @@ __global__ void __launch_bounds__(CT) cell_ggn_hvp_kernel(Q1Const q, const doubl
             f[2][1] += k0; f[1][2] -= k0;
             f[0][2] += k1; f[2][0] -= k1;
             f[1][0] += k2; f[0][1] -= k2;
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                S[0][iy][iz][r] += f[r][0];
-                S[1][ix][iz][r] += f[r][1];
-                S[2][ix][iy][r] += f[r][2];
-            }
+            add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
         }
-        scatter_edges(S, q.gn, q.gm, q.ih, out);
-        double Gc[3][3][3][3], Gcv[3][3][3][3];
-        closed_tables(v, q, Gc);
-        closed_tables(w, q, Gcv);
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-#pragma unroll
-            for (int s = 0; s < 3; s++)
-#pragma unroll
-                for (int t = 0; t < 3; t++)
-#pragma unroll
-                    for (int r = 0; r < 3; r++) S[j][s][t][r] = 0.;
+        scatter_slice(sl, T, q.gn, q.gm, q.ih, out);
+        zero_slice(sl, T, 81);
         bool any = false;
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-            double V[3][3], W[3][3], A[3][3], J;
-            grad_at(Gc, ix, iy, iz, V);
+            const PointW w = closed_w(p);
+            double V[3][3];
+            grad_point(E, w, q, V);
+            if (!(det_only(V) < q.act)) continue;
+            double W[3][3], A[3][3], J, b, b1, b2;
             cofactor_det(V, A, J);
-            if (!(J < q.act)) continue;
-            grad_at(Gcv, ix, iy, iz, W);
-            double b, b1, b2;
+            grad_point(Ev, w, q, W);
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
             double lj = 0.;
 #pragma unroll
@@ -561,15 +597,15 @@ __global__ void __launch_bounds__(CT) cell_ggn_hvp_kernel(Q1Const q, const doubl
 #pragma unroll
                 for (int jj = 0; jj < 3; jj++) lj += A[r][jj] * W[r][jj];
             lj *= b2;
-            any = true;
+            double f[3][3];
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-                S[0][iy][iz][r] += A[r][0] * lj;
-                S[1][ix][iz][r] += A[r][1] * lj;
-                S[2][ix][iy][r] += A[r][2] * lj;
-            }
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * lj;
+            add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
+            any = true;
         }
-        if (any) scatter_edges(S, cn, cm, q.ih, out);
+        if (any) scatter_slice(sl, T, cn, cm, q.ih, out);
         store_locals(L, c, q.ncell, out);
     }
 }
@@ -645,46 +681,59 @@ __global__ void __launch_bounds__(256) node_diff_kernel(Q1Const q, const double 
     block_reduce_dd<2>(acc, partial);
 }
 
-__global__ void __launch_bounds__(CT) cell_diff_kernel(Q1Const q, const double *__restrict__ ua,
+// Reference J and curl at the Gauss points go to the thread's shared slice first (108 values), so only the two
+// compared fields' edges are live in registers during the main pass.
+__global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *__restrict__ ua,
                                                        const double *__restrict__ ub,
                                                        const double *__restrict__ uref, dd *partial) {
+    extern __shared__ double smem[];
+    double *sl = smem + threadIdx.x;
+    const int T = blockDim.x;
     dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        double va[8][3], vb[8][3], vr[8][3];
-        double Ga[3][3][3][3], Gb[3][3][3][3], Gr[3][3][3][3];
-        load_cell(ua, n0, q, va);
-        load_cell(ub, n0, q, vb);
-        load_cell(uref, n0, q, vr);
-        gauss_tables(va, q, Ga);
-        gauss_tables(vb, q, Gb);
-        gauss_tables(vr, q, Gr);
+        {
+            double Er[3][4][3];
+            load_edges(uref, n0, q, Er);
+#pragma unroll 1
+            for (int p = 0; p < 27; p++) {
+                double Vr[3][3], Cr[3];
+                grad_point(Er, gauss_w(q, p), q, Vr);
+                curl_of(Vr, Cr);
+                sl[(4 * p) * T] = det_only(Vr);
+                sl[(4 * p + 1) * T] = Cr[0];
+                sl[(4 * p + 2) * T] = Cr[1];
+                sl[(4 * p + 3) * T] = Cr[2];
+            }
+        }
+        double Ea[3][4][3], Eb[3][4][3];
+        load_edges(ua, n0, q, Ea);
+        load_edges(ub, n0, q, Eb);
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-            double Va[3][3], Vb[3][3], Vr[3][3], Ca[3], Cb[3], Cr[3];
-            grad_at(Ga, ix, iy, iz, Va);
-            grad_at(Gb, ix, iy, iz, Vb);
-            grad_at(Gr, ix, iy, iz, Vr);
-            double jr = det_only(Vr);
-            double smu = sqrt(q.mu * q.gw[p]), snu = sqrt(q.nu * q.gw[p]);
+            const PointW w = gauss_w(q, p);
+            double Va[3][3], Vb[3][3], Ca[3], Cb[3];
+            grad_point(Ea, w, q, Va);
+            grad_point(Eb, w, q, Vb);
+            const double jr = sl[(4 * p) * T];
+            const double smu = sqrt(q.mu * q.gw[p]), snu = sqrt(q.nu * q.gw[p]);
             acc[0] = dd_add(acc[0], sq_change(smu * (det_only(Va) - jr), smu * (det_only(Vb) - jr)));
             curl_of(Va, Ca);
             curl_of(Vb, Cb);
-            curl_of(Vr, Cr);
 #pragma unroll
-            for (int r = 0; r < 3; r++) acc[1] = dd_add(acc[1], sq_change(snu * (Ca[r] - Cr[r]), snu * (Cb[r] - Cr[r])));
+            for (int r = 0; r < 3; r++) {
+                const double cr = sl[(4 * p + 1 + r) * T];
+                acc[1] = dd_add(acc[1], sq_change(snu * (Ca[r] - cr), snu * (Cb[r] - cr)));
+            }
         }
-        closed_tables(va, q, Ga);
-        closed_tables(vb, q, Gb);
         double sb = 0.;
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            const PointW w = closed_w(p);
             double Va[3][3], Vb[3][3];
-            grad_at(Ga, ix, iy, iz, Va);
-            grad_at(Gb, ix, iy, iz, Vb);
+            grad_point(Ea, w, q, Va);
+            grad_point(Eb, w, q, Vb);
             double ja = det_only(Va), jb = det_only(Vb);
             if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
         }
@@ -694,38 +743,41 @@ __global__ void __launch_bounds__(CT) cell_diff_kernel(Q1Const q, const double *
 }
 
 // ============================================================================================== node JD measure
-__global__ void __launch_bounds__(CT) cell_min_jd_kernel(Q1Const q, const double *__restrict__ u,
+__global__ void __launch_bounds__(CS) cell_min_jd_kernel(Q1Const q, const double *__restrict__ u,
                                                          double *__restrict__ m) {
+    extern __shared__ double smem[];
+    double *J = smem + threadIdx.x;
+    const int T = blockDim.x;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
-        double v[8][3], G[3][3][3][3], J[27];
-        load_cell(u, cell_node0(c, q), q, v);
-        closed_tables(v, q, G);
+        double E[3][4][3];
+        load_edges(u, cell_node0(c, q), q, E);
         double mn = __longlong_as_double(0x7FF0000000000000LL);
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
             double V[3][3];
-            grad_at(G, p % 3, (p / 3) % 3, p / 9, V);
-            J[p] = det_only(V);
-            mn = fmin(mn, J[p]);
+            grad_point(E, closed_w(p), q, V);
+            double j = det_only(V);
+            J[p * T] = j;
+            mn = fmin(mn, j);
         }
         // exact interior minima of the edge quadratics through t = 0, 1/2, 1 (solvers/jd_affine.py:24)
 #pragma unroll 1
         for (int e = 0; e < 12; e++) {
-            int f0, f1, f2;
+            int f0, st;
             if (e < 4) {            // x edges: iz, iy in {0, 2}
-                int iz = (e >> 1) * 2, iy = (e & 1) * 2;
-                f0 = 9 * iz + 3 * iy; f1 = f0 + 1; f2 = f0 + 2;
+                f0 = 9 * ((e >> 1) * 2) + 3 * ((e & 1) * 2); st = 1;
             } else if (e < 8) {     // y edges: iz, ix in {0, 2}
-                int k = e - 4, iz = (k >> 1) * 2, ix = (k & 1) * 2;
-                f0 = 9 * iz + ix; f1 = f0 + 3; f2 = f0 + 6;
+                int k = e - 4;
+                f0 = 9 * ((k >> 1) * 2) + (k & 1) * 2; st = 3;
             } else {                // z edges: iy, ix in {0, 2}
-                int k = e - 8, iy = (k >> 1) * 2, ix = (k & 1) * 2;
-                f0 = 3 * iy + ix; f1 = f0 + 9; f2 = f0 + 18;
+                int k = e - 8;
+                f0 = 3 * ((k >> 1) * 2) + (k & 1) * 2; st = 9;
             }
-            double a = 2 * (J[f0] - 2 * J[f1] + J[f2]);
-            double b = -3 * J[f0] + 4 * J[f1] - J[f2];
-            if (a > 0 && b < 0 && -b < 2 * a) mn = fmin(mn, J[f0] - b * b / (4 * a));
+            double j0 = J[f0 * T], j1 = J[(f0 + st) * T], j2 = J[(f0 + 2 * st) * T];
+            double a = 2 * (j0 - 2 * j1 + j2);
+            double b = -3 * j0 + 4 * j1 - j2;
+            if (a > 0 && b < 0 && -b < 2 * a) mn = fmin(mn, j0 - b * b / (4 * a));
         }
         m[c] = mn;
     }
@@ -791,19 +843,16 @@ __global__ void __launch_bounds__(CT) jd_root_kernel(Q1Const q, const double *__
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        double v[8][3], w[8][3], G[3][3][3][3], Gp[3][3][3][3];
-        load_cell(u, n0, q, v);
-        load_cell(pv, n0, q, w);
-        closed_tables(v, q, G);
-        closed_tables(w, q, Gp);
+        double E[3][4][3], Ep[3][4][3];
+        load_edges(u, n0, q, E);
+        load_edges(pv, n0, q, Ep);
 #pragma unroll 1
         for (int p = 0; p < 27; p++) {
-            int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
+            const PointW w = closed_w(p);
             double V[3][3], W[3][3], AF[3][3], AV[3][3], J, JV;
-            grad_at(G, ix, iy, iz, V);
-            grad_at(Gp, ix, iy, iz, W);
+            grad_point(E, w, q, V);
+            grad_point(Ep, w, q, W);
             cofactor_det(V, AF, J);
-            // cofactor of V alone (no identity)
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 int j = (r + 1) % 3, k = (r + 2) % 3;
@@ -906,6 +955,15 @@ SplineRef spline_ref(const svp_pair *p) {
 }
 
 unsigned cell_blocks(const svp_pair *p) { return blocks_for(p->q.ncell, CT, CELL_PER_SM); }
+unsigned slice_blocks(const svp_pair *p) { return blocks_for(p->q.ncell, CS, 2 * CELL_PER_SM); }
+// dynamic shared memory of the slice kernels: k doubles per thread
+constexpr size_t slice_bytes(int k) { return sizeof(double) * (size_t)k * CS; }
+int allow_slices() {
+    // cell_diff_kernel's slice is above the 48 KB default; the attribute is per device context, so set it per call
+    SVP_CUDA(cudaFuncSetAttribute(cell_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)slice_bytes(108)));
+    return SVP_OK;
+}
 unsigned node_blocks(long long n) { return blocks_for(n, 256, 8); }
 
 }  // namespace
@@ -994,13 +1052,15 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
                                      void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && diff2, "svp_energy_difference: null");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned nb = node_blocks(p->q.nnode), cb = cell_blocks(p);
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
     int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
+    if (rc) return rc;
+    rc = allow_slices();
     if (rc) return rc;
     { svp::KernelTimer _t("node_diff_kernel", s); SVP_LAUNCH(node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
                                         p->partial)); }
     dd *pc = p->partial + (long long)nb * 2;
-    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CT, 0, s>>>(p->q, base_u, trial_u, p->u_ref, pc)); }
+    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pc)); }
     SVP_LAUNCH_CHECK("difference kernels");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4));
@@ -1034,7 +1094,7 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
     if (cellwork) {
         int rc = pair_locals(p, 1);
         if (rc) return rc;
-        { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
+        { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
                                                        (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr)); }
         SVP_LAUNCH_CHECK("cell_grad_kernel");
@@ -1055,7 +1115,7 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 2);
     if (rc) return rc;
-    { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
+    { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
     GatherSpec g{};
     g.nout = 3;
@@ -1088,7 +1148,7 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
     double *vv = p->loc2;
     rc = svp_inject(&p->grid, pvec, vv, stream);
     if (rc) return rc;
-    { svp::KernelTimer _t("cell_ggn_hvp_kernel", s); SVP_LAUNCH(cell_ggn_hvp_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, vv, p->loc1)); }
+    { svp::KernelTimer _t("cell_ggn_hvp_kernel", s); SVP_LAUNCH(cell_ggn_hvp_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, vv, p->loc1)); }
     SVP_LAUNCH(ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out));
     SVP_LAUNCH_CHECK("ggn hvp");
     return SVP_OK;
@@ -1097,7 +1157,7 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
 extern "C" int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream) {
     SVP_REQUIRE(p && u && node, "svp_node_min_jd: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    { svp::KernelTimer _t("cell_min_jd_kernel", s); SVP_LAUNCH(cell_min_jd_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->cellbuf)); }
+    { svp::KernelTimer _t("cell_min_jd_kernel", s); SVP_LAUNCH(cell_min_jd_kernel<<<slice_blocks(p), CS, slice_bytes(27), s>>>(p->q, u, p->cellbuf)); }
     SVP_LAUNCH(node_min_kernel<<<node_blocks(p->q.nnode), 256, 0, s>>>(p->q, p->cellbuf, node));
     SVP_LAUNCH_CHECK("node_min_jd");
     return SVP_OK;

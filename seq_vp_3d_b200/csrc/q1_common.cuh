@@ -131,6 +131,18 @@ __device__ __forceinline__ void point_derivatives(const T E[3][4][3], const T n[
             }
 }
 
+// Column j of grad u at one point, straight from the edges (the same operation sequence as point_derivatives, so
+// the values are bitwise those of the tables): s indexes the lower-numbered other axis, t the higher.
+template <int J, class T>
+__device__ __forceinline__ void column(const T E[3][4][3], T ms, T ns, T mt, T nt, T ih, T out[3]) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        T l0 = ms * E[J][0][r] + ns * E[J][1][r];
+        T l1 = ms * E[J][2][r] + ns * E[J][3][r];
+        out[r] = (mt * l0 + nt * l1) * ih;
+    }
+}
+
 // V[r][j] at point (ix, iy, iz) from the tables
 template <class T>
 __device__ __forceinline__ void grad_at(const T G[3][3][3][3], int ix, int iy, int iz, T V[3][3]) {
