@@ -171,6 +171,16 @@ int svp_energy(svp_pair *p, const double *u, const double *warped, double *terms
 int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
                           const double *trial_warped, double *diff2, void *stream);
 
+/* A line-search trial against its base in one node pass and one cell pass (one synchronisation): warps
+ * trial_u into trial_warped (and trial_image_grad when not NULL, the gradient promotion needs), and returns the
+ * trial's terms5 and barrier_violations exactly as svp_energy and diff2 = trial - base exactly as
+ * svp_energy_difference (bitwise: same sums in the same order).  Replaces the evaluate_trial -> _energy ->
+ * stable_energy_reductions sequence of the reference's line search (solvers/poisson_gradient.py:1245-1290;
+ * backends/accelerated.py:1667 evaluate_trial, :3062 _compare).  The caller certifies trial_u first. */
+int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                     double *trial_warped, double *trial_image_grad, double *terms5, double *diff2,
+                     int64_t *barrier_violations, void *stream);
+
 /* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
 #define SVP_TERM_IMAGE 1
 #define SVP_TERM_PROXIMITY 2

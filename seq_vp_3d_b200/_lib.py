@@ -71,6 +71,7 @@ SIGNATURES = {
     "svp_sample_points": [P, P, I64, P, P, P],
     "svp_energy": [P, P, P, P, P, P],
     "svp_energy_difference": [P, P, P, P, P, P, P],
+    "svp_trial_energy": [P, P, P, P, P, P, P, P, P, P],
     "svp_gradient": [P, P, P, P, I32, P, P],
     "svp_outer_gradients": [P, P, P, P, P, P, P, P],
     "svp_ggn_diagonal": [P, P, P, P, P],

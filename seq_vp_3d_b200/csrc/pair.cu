@@ -101,6 +101,10 @@ Q1Const make_const(const svp_grid *g, const svp_weights *w) {
     q.omega = (g->hx * g->hy) * g->hz;
     for (int p = 0; p < 27; p++) q.gw[p] = ((q.omega * w1[p % 3]) * w1[(p / 3) % 3]) * w1[p / 9];
     q.lam = w->lam; q.mu = w->mu; q.nu = w->nu;
+    for (int p = 0; p < 27; p++) {       // IEEE square roots: the values the device's sqrt gives
+        q.sqmu[p] = std::sqrt(q.mu * q.gw[p]);
+        q.sqnu[p] = std::sqrt(q.nu * q.gw[p]);
+    }
     q.bw = w->kappa * q.omega / 27;
     q.act = w->activation;
     q.delta = w->delta;
@@ -115,7 +119,7 @@ using namespace svp;
 extern "C" int svp_pair_destroy(svp_pair *p) {
     if (!p) return SVP_OK;
     cudaFree(p->fixed); cudaFree(p->coeff); cudaFree(p->u_ref);
-    for (int k = 0; k < 3; k++) { cudaFree(p->knots[k]); cudaFree(p->dst_mat[k]); }
+    for (int k = 0; k < 3; k++) { cudaFree(p->knots[k]); cudaFree(p->dst_half[k]); }
     cudaFree(p->loc1); cudaFree(p->loc2); cudaFree(p->cellbuf); cudaFree(p->partial); cudaFree(p->result);
     cudaFree(p->counter); cudaFree(p->dst_tmp); cudaFree(p->den);
     delete p;

@@ -20,7 +20,8 @@ struct svp_pair {
     double *result = nullptr;                 // small device result area (64 doubles)
     long long *counter = nullptr;             // small device counters (8)
     // DST-I Poisson metric
-    double *dst_mat[3] = {nullptr, nullptr, nullptr};  // orthonormal sine matrices (n-2)^2, x, y, z
+    double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
+    int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)
     double *dst_tmp = nullptr;                          // 2 * 3 * nfree scratch
     double *den = nullptr;                              // (nz-2, ny-2, nx-2) omega (a + b lambda)
     double den_a = -1, den_b = -1;

@@ -175,115 +175,12 @@ __global__ void __launch_bounds__(256) sample_points_kernel(SplineRef S, const d
     }
 }
 
-// ============================================================================================== cell energy
-
-// Gauss27 sums of one cell, fully unrolled from the edges of u and u_ref (registers only, no tables)
-__device__ __forceinline__ void gauss_penalty_sums(const double E[3][4][3], const double Er[3][4][3], const Q1Const &q,
-                                                   double &sj, double &sc) {
-#pragma unroll 1
-    for (int p = 0; p < 27; p++) {
-        const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-        const double mx = q.gm[ix], nx = q.gn[ix], my = q.gm[iy], ny = q.gn[iy], mz = q.gm[iz], nz = q.gn[iz];
-        double X[3], Y[3], Z[3], Xr[3], Yr[3], Zr[3];
-        column<0>(E, my, ny, mz, nz, q.ih[0], X);
-        column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
-        column<2>(E, mx, nx, my, ny, q.ih[2], Z);
-        column<0>(Er, my, ny, mz, nz, q.ih[0], Xr);
-        column<1>(Er, mx, nx, mz, nz, q.ih[1], Yr);
-        column<2>(Er, mx, nx, my, ny, q.ih[2], Zr);
-        double V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
-        double Vr[3][3] = {{Xr[0], Yr[0], Zr[0]}, {Xr[1], Yr[1], Zr[1]}, {Xr[2], Yr[2], Zr[2]}};
-        double dj = det_only(V) - det_only(Vr);
-        double C[3], Cr[3];
-        curl_of(V, C);
-        curl_of(Vr, Cr);
-        double c0 = C[0] - Cr[0], c1 = C[1] - Cr[1], c2 = C[2] - Cr[2];
-        const double w = q.gw[p];
-        sj += w * dj * dj;
-        sc += w * (c0 * c0 + c1 * c1 + c2 * c2);
-    }
-}
-
-// closed27 localized barrier of one cell from the edges of u; violations (J <= delta) counted
-__device__ __forceinline__ void closed_barrier_sum(const double E[3][4][3], const Q1Const &q, double &sb,
-                                                   unsigned long long &nbad) {
-#pragma unroll 1
-    for (int p = 0; p < 27; p++) {
-        const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-        const double nx = .5 * ix, ny = .5 * iy, nz = .5 * iz, mx = 1. - nx, my = 1. - ny, mz = 1. - nz;
-        double X[3], Y[3], Z[3];
-        column<0>(E, my, ny, mz, nz, q.ih[0], X);
-        column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
-        column<2>(E, mx, nx, my, ny, q.ih[2], Z);
-        double V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
-        double J = det_only(V);
-        if (!(J > q.delta)) { nbad++; continue; }
-        if (J < q.act) {
-            double b, b1, b2;
-            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-            sb += b;
-        }
-    }
-}
-
-// partial[block][0..2] = sum w (J - Jr)^2, sum w |C - Cr|^2, sum barrier; violations counted in *bad
-__global__ void __launch_bounds__(CT) cell_energy_kernel(Q1Const q, const double *__restrict__ u,
-                                                         const double *__restrict__ uref, dd *partial,
-                                                         unsigned long long *bad) {
-    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
-    unsigned long long nbad = 0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
-         c += (long long)gridDim.x * blockDim.x) {
-        long long n0 = cell_node0(c, q);
-        double E[3][4][3], Er[3][4][3];
-        {
-            double v[8][3];
-            load_cell(u, n0, q, v);
-            cell_edges(v, E);
-            load_cell(uref, n0, q, v);
-            cell_edges(v, Er);
-        }
-        double sj = 0., sc = 0., sb = 0.;
-        gauss_penalty_sums(E, Er, q, sj, sc);
-        closed_barrier_sum(E, q, sb, nbad);
-        acc[0] = dd_add_d(acc[0], sj);
-        acc[1] = dd_add_d(acc[1], sc);
-        acc[2] = dd_add_d(acc[2], sb);
-    }
-    block_reduce_dd<3>(acc, partial);
-    for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
-    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
-}
-
-// ============================================================================================== cell gradients
+// ============================================================================================== cell helpers
 // Kernels with 27-point tables keep them in a per-thread slice of dynamic shared memory (slice k at
 // smem[k * blockDim.x + threadIdx.x]: bank-conflict free); the edges of the fields stay in registers and the
 // point loops stay rolled, so no kernel touches local memory.
 constexpr int CS = 64;     // threads per block of the shared-memory cell kernels
 
-struct PointW {
-    double mx, nx, my, ny, mz, nz;
-};
-__device__ __forceinline__ PointW gauss_w(const Q1Const &q, int p) {
-    const int ix = p % 3, iy = (p / 3) % 3, iz = p / 9;
-    return {q.gm[ix], q.gn[ix], q.gm[iy], q.gn[iy], q.gm[iz], q.gn[iz]};
-}
-__device__ __forceinline__ PointW closed_w(int p) {
-    const double nx = .5 * (p % 3), ny = .5 * ((p / 3) % 3), nz = .5 * (p / 9);
-    return {1. - nx, nx, 1. - ny, ny, 1. - nz, nz};
-}
-__device__ __forceinline__ void grad_point(const double E[3][4][3], const PointW &w, const Q1Const &q, double V[3][3]) {
-    double X[3], Y[3], Z[3];
-    column<0>(E, w.my, w.ny, w.mz, w.nz, q.ih[0], X);
-    column<1>(E, w.mx, w.nx, w.mz, w.nz, q.ih[1], Y);
-    column<2>(E, w.mx, w.nx, w.my, w.ny, q.ih[2], Z);
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        V[r][0] = X[r];
-        V[r][1] = Y[r];
-        V[r][2] = Z[r];
-    }
-}
 __device__ __forceinline__ void load_edges(const double *__restrict__ u, long long n0, const Q1Const &q,
                                            double E[3][4][3]) {
     double v[8][3];
@@ -334,6 +231,65 @@ __device__ __forceinline__ void scatter_slice(const double *sl, int T, const dou
         }
 }
 
+// ============================================================================================== cell energy
+// Reference J and curl at the Gauss points of one cell into the thread's shared slice (4 values per point).
+__device__ __forceinline__ void reference_points(const double *__restrict__ uref, long long n0, const Q1Const &q,
+                                                 double *sl, int T) {
+    double Er[3][4][3];
+    load_edges(uref, n0, q, Er);
+    sweep<false>(Er, q, [&](int p, int, int, int, const double (&Vr)[3][3]) {
+        double Cr[3];
+        curl_of(Vr, Cr);
+        sl[(4 * p) * T] = det_only(Vr);
+        sl[(4 * p + 1) * T] = Cr[0];
+        sl[(4 * p + 2) * T] = Cr[1];
+        sl[(4 * p + 3) * T] = Cr[2];
+    });
+}
+
+// partial[block][0..2] = sum w (J - Jr)^2, sum w |C - Cr|^2, sum barrier; violations counted in *bad
+__global__ void __launch_bounds__(CS) cell_energy_kernel(Q1Const q, const double *__restrict__ u,
+                                                         const double *__restrict__ uref, dd *partial,
+                                                         unsigned long long *bad) {
+    extern __shared__ double smem[];
+    double *sl = smem + threadIdx.x;
+    const int T = blockDim.x;
+    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    unsigned long long nbad = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        reference_points(uref, n0, q, sl, T);
+        double E[3][4][3];
+        load_edges(u, n0, q, E);
+        double sj = 0., sc = 0., sb = 0.;
+        sweep<false>(E, q, [&](int p, int, int, int, const double (&V)[3][3]) {
+            double C[3];
+            curl_of(V, C);
+            double dj = det_only(V) - sl[(4 * p) * T];
+            double c0 = C[0] - sl[(4 * p + 1) * T], c1 = C[1] - sl[(4 * p + 2) * T], c2 = C[2] - sl[(4 * p + 3) * T];
+            const double w = q.gw[p];
+            sj += w * dj * dj;
+            sc += w * (c0 * c0 + c1 * c1 + c2 * c2);
+        });
+        sweep<true>(E, q, [&](int, int, int, int, const double (&V)[3][3]) {
+            double J = det_only(V);
+            if (!(J > q.delta)) { nbad++; return; }
+            if (J < q.act) {
+                double b, b1, b2;
+                barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+                sb += b;
+            }
+        });
+        acc[0] = dd_add_d(acc[0], sj);
+        acc[1] = dd_add_d(acc[1], sc);
+        acc[2] = dd_add_d(acc[2], sb);
+    }
+    block_reduce_dd<3>(acc, partial);
+    for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
+}
+
 // Per-cell vertex values -> SoA locals L[(a * 3 + r) * ncell + c].
 __device__ __forceinline__ void store_locals(double *__restrict__ L, long long c, long long ncell,
                                              const double v[8][3]) {
@@ -343,6 +299,7 @@ __device__ __forceinline__ void store_locals(double *__restrict__ L, long long c
         for (int r = 0; r < 3; r++) L[(long long)(a * 3 + r) * ncell + c] = v[a][r];
 }
 
+// ============================================================================================== cell gradients
 // L1 = soft (JD, curl penalties scaled by mu_scale, nu_scale) + barrier; with split, L2 = barrier alone.
 __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *__restrict__ u,
                                                        const double *__restrict__ uref, double mu_scale,
@@ -366,12 +323,9 @@ __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *
             double Er[3][4][3];
             load_edges(uref, n0, q, Er);
             zero_slice(sl, T, 81);
-#pragma unroll 1
-            for (int p = 0; p < 27; p++) {
-                const PointW w = gauss_w(q, p);
-                double V[3][3], Vr[3][3], A[3][3], J, C[3], Cr[3];
-                grad_point(E, w, q, V);
-                grad_point(Er, w, q, Vr);
+            sweep2<false>(E, Er, q, [&](int p, int ix, int iy, int iz, const double (&V)[3][3],
+                                        const double (&Vr)[3][3]) {
+                double A[3][3], J, C[3], Cr[3];
                 cofactor_det(V, A, J);
                 double Jr = det_only(Vr);
                 curl_of(V, C);
@@ -387,18 +341,15 @@ __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *
                 f[2][1] += k0; f[1][2] -= k0;
                 f[0][2] += k1; f[2][0] -= k1;
                 f[1][0] += k2; f[0][1] -= k2;
-                add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
-            }
+                add_flux(sl, T, ix, iy, iz, f);
+            });
             scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
         }
         bool any = false;
         if (barrier) {
             zero_slice(sl, T, 81);
-#pragma unroll 1
-            for (int p = 0; p < 27; p++) {
-                double V[3][3];
-                grad_point(E, closed_w(p), q, V);
-                if (!(det_only(V) < q.act)) continue;
+            sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
+                if (!(det_only(V) < q.act)) return;
                 double A[3][3], J, b, b1, b2;
                 cofactor_det(V, A, J);
                 barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
@@ -407,9 +358,9 @@ __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *
                 for (int r = 0; r < 3; r++)
 #pragma unroll
                     for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * b1;
-                add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
+                add_flux(sl, T, ix, iy, iz, f);
                 any = true;
-            }
+            });
         }
         double Lb[8][3];
 #pragma unroll
@@ -470,12 +421,15 @@ __global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, co
 
 // ============================================================================================== GGN
 // Per-cell diagonal contributions: sum_p w (mu lj^2 + nu cs) + sum_closed27 b'' lc^2, lj = sum_j A_rj D_jpa.
-__device__ __forceinline__ void point_D(const PointW &w, int a, const double ih[3], double D[3]) {
+template <bool CLOSED>
+__device__ __forceinline__ void point_D(const Q1Const &q, int ix, int iy, int iz, int a, double D[3]) {
     const int bx = a & 1, by = (a >> 1) & 1, bz = (a >> 2) & 1;
-    const double fx = bx ? w.nx : w.mx, fy = by ? w.ny : w.my, fz = bz ? w.nz : w.mz;
-    D[0] = (bx ? ih[0] : -ih[0]) * fy * fz;
-    D[1] = (by ? ih[1] : -ih[1]) * fx * fz;
-    D[2] = (bz ? ih[2] : -ih[2]) * fx * fy;
+    const double fx = bx ? rule_n<CLOSED>(q, ix) : rule_m<CLOSED>(q, ix);
+    const double fy = by ? rule_n<CLOSED>(q, iy) : rule_m<CLOSED>(q, iy);
+    const double fz = bz ? rule_n<CLOSED>(q, iz) : rule_m<CLOSED>(q, iz);
+    D[0] = (bx ? q.ih[0] : -q.ih[0]) * fy * fz;
+    D[1] = (by ? q.ih[1] : -q.ih[1]) * fx * fz;
+    D[2] = (bz ? q.ih[2] : -q.ih[2]) * fx * fy;
 }
 
 __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const double *__restrict__ u,
@@ -488,17 +442,14 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] = 0.;
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = gauss_w(q, p);
-            double V[3][3], A[3][3], J;
-            grad_point(E, w, q, V);
+        sweep<false>(E, q, [&](int p, int ix, int iy, int iz, const double (&V)[3][3]) {
+            double A[3][3], J;
             cofactor_det(V, A, J);
             const double gw = q.gw[p];
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 double D[3];
-                point_D(w, a, q.ih, D);
+                point_D<false>(q, ix, iy, iz, a, D);
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
@@ -509,27 +460,23 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
                     out[a][r] += gw * (q.mu * lj * lj + q.nu * cs);
                 }
             }
-        }
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = closed_w(p);
-            double V[3][3];
-            grad_point(E, w, q, V);
-            if (!(det_only(V) < q.act)) continue;
+        });
+        sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
+            if (!(det_only(V) < q.act)) return;
             double A[3][3], J, b, b1, b2;
             cofactor_det(V, A, J);
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 double D[3];
-                point_D(w, a, q.ih, D);
+                point_D<true>(q, ix, iy, iz, a, D);
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lc = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
                     out[a][r] += b2 * lc * lc;
                 }
             }
-        }
+        });
         store_locals(L, c, q.ncell, out);
     }
 }
@@ -552,12 +499,9 @@ __global__ void __launch_bounds__(CS) cell_ggn_hvp_kernel(Q1Const q, const doubl
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] = 0.;
         zero_slice(sl, T, 81);
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = gauss_w(q, p);
-            double V[3][3], W[3][3], A[3][3], J, K[3];
-            grad_point(E, w, q, V);
-            grad_point(Ev, w, q, W);
+        sweep2<false>(E, Ev, q, [&](int p, int ix, int iy, int iz, const double (&V)[3][3],
+                                    const double (&W)[3][3]) {
+            double A[3][3], J, K[3];
             cofactor_det(V, A, J);
             double jd = 0.;
 #pragma unroll
@@ -576,20 +520,15 @@ __global__ void __launch_bounds__(CS) cell_ggn_hvp_kernel(Q1Const q, const doubl
             f[2][1] += k0; f[1][2] -= k0;
             f[0][2] += k1; f[2][0] -= k1;
             f[1][0] += k2; f[0][1] -= k2;
-            add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
-        }
+            add_flux(sl, T, ix, iy, iz, f);
+        });
         scatter_slice(sl, T, q.gn, q.gm, q.ih, out);
         zero_slice(sl, T, 81);
         bool any = false;
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = closed_w(p);
-            double V[3][3];
-            grad_point(E, w, q, V);
-            if (!(det_only(V) < q.act)) continue;
-            double W[3][3], A[3][3], J, b, b1, b2;
+        sweep2<true>(E, Ev, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3], const double (&W)[3][3]) {
+            if (!(det_only(V) < q.act)) return;
+            double A[3][3], J, b, b1, b2;
             cofactor_det(V, A, J);
-            grad_point(Ev, w, q, W);
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
             double lj = 0.;
 #pragma unroll
@@ -602,9 +541,9 @@ __global__ void __launch_bounds__(CS) cell_ggn_hvp_kernel(Q1Const q, const doubl
             for (int r = 0; r < 3; r++)
 #pragma unroll
                 for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * lj;
-            add_flux(sl, T, p % 3, (p / 3) % 3, p / 9, f);
+            add_flux(sl, T, ix, iy, iz, f);
             any = true;
-        }
+        });
         if (any) scatter_slice(sl, T, cn, cm, q.ih, out);
         store_locals(L, c, q.ncell, out);
     }
@@ -682,7 +621,13 @@ __global__ void __launch_bounds__(256) node_diff_kernel(Q1Const q, const double 
 }
 
 // Reference J and curl at the Gauss points go to the thread's shared slice first (108 values), so only the two
-// compared fields' edges are live in registers during the main pass.
+// compared fields' edges are live in registers during the main pass.  Per-point changes are exact products
+// (sq_change) summed with a compensated (hi, lo) accumulator.
+__device__ __forceinline__ void acc_add(dd &acc, dd t) {
+    dd s = two_sum(acc.hi, t.hi);
+    acc.hi = s.hi;
+    acc.lo += s.lo + t.lo;
+}
 __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *__restrict__ ua,
                                                        const double *__restrict__ ub,
                                                        const double *__restrict__ uref, dd *partial) {
@@ -693,53 +638,139 @@ __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
-        {
-            double Er[3][4][3];
-            load_edges(uref, n0, q, Er);
-#pragma unroll 1
-            for (int p = 0; p < 27; p++) {
-                double Vr[3][3], Cr[3];
-                grad_point(Er, gauss_w(q, p), q, Vr);
-                curl_of(Vr, Cr);
-                sl[(4 * p) * T] = det_only(Vr);
-                sl[(4 * p + 1) * T] = Cr[0];
-                sl[(4 * p + 2) * T] = Cr[1];
-                sl[(4 * p + 3) * T] = Cr[2];
-            }
-        }
+        reference_points(uref, n0, q, sl, T);
         double Ea[3][4][3], Eb[3][4][3];
         load_edges(ua, n0, q, Ea);
         load_edges(ub, n0, q, Eb);
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = gauss_w(q, p);
-            double Va[3][3], Vb[3][3], Ca[3], Cb[3];
-            grad_point(Ea, w, q, Va);
-            grad_point(Eb, w, q, Vb);
+        sweep2<false>(Ea, Eb, q, [&](int p, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
+            double Ca[3], Cb[3];
             const double jr = sl[(4 * p) * T];
-            const double smu = sqrt(q.mu * q.gw[p]), snu = sqrt(q.nu * q.gw[p]);
-            acc[0] = dd_add(acc[0], sq_change(smu * (det_only(Va) - jr), smu * (det_only(Vb) - jr)));
+            const double smu = q.sqmu[p], snu = q.sqnu[p];
+            acc_add(acc[0], sq_change(smu * (det_only(Va) - jr), smu * (det_only(Vb) - jr)));
             curl_of(Va, Ca);
             curl_of(Vb, Cb);
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 const double cr = sl[(4 * p + 1 + r) * T];
-                acc[1] = dd_add(acc[1], sq_change(snu * (Ca[r] - cr), snu * (Cb[r] - cr)));
+                acc_add(acc[1], sq_change(snu * (Ca[r] - cr), snu * (Cb[r] - cr)));
             }
-        }
+        });
         double sb = 0.;
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = closed_w(p);
-            double Va[3][3], Vb[3][3];
-            grad_point(Ea, w, q, Va);
-            grad_point(Eb, w, q, Vb);
+        sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
             double ja = det_only(Va), jb = det_only(Vb);
             if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
-        }
-        acc[2] = dd_add_d(acc[2], q.bw * sb);
+        });
+        acc_add(acc[2], dd{q.bw * sb, 0.});
     }
+#pragma unroll
+    for (int k = 0; k < 3; k++) acc[k] = two_sum(acc[k].hi, acc[k].lo);
     block_reduce_dd<3>(acc, partial);
+}
+
+// ============================================================================================== line-search trial
+// A trial evaluated against its base in one node pass and one cell pass: the trial's warped image (and image
+// gradient), its energy sums exactly as node_energy_kernel / cell_energy_kernel form them, and the stable base ->
+// trial changes exactly as node_diff_kernel / cell_diff_kernel form them (same grids, same per-thread order, so the
+// results are bitwise those of the separate passes).
+template <bool GRAD>
+__global__ void __launch_bounds__(256) warp_trial_kernel(Q1Const q, SplineRef S, const double *__restrict__ ua,
+                                                         const double *__restrict__ wa,
+                                                         const double *__restrict__ ub,
+                                                         const double *__restrict__ fixed,
+                                                         const double *__restrict__ uref, double *__restrict__ wb,
+                                                         double *__restrict__ image_grad, dd *pe, dd *pd) {
+    dd acc[2] = {{0., 0.}, {0., 0.}}, dif[2] = {{0., 0.}, {0., 0.}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        double ux = ub[3 * i], uy = ub[3 * i + 1], uz = ub[3 * i + 2];
+        double px = (q.x0[0] + q.h[0] * (double)x) + ux;
+        double py = (q.x0[1] + q.h[1] * (double)y) + uy;
+        double pz = (q.x0[2] + q.h[2] * (double)z) + uz;
+        double g[3];
+        double w = spline_eval<GRAD>(S, px, py, pz, g);
+        wb[i] = w;
+        if (GRAD) {
+            image_grad[3 * i] = g[0];
+            image_grad[3 * i + 1] = g[1];
+            image_grad[3 * i + 2] = g[2];
+        }
+        double qw = node_weight(x, y, z, q);
+        double f = fixed[i];
+        double d = w - f;
+        double r0 = uref[3 * i], r1 = uref[3 * i + 1], r2 = uref[3 * i + 2];
+        double e0 = ux - r0, e1 = uy - r1, e2 = uz - r2;
+        acc[0] = dd_add_d(acc[0], qw * d * d);
+        acc[1] = dd_add_d(acc[1], qw * (e0 * e0 + e1 * e1 + e2 * e2));
+        double sq = sqrt(qw), sl = sqrt(q.lam * qw);
+        dif[0] = dd_add(dif[0], sq_change(sq * (wa[i] - f), sq * d));
+        dif[1] = dd_add(dif[1], sq_change(sl * (ua[3 * i] - r0), sl * e0));
+        dif[1] = dd_add(dif[1], sq_change(sl * (ua[3 * i + 1] - r1), sl * e1));
+        dif[1] = dd_add(dif[1], sq_change(sl * (ua[3 * i + 2] - r2), sl * e2));
+    }
+    block_reduce_dd<2>(acc, pe);
+    __syncthreads();     // the two reductions share block_reduce_dd's shared array
+    block_reduce_dd<2>(dif, pd);
+}
+
+__global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double *__restrict__ ua,
+                                                        const double *__restrict__ ub,
+                                                        const double *__restrict__ uref, dd *pe, dd *pd,
+                                                        unsigned long long *bad) {
+    extern __shared__ double smem[];
+    double *sl = smem + threadIdx.x;
+    const int T = blockDim.x;
+    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}}, dif[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    unsigned long long nbad = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        reference_points(uref, n0, q, sl, T);
+        double Ea[3][4][3], Eb[3][4][3];
+        load_edges(ua, n0, q, Ea);
+        load_edges(ub, n0, q, Eb);
+        double sj = 0., sc = 0., sb = 0., sbd = 0.;
+        sweep2<false>(Ea, Eb, q, [&](int p, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
+            double Ca[3], Cb[3];
+            const double jr = sl[(4 * p) * T];
+            const double smu = q.sqmu[p], snu = q.sqnu[p];
+            const double jb = det_only(Vb);
+            acc_add(dif[0], sq_change(smu * (det_only(Va) - jr), smu * (jb - jr)));
+            curl_of(Va, Ca);
+            curl_of(Vb, Cb);
+            double cd[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const double cr = sl[(4 * p + 1 + r) * T];
+                cd[r] = Cb[r] - cr;
+                acc_add(dif[1], sq_change(snu * (Ca[r] - cr), snu * cd[r]));
+            }
+            const double w = q.gw[p], dj = jb - jr;
+            sj += w * dj * dj;
+            sc += w * (cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+        });
+        sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
+            double ja = det_only(Va), jb = det_only(Vb);
+            if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+            if (!(jb > q.delta)) { nbad++; return; }
+            if (jb < q.act) {
+                double b, b1, b2;
+                barrier_eval(jb, q.act, q.delta, q.bw, b, b1, b2);
+                sb += b;
+            }
+        });
+        acc[0] = dd_add_d(acc[0], sj);
+        acc[1] = dd_add_d(acc[1], sc);
+        acc[2] = dd_add_d(acc[2], sb);
+        acc_add(dif[2], dd{q.bw * sbd, 0.});
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) dif[k] = two_sum(dif[k].hi, dif[k].lo);
+    block_reduce_dd<3>(acc, pe);
+    __syncthreads();     // the two reductions share block_reduce_dd's shared array
+    block_reduce_dd<3>(dif, pd);
+    for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
 }
 
 // ============================================================================================== node JD measure
@@ -753,14 +784,11 @@ __global__ void __launch_bounds__(CS) cell_min_jd_kernel(Q1Const q, const double
         double E[3][4][3];
         load_edges(u, cell_node0(c, q), q, E);
         double mn = __longlong_as_double(0x7FF0000000000000LL);
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            double V[3][3];
-            grad_point(E, closed_w(p), q, V);
+        sweep<true>(E, q, [&](int p, int, int, int, const double (&V)[3][3]) {
             double j = det_only(V);
             J[p * T] = j;
             mn = fmin(mn, j);
-        }
+        });
         // exact interior minima of the edge quadratics through t = 0, 1/2, 1 (solvers/jd_affine.py:24)
 #pragma unroll 1
         for (int e = 0; e < 12; e++) {
@@ -846,12 +874,8 @@ __global__ void __launch_bounds__(CT) jd_root_kernel(Q1Const q, const double *__
         double E[3][4][3], Ep[3][4][3];
         load_edges(u, n0, q, E);
         load_edges(pv, n0, q, Ep);
-#pragma unroll 1
-        for (int p = 0; p < 27; p++) {
-            const PointW w = closed_w(p);
-            double V[3][3], W[3][3], AF[3][3], AV[3][3], J, JV;
-            grad_point(E, w, q, V);
-            grad_point(Ep, w, q, W);
+        sweep2<true>(E, Ep, q, [&](int, int, int, int, const double (&V)[3][3], const double (&W)[3][3]) {
+            double AF[3][3], AV[3][3], J, JV;
             cofactor_det(V, AF, J);
 #pragma unroll
             for (int r = 0; r < 3; r++) {
@@ -871,11 +895,11 @@ __global__ void __launch_bounds__(CT) jd_root_kernel(Q1Const q, const double *__
                     c1 += AF[r][cc] * W[r][cc];
                     c2 += (V[r][cc] + (r == cc ? 1. : 0.)) * AV[r][cc];
                 }
-            if (!(c0 > 0)) { nbad++; continue; }
+            if (!(c0 > 0)) { nbad++; return; }
             double s = first_root(c0, c1 * limit, c2 * L2, JV * L3);
             long long k = order_key(s);
             key = k < key ? k : key;
-        }
+        });
     }
     for (int o = 16; o; o >>= 1) {
         long long y = __shfl_xor_sync(0xFFFFFFFFu, key, o);
@@ -959,8 +983,12 @@ unsigned slice_blocks(const svp_pair *p) { return blocks_for(p->q.ncell, CS, 2 *
 // dynamic shared memory of the slice kernels: k doubles per thread
 constexpr size_t slice_bytes(int k) { return sizeof(double) * (size_t)k * CS; }
 int allow_slices() {
-    // cell_diff_kernel's slice is above the 48 KB default; the attribute is per device context, so set it per call
+    // the 108-value slices are above the 48 KB default; the attribute is per device context, so set it per call
     SVP_CUDA(cudaFuncSetAttribute(cell_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)slice_bytes(108)));
+    SVP_CUDA(cudaFuncSetAttribute(cell_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)slice_bytes(108)));
+    SVP_CUDA(cudaFuncSetAttribute(cell_trial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)slice_bytes(108)));
     return SVP_OK;
 }
@@ -1018,14 +1046,15 @@ extern "C" int svp_energy(svp_pair *p, const double *u, const double *warped, do
                           int64_t *barrier_violations, void *stream) {
     SVP_REQUIRE(p && u && warped && terms5, "svp_energy: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned nb = node_blocks(p->q.nnode), cb = cell_blocks(p);
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
     int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
     if (rc) return rc;
+    if ((rc = allow_slices())) return rc;
     SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
     { svp::KernelTimer _t("node_energy_kernel", s); SVP_LAUNCH(node_energy_kernel<<<nb, 256, 0, s>>>(p->q, u, warped, p->fixed, p->u_ref, p->partial)); }
     SVP_LAUNCH_CHECK("node_energy_kernel");
     dd *pc = p->partial + (long long)nb * 2;
-    { svp::KernelTimer _t("cell_energy_kernel", s); SVP_LAUNCH(cell_energy_kernel<<<cb, CT, 0, s>>>(p->q, u, p->u_ref, pc, (unsigned long long *)p->counter)); }
+    { svp::KernelTimer _t("cell_energy_kernel", s); SVP_LAUNCH(cell_energy_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, u, p->u_ref, pc, (unsigned long long *)p->counter)); }
     SVP_LAUNCH_CHECK("cell_energy_kernel");
     double node2[2], cell3[3];
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
@@ -1071,6 +1100,59 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
     // E = image + proximity + jd + curl + barrier; F = image + barrier (sums of double-double pieces)
     double img = tmp[0] + tmp[1], prox = tmp[2] + tmp[3];
     double jd = tmp[4] + tmp[5], curl = tmp[6] + tmp[7], bar = tmp[8] + tmp[9];
+    diff2[0] = (((img + prox) + jd) + curl) + bar;
+    diff2[1] = img + bar;
+    return SVP_OK;
+}
+
+extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warped,
+                                const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                double *terms5, double *diff2, int64_t *barrier_violations, void *stream) {
+    SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && terms5 && diff2,
+                "svp_trial_energy: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
+    int rc = pair_partials(p, (long long)nb * 4 + (long long)cb * 6, 1);
+    if (rc) return rc;
+    if ((rc = allow_slices())) return rc;
+    SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
+    dd *pne = p->partial, *pnd = pne + (long long)nb * 2, *pce = pnd + (long long)nb * 2, *pcd = pce + (long long)cb * 3;
+    SplineRef S = spline_ref(p);
+    if (trial_image_grad) {
+        svp::KernelTimer _t("warp_trial_kernel_grad", s);
+        SVP_LAUNCH(warp_trial_kernel<true><<<nb, 256, 0, s>>>(p->q, S, base_u, base_warped, trial_u, p->fixed,
+                                                                p->u_ref, trial_warped, trial_image_grad, pne, pnd));
+    } else {
+        svp::KernelTimer _t("warp_trial_kernel", s);
+        SVP_LAUNCH(warp_trial_kernel<false><<<nb, 256, 0, s>>>(p->q, S, base_u, base_warped, trial_u, p->fixed,
+                                                                 p->u_ref, trial_warped, nullptr, pne, pnd));
+    }
+    SVP_LAUNCH_CHECK("warp_trial_kernel");
+    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter)); }
+    SVP_LAUNCH_CHECK("cell_trial_kernel");
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pnd, nb, 2, p->result + 10));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 3, p->result + 14));
+    SVP_LAUNCH_CHECK("final_reduce_kernel");
+    double tmp[20];
+    long long bad = 0;
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaMemcpyAsync(&bad, p->counter, sizeof bad, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    // energy terms exactly as svp_energy
+    double node2[2], cell3[3];
+    for (int k = 0; k < 2; k++) node2[k] = tmp[2 * k] + tmp[2 * k + 1];
+    for (int k = 0; k < 3; k++) cell3[k] = tmp[4 + 2 * k] + tmp[4 + 2 * k + 1];
+    terms5[0] = .5 * node2[0];
+    terms5[1] = .5 * p->q.lam * node2[1];
+    terms5[2] = .5 * p->q.mu * cell3[0];
+    terms5[3] = .5 * p->q.nu * cell3[1];
+    terms5[4] = cell3[2];
+    if (barrier_violations) *barrier_violations = bad;
+    // differences exactly as svp_energy_difference
+    double img = tmp[10] + tmp[11], prox = tmp[12] + tmp[13];
+    double jd = tmp[14] + tmp[15], curl = tmp[16] + tmp[17], bar = tmp[18] + tmp[19];
     diff2[0] = (((img + prox) + jd) + curl) + bar;
     diff2[1] = img + bar;
     return SVP_OK;

@@ -88,6 +88,18 @@ class DevicePair:
                   stream_ptr(stream))
         return d[0], d[1]
 
+    def trial_energy(self, base_u, base_w, trial_u, with_gradient=True, stream=None):
+        """Warp and evaluate a trial against its base in one pass: (warped, image_grad or None, terms[5],
+        barrier violations, (E(trial) - E(base), F(trial) - F(base)))."""
+        w = self.node()
+        g = self.node(3) if with_gradient else None
+        t = (ctypes.c_double * 5)()
+        d = (ctypes.c_double * 2)()
+        bad = ctypes.c_int64()
+        _lib.call("svp_trial_energy", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g), t, d,
+                  ctypes.byref(bad), stream_ptr(stream))
+        return w, g, np.array(t[:]), int(bad.value), (d[0], d[1])
+
     def gradient(self, u, warped, image_grad, term="total", out=None, stream=None):
         out = self.free() if out is None else out
         _lib.call("svp_gradient", self._h, ptr(u), ptr(warped), ptr(image_grad), _lib.TERMS[term], ptr(out),

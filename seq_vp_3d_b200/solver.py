@@ -66,6 +66,7 @@ class State:
     eval_id: int
     image_grad: torch.Tensor = None    # set by promotion
     norms: tuple = None                # (GF, GD, GE) when computed with the final gradient
+    differences: tuple = None          # ((base eval_id, reference version), (dE, dF)) from the one-pass trial
 
     @property
     def total(self):
@@ -126,6 +127,7 @@ class Registration:
         self.q_sum = float(np.sum(grid.node_weights(), dtype=np.longdouble))
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0
+        self._reference_version = 0
         ref = self.certify(torch.as_tensor(np.ascontiguousarray(u_ref, dtype=np.float64), device="cuda"))
         if ref.status != "certified_feasible":
             raise ValueError(f"u_ref: not certified feasible ({ref.reason})")
@@ -136,7 +138,10 @@ class Registration:
         rec = self.certifier.run(u)
         return cert_mod.result_from_record(rec, self.grid, self.config, None)
 
-    def evaluate_trial(self, theta, observer=None):
+    def evaluate_trial(self, theta, observer=None, base=None):
+        """Certify, warp and evaluate theta.  With the line search's base, the trial is warped (with its image
+        gradient, so promotion is free) and evaluated against the base in one pass, and the stable base -> trial
+        differences are kept for stable_reductions (bitwise the separate passes' values)."""
         u = self.pair.inject(theta)
         c = self.certify(u)
         if observer is not None:
@@ -145,16 +150,23 @@ class Registration:
             reason = ("NONFINITE_STATE" if c.reason == "NONFINITE_STATE" else
                       "FEASIBILITY_UNCERTAIN" if c.status == "uncertain" else c.reason)
             return InvalidTrial(reason, "trial not certified: " + c.reason, c.n_uncertain + c.n_infeasible)
-        warped, _ = self.pair.warp(u)
-        terms, bad = self.pair.energy(u, warped)
+        grad = diff = None
+        if base is None:
+            warped, _ = self.pair.warp(u)
+            terms, bad = self.pair.energy(u, warped)
+        else:
+            warped, grad, terms, bad, diff = self.pair.trial_energy(base.u, base.warped, u)
         if bad or not np.all(np.isfinite(terms)):
             return InvalidTrial("NONFINITE_STATE", "floating barrier-point evaluation contradicts feasible certificate", 1)
         self._eval += 1
-        return State(theta, u, warped, terms, c, self._eval)
+        state = State(theta, u, warped, terms, c, self._eval, image_grad=grad)
+        if diff is not None:
+            state.differences = ((base.eval_id, self._reference_version), diff)
+        return state
 
     def promote_trial(self, state):
-        _, grad = self.pair.warp(state.u, with_gradient=True)
-        state.image_grad = grad
+        if state.image_grad is None:
+            _, state.image_grad = self.pair.warp(state.u, with_gradient=True)
         return state
 
     def prepare_base(self, theta):
@@ -165,6 +177,7 @@ class Registration:
         """Self-reference refresh (problem.py:397 make_self_reference; sequential.py:347): u_ref = u of a certified
         state; that state's proximity/JD/curl penalties become exactly zero."""
         self.pair.set_reference(state.u)
+        self._reference_version += 1
         self.reference_certificate = state.certificate
         e = state.energy.copy()
         e[1:4] = 0.
@@ -184,7 +197,11 @@ class Registration:
 
     def stable_reductions(self, base, trial):
         """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:266)."""
-        dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped)
+        cached = trial.differences
+        if cached is not None and cached[0] == (base.eval_id, self._reference_version):
+            dE, dF = cached[1]
+        else:
+            dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped)
         rE = 16 * EPS * max(base.total, trial.total)
         rF = 16 * EPS * max(base.outer, trial.outer)
         return (-dE, rE), (-dF, rF)
@@ -428,7 +445,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         for attempt in range(config.max_backtracks + 1):
             candidate = axpy(base.theta, tau, p)
             required = -config.c1 * tau * slope
-            trial = reg.evaluate_trial(candidate, observer=memory.certificate)
+            trial = reg.evaluate_trial(candidate, observer=memory.certificate, base=base)
             valid = not isinstance(trial, InvalidTrial)
             actual = resolution = None
             if valid:

@@ -84,6 +84,22 @@ def test_stable_difference(gold):
         assert abs(got - ref) <= min(TOL * abs(ref), res / 8), (dE, dF, red)
 
 
+def test_one_pass_trial_matches_separate_passes(gold):
+    """svp_trial_energy: warped image, image gradient, energy terms, violations and base -> trial differences are
+    bitwise those of svp_warp, svp_energy and svp_energy_difference."""
+    d, grid, P, u1, w1, g1 = gold
+    u2 = dev(d["u2"])
+    w2, g2 = P.warp(u2, with_gradient=True)
+    terms, bad = P.energy(u2, w2)
+    diff = P.energy_difference(u1, w1, u2, w2)
+    tw, tg, tterms, tbad, tdiff = P.trial_energy(u1, w1, u2)
+    assert torch.equal(tw, w2) and torch.equal(tg, g2)
+    assert same_bits(tterms, terms) and tbad == bad
+    assert same_bits(np.array(tdiff), np.array(diff))
+    tw, none, tterms, tbad, tdiff = P.trial_energy(u1, w1, u2, with_gradient=False)
+    assert none is None and torch.equal(tw, w2) and same_bits(tterms, terms)
+
+
 def test_poisson_metric_direction(gold):
     d, grid, P, u1, w1, g1 = gold
     alpha, a, b, m = d["poisson_ab"]
