@@ -38,10 +38,13 @@ PER_OUTER = dict(trials=5, gradients=5, outer_triples=1, directions=5, metric_bu
 def parse():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--outer", type=int, default=20, help="outer steps per registration")
+    ap.add_argument("--outer", type=int, default=200, help="outer steps per registration (config 2: 200)")
+    ap.add_argument("--preopt", action=argparse.BooleanOptionalAction, default=False,
+                    help="config-2 route: float32 8/4/2/1 pyramid pre-optimizer + certified transfer before the "
+                         "native steps")
     ap.add_argument("--shape", default="160,192,224", help="nx,ny,nz")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -104,27 +107,63 @@ def peaks():
 
 
 # ------------------------------------------------------------------------------------------ algorithmic counts
+# FP64 operations per cell of the cell kernels, counted from their source (csrc/q1.cu, csrc/q1_common.cuh):
+# one grad-u column = 30 (3 components x (2 bilinear lerps of 3 + final lerp and 1/h of 4)); det = 17; cofactor+det
+# = 35; curl = 3; sq_change = 20; compensated add = 8.  Barrier-active points add a few hundred more (not counted).
+FLOP_PER_CELL = {
+    # edges 108 + reference sweep (45 columns + 27 x (det + curl)) 1890 + Gauss sweep2 (126 columns) 3780
+    # + 27 x (2 det + 2 curl + 4 stable changes + trial energy) 4833 + closed sweep2 3780 + 27 x 2 det 918
+    "cell_trial_kernel": 15309,
+    "cell_diff_kernel": 15006,
+    # edges 72 + ref sweep 1890 + Gauss sweep (45 columns) 1350 + 27 x 31 + closed sweep 1350 + 27 x det 459
+    "cell_energy_kernel": 5958,
+    # edges 72 + soft sweep2 3780 + 27 x 94 (cofactor, det, curls, fluxes) + adjoint scatter 693
+    # + barrier sweep 1350 + 27 x det 459
+    "cell_grad_kernel": 8892,
+    # edges 36 + Gauss sweep 1350 + 27 x (cofactor 35 + 8 vertices x 48) + closed sweep 1350 + 27 x det 459
+    "cell_ggn_diag_kernel": 14508,
+    "cell_min_jd_kernel": 2009,
+}
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12     # nominal: 148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz
+# DRAM bytes (read + write) per cell measured by ncu on the 160x192x96 pair (2,885,055 cells; profiles/
+# traffic_cell_trial_edge_hull_warp_160x192x96.md); scaled to a launch by the cells it processes (traffic grows with
+# the cell count: every launch streams its fields once, plus neighbour re-reads of the same order)
+TRAFFIC_PER_CELL = {"cell_trial_kernel": (325667584 + 1371392) / 2885055,
+                    "edge_hull_kernel": (74312512 + 8776576) / 2885055,
+                    "warp_trial_kernel_grad": (312493568 + 74758400) / 2885055}
+
+
 def kernel_counts(shape):
-    """Algorithmic HBM bytes per launch of the hot kernels (each input field read once, outputs written once)."""
+    """(algorithmic HBM bytes, FP64 FLOP) per launch of the hot kernels: each input field read once, outputs written
+    once; FLOP from FLOP_PER_CELL (cell kernels) or the GEMM count (DST-I passes, averaged over the passes)."""
     nx, ny, nz = shape
     nn, nc, nf = nx * ny * nz, (nx - 1) * (ny - 1) * (nz - 1), (nx - 2) * (ny - 2) * (nz - 2)
+    f = [nx - 2, ny - 2, nz - 2]
+    # one folded DST-I pass along an axis of length n: 2 (ceil(n/2)^2 + floor(n/2)^2) FLOP per line, 3 nf / n lines
+    dst = [2 * (((n + 1) // 2) ** 2 + (n // 2) ** 2) * 3 * nf / n for n in f]
+    c = lambda name: FLOP_PER_CELL[name] * nc
     return {
-        # u, u_ref, base: 24 B/node each; per-block partial sums negligible
-        "cell_diff_kernel": 3 * 24 * nn,
-        "cell_energy_kernel": 2 * 24 * nn,
-        # u, u_ref in; 24 doubles per cell out per locals buffer (1 or 2; counted as 1.5 on average: total and outer)
-        "cell_grad_kernel": 2 * 24 * nn + 192 * nc,
-        "gather_kernel": 192 * nc + nn * (24 + 24 + 8 + 8 + 24) + 3 * 8 * nf,
-        "cell_ggn_diag_kernel": 24 * nn + 192 * nc,
-        "edge_hull_kernel": 24 * nn + 9 * nc,
-        "warp_kernel": 24 * nn + 8 * nn + 8 * nn,              # u, coefficients (cache resident), warped out
-        "warp_kernel_grad": 24 * nn + 8 * nn + 32 * nn,
-        "gemm_left_kernel": 2 * 3 * 8 * nf,
-        "gemm_right_kernel": 2 * 3 * 8 * nf,
-        "node_diff_kernel": 2 * (24 + 8) * nn + 8 * nn + 24 * nn,
-        "node_energy_kernel": (24 + 8 + 8 + 24) * nn,
-        "precheck_kernel": 24 * nn,
-        "cell_min_jd_kernel": 24 * nn + 8 * nc,
+        # base u, trial u, u_ref: 24 B/node each
+        "cell_trial_kernel": (3 * 24 * nn, c("cell_trial_kernel")),
+        "cell_diff_kernel": (3 * 24 * nn, c("cell_diff_kernel")),
+        "cell_energy_kernel": (2 * 24 * nn, c("cell_energy_kernel")),
+        # u, u_ref in; 24 doubles per cell out (one locals buffer; two for the outer triple)
+        "cell_grad_kernel": (2 * 24 * nn + 192 * nc, c("cell_grad_kernel")),
+        "gather_kernel": (192 * nc + nn * (24 + 24 + 8 + 8 + 24) + 3 * 8 * nf, None),
+        "cell_ggn_diag_kernel": (24 * nn + 192 * nc, c("cell_ggn_diag_kernel")),
+        "edge_hull_kernel": (24 * nn + 9 * nc, None),
+        # trial u, base u, base warped, fixed, u_ref in; warped (+ gradient) out; coefficients cache resident
+        "warp_trial_kernel_grad": ((24 + 24 + 8 + 8 + 24 + 8 + 24) * nn, None),
+        "warp_trial_kernel": ((24 + 24 + 8 + 8 + 24 + 8) * nn, None),
+        "warp_kernel": ((24 + 8) * nn, None),
+        "warp_kernel_grad": ((24 + 8 + 24) * nn, None),
+        # folded input read once, output written once (+ the scale / denominator arrays where fused)
+        "dst_left_kernel": (2 * 3 * 8 * nf, (dst[1] + dst[2]) / 2),
+        "dst_right_kernel": (2 * 3 * 8 * nf, dst[0]),
+        "node_diff_kernel": (2 * (24 + 8) * nn + 8 * nn + 24 * nn, None),
+        "node_energy_kernel": ((24 + 8 + 8 + 24) * nn, None),
+        "precheck_kernel": (24 * nn, None),
+        "cell_min_jd_kernel": (24 * nn + 8 * nc, c("cell_min_jd_kernel")),
     }
 
 
@@ -193,8 +232,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from seq_vp_3d_b200.synthetic import default_weights, head_pair
     weights = default_weights((nz, ny, nx), (1., 1., 1.))
+    start = ("float32 8/4/2/1 pyramid pre-optimizer, taper, certified transfer, then" if args.preopt else "from u=0:")
     config = {"workload": f"head phantom pair {nx}x{ny}x{nz} (x fastest), 1 mm, float64, certified proximal loop "
-                          f"from u=0: {args.outer} outer steps x 5 PG steps",
+                          f"{start} {args.outer} outer steps x 5 PG steps (T73 metric)",
               "grid_nodes": nx * ny * nz, "outer_steps": args.outer, "inner_steps": 5,
               "form": "plain FP64", "l2_policy": "inputs larger than L2 (6.9M-node fields, 55-165 MB each)"}
     if args.impl == "reference":
@@ -237,8 +277,13 @@ def main():
     stream = torch.cuda.current_stream()
 
     def step(f, m):
-        reg = Registration(grid, f, m, **weights)
-        res = solve_sequential(reg, config=outer_cfg, inner_config=inner_cfg)
+        if args.preopt:
+            from seq_vp_3d_b200.preopt import register_pair
+            res, _ = register_pair(f, m, grid, weights, outer=args.outer, inner_config=inner_cfg)
+            reg = None
+        else:
+            reg = Registration(grid, f, m, **weights)
+            res = solve_sequential(reg, config=outer_cfg, inner_config=inner_cfg)
         if not res.certified:
             raise RuntimeError(f"registration ended without a certified state: {res.status}")
         return reg, res
@@ -310,11 +355,19 @@ def main():
         if dominant:
             cnt, ms = timers[dominant]
             per_launch_s = ms / 1e3 / cnt
-            achieved = counts[dominant] / per_launch_s / 1e9
+            nbytes, flop = counts[dominant]
+            achieved = nbytes / per_launch_s / 1e9
+            ncell = (nx - 1) * (ny - 1) * (nz - 1)
+            traffic = TRAFFIC_PER_CELL[dominant] * ncell if dominant in TRAFFIC_PER_CELL else None
             roofline = dict(kernel=dominant, bound="hbm", achieved=achieved, peak=hbm, unit="GB/s",
-                            frac=achieved / hbm, traffic=None, peak_source=kind, launches=cnt,
-                            avg_launch_ms=ms / cnt, algorithmic_bytes_per_launch=counts[dominant],
+                            frac=achieved / hbm, traffic=traffic, peak_source=kind, launches=cnt,
+                            avg_launch_ms=ms / cnt, algorithmic_bytes_per_launch=nbytes,
                             share_of_timed=ms / 1e3 / (seconds * world) if seconds else None)
+            if flop:
+                # the cell kernels are FP64-pipe bound: their FLOP rate against the nominal FP64 peak
+                roofline["fp64"] = dict(flop_per_launch=flop, achieved_tflops=flop / per_launch_s / 1e12,
+                                        peak_tflops=FP64_PEAK_TFLOPS, frac=flop / per_launch_s / 1e12 / FP64_PEAK_TFLOPS,
+                                        peak_source="nominal (148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz)")
         if args.profile:
             total = sum(v[1] for v in timers.values())
             for k, (c, ms) in sorted(timers.items(), key=lambda kv: -kv[1][1]):

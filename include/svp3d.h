@@ -203,6 +203,14 @@ int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_grad, const do
 /* Node JD measure J_a = min over the cells containing node a of (closed27 values and edge-quadratic minima)
  * (solvers/jd_affine.py:205 node_min_jd without the face/interior extension).  node: (nz, ny, nx). */
 int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream);
+/* The same measure with the T69/T73 face/interior extension (solvers/jd_affine.py:205 node_min_jd with
+ * extension_activation; :173 extend_minima): cells whose closed27 Bernstein coefficients allow a value below
+ * min(m_c, extension_activation) take m_c = min(m_c, mu_c), mu_c the minimum over the 9^3 grid and a bounded Newton
+ * descent from its 4 lowest points (a value the cell's J attains: a metric estimate, never a bound).
+ * extension_activation 0 gives svp_node_min_jd exactly.  candidates (host, optional; synchronizes) receives the
+ * number of candidate cells. */
+int svp_node_min_jd_extended(svp_pair *p, const double *u, double extension_activation, double *node,
+                             int64_t *candidates, void *stream);
 /* First root tau in (0, limit] of det(I + grad u + tau grad p) - delta over all closed27 points
  * (solvers/global_jd_step.py:107 global_root_cpu; backends/torch_ops.py:636 global_jd_root).  root: host, +inf when
  * no root; invalid: host count of points with det(I + grad u) - delta <= 0.  Synchronizes. */
@@ -249,6 +257,36 @@ int svp_image_shift(svp_pair *p, const double *image_grad, double factor, double
  * where d <= 0 or the scale is not finite and positive (the reference raises there).  Synchronizes. */
 int svp_pg_scale(svp_pair *p, const double *diag, const double *node_jd, double m, double activation, double floor_,
                  double *scale, int64_t *bad, void *stream);
+
+/* ---------------------------------------------------------------- float32 pyramid pre-optimizer (uncertified) */
+/* Pre-objective weights and Adam settings of one level (preopt.py:32 PreoptConfig, the level's mu and alpha). */
+typedef struct svp_pre_params {
+    double mu, alpha, kappa, j0;      /* geometry weight, curvature weight, positivity-floor weight and floor */
+    double lr, cap;                   /* Adam step (voxels) and the largest node move per iteration (voxels) */
+    double sigma_grad, sigma_field;   /* Gaussian smoothing of the gradient / of the field after a step (0: off) */
+    double beta1, beta2, eps;
+} svp_pre_params;
+/* Pre-objective terms (data, geometry, floor, curvature, min cell-centre det, total; terms6 host) and its gradient
+ * with respect to the interior displacement u_int (3, D-2, H-2, W-2), voxel units, float32 (preopt.py:157
+ * _pre_energy_tensors and its autograd gradient; preopt_grad.py:358 TritonPreGrad).  fixed, moving: (D, H, W). */
+int svp_pre_energy_grad(const float *fixed, const float *moving, int32_t D, int32_t H, int32_t W, double hx, double hy,
+                        double hz, const float *u_int, double mu, double alpha, double kappa, double j0, float *grad,
+                        float *terms6, void *stream);
+/* `iterations` Adam iterations of one level on the device (preopt.py:217 _run_level_default): u_int, m, v updated in
+ * place; the Adam step counter starts at first_iteration + 1.  terms_first / terms_last (host, 6 each, optional):
+ * the terms at the first and the last iteration; cap_hits (host, optional): iterations whose step was capped. */
+int svp_pre_level(const float *fixed, const float *moving, int32_t D, int32_t H, int32_t W, double hx, double hy,
+                  double hz, const svp_pre_params *params, int32_t first_iteration, int32_t iterations, float *u_int,
+                  float *m, float *v, float *terms_first, float *terms_last, int64_t *cap_hits, void *stream);
+/* Pyramid image (nifti.py:128 downsample_array): Gaussian sigma = .5 sqrt(ratio^2 - 1) per axis (mode nearest,
+ * truncate 4) then linear resampling at linspace(0, n - 1, m) per axis.  src (nz, ny, nx), dst (mz, my, mx). */
+int svp_image_downsample(const double *src, int32_t nz, int32_t ny, int32_t nx, double *dst, int32_t mz, int32_t my,
+                         int32_t mx, void *stream);
+/* Q1 transfer of a displacement (nz, ny, nx, 3) between pyramid grids (multiresolution.py:55 prolong_displacement):
+ * separable linear interpolation z, then y, then x with the per-axis (left index, weight) tables the host derives
+ * from the two grids' axes (left_zyx, weight_zyx: tz + ty + tx entries, host).  Synchronizes. */
+int svp_field_prolong(const double *u, int32_t sz, int32_t sy, int32_t sx, double *out, int32_t tz, int32_t ty,
+                      int32_t tx, const int32_t *left_zyx, const double *weight_zyx, void *stream);
 
 #ifdef __cplusplus
 }

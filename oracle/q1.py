@@ -510,16 +510,105 @@ def closed27_cell_minima(J):
     return np.minimum(J.min(axis=1), em.min(axis=1))
 
 
-def node_min_jd(problem, u):
-    """T62 node measure (solvers/jd_affine.py:205 without the extension)."""
+def to_bernstein27(J):
+    """bernstein_barrier.py:26: closed27 values -> Bernstein coefficients, per axis x, y, z middle = 2b - (a+c)/2."""
+    v = np.array(J, dtype=np.float64).reshape(-1, 3, 3, 3)
+    v[..., 1] = 2. * v[..., 1] - .5 * (v[..., 0] + v[..., 2])
+    v[..., 1, :] = 2. * v[..., 1, :] - .5 * (v[..., 0, :] + v[..., 2, :])
+    v[:, 1] = 2. * v[:, 1] - .5 * (v[:, 0] + v[:, 2])
+    return v.reshape(-1, 27)
+
+
+_LAGRANGE_TO_POWER = np.array([[1., -3., 2.], [0., 4., -4.], [0., -1., 2.]])   # L_a(t) = sum_i M[a, i] t^i
+
+
+def _lagrange3(t):
+    t = np.asarray(t, dtype=np.float64)
+    return np.stack([2 * (t - .5) * (t - 1), -4 * t * (t - 1), 2 * t * (t - .5)], axis=-1)
+
+
+def _tri_eval(C, x, dx=(0, 0, 0)):
+    """sum C[k,j,i] d^dz z^k d^dy y^j d^dx x^i at points x (n, 3) (xyz); C (n, 27) monomial coefficients."""
+    def pw(t, d):
+        one, zero = np.ones_like(t), np.zeros_like(t)
+        return [np.stack([one, t, t * t], -1), np.stack([zero, one, 2 * t], -1), np.stack([zero, zero, 2 * one], -1)][d]
+    X, Y, Z = pw(x[:, 0], dx[0]), pw(x[:, 1], dx[1]), pw(x[:, 2], dx[2])
+    row = (Z[:, :, None, None] * Y[:, None, :, None] * X[:, None, None, :]).reshape(len(x), 27)
+    return np.sum(C * row, axis=1)
+
+
+def face_interior_minima(J27, starts=4, iterations=30):
+    """solvers/jd_affine.py:130 (T69): min over the 9^3 grid of the cell's triquadratic J and of a bounded projected
+    Newton descent (30 iterations, <= 40 halvings, strict decrease) from the `starts` lowest grid points."""
+    J27 = np.asarray(J27, dtype=np.float64).reshape(-1, 27)
+    n = len(J27)
+    M = _LAGRANGE_TO_POWER
+    C = np.einsum("ncba,ck,bj,ai->nkji", J27.reshape(-1, 3, 3, 3), M, M, M).reshape(-1, 27)
+    t9 = np.linspace(0., 1., 9)
+    L = _lagrange3(t9)
+    V9 = np.kron(L, np.kron(L, L))                                  # (729, 27), z-major rows
+    G9 = np.array([(x, y, z) for z in t9 for y in t9 for x in t9])
+    grid_values = J27 @ V9.T
+    order = np.argsort(grid_values, axis=1, kind="stable")[:, :starts]
+    best = grid_values.min(axis=1)
+    found = np.full(n, np.inf)
+    for s in range(order.shape[1]):
+        x = G9[order[:, s]].copy()
+        f = _tri_eval(C, x)
+        live = np.ones(n, dtype=bool)
+        for _ in range(iterations):
+            idx = np.flatnonzero(live)
+            if idx.size == 0:
+                break
+            xi, Ci = x[idx], C[idx]
+            g = np.stack([_tri_eval(Ci, xi, (1, 0, 0)), _tri_eval(Ci, xi, (0, 1, 0)), _tri_eval(Ci, xi, (0, 0, 1))], -1)
+            H = np.empty((idx.size, 3, 3))
+            for a, b in ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)):
+                d = [0, 0, 0]
+                d[a] += 1
+                d[b] += 1
+                H[:, a, b] = H[:, b, a] = _tri_eval(Ci, xi, tuple(d))
+            free = ~(((xi <= 0.) & (g > 0)) | ((xi >= 1.) & (g < 0)))
+            gf = np.where(free, g, 0.)
+            Hf = H * free[:, :, None] * free[:, None, :] + np.eye(3) * (~free)[:, :, None]
+            w, Q = np.linalg.eigh(Hf)
+            scale = np.maximum(1., np.abs(w).max(axis=1))
+            ok = np.all(w > 1e-12 * scale[:, None], axis=1)
+            newton = -np.einsum("nij,nj,nkj,nk->ni", Q, 1 / np.where(ok[:, None], w, 1.), Q, gf)
+            d = np.where(ok[:, None], newton, -gf / scale[:, None])
+            step, done = np.ones(idx.size), np.zeros(idx.size, dtype=bool)
+            for _ in range(40):
+                xt = np.clip(xi + step[:, None] * d, 0., 1.)
+                ft = _tri_eval(Ci, xt)
+                take = (~done) & (ft < f[idx])
+                x[idx[take]], f[idx[take]] = xt[take], ft[take]
+                done |= take
+                step = np.where(done, step, .5 * step)
+                if done.all():
+                    break
+            live[idx[~done]] = False
+        found = np.minimum(found, f)
+    return np.minimum(best, found)
+
+
+def node_min_jd(problem, u, extension_activation=None):
+    """T62 node measure (solvers/jd_affine.py:205); with extension_activation, the T69/T73 face/interior extension
+    on candidate cells (jd_affine.py:173 extend_minima).  Returns (node, number of candidate cells)."""
     g = problem.grid
     J = geometry(local(u, g), ops(g, "closed27_uniform"))[2]
     m = closed27_cell_minima(J)
+    ncand = 0
+    if extension_activation is not None:
+        cand = np.flatnonzero(to_bernstein27(J).min(axis=1) < np.minimum(m, extension_activation))
+        ncand = cand.size
+        if ncand:
+            m[cand] = np.minimum(m[cand], face_interior_minima(J[cand]))
     node = np.full(g.shape, np.inf).ravel()
     nodes = cell_nodes(g)
     for a in range(8):
         np.minimum.at(node, nodes[:, a], m)
-    return node.reshape(g.shape)
+    node = node.reshape(g.shape)
+    return node if extension_activation is None else (node, ncand)
 
 
 def affine_factors(node, activation=.25, floor=1e-12):

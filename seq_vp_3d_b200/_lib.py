@@ -48,6 +48,11 @@ class Weights(ctypes.Structure):
     _fields_ = [("lam", D), ("mu", D), ("nu", D), ("kappa", D), ("activation", D), ("delta", D)]
 
 
+class PreParams(ctypes.Structure):
+    _fields_ = [(n, D) for n in ("mu", "alpha", "kappa", "j0", "lr", "cap", "sigma_grad", "sigma_field", "beta1",
+                                 "beta2", "eps")]
+
+
 # name -> argtypes (restype int)
 SIGNATURES = {
     "svp_last_error": [ctypes.c_char_p, ctypes.c_size_t],
@@ -72,11 +77,19 @@ SIGNATURES = {
     "svp_energy": [P, P, P, P, P, P],
     "svp_energy_difference": [P, P, P, P, P, P, P],
     "svp_trial_energy": [P, P, P, P, P, P, P, P, P, P],
+    "svp_pre_energy_grad": [P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, D, D, D, P, D, D, D, D, P, P, P],
+    "svp_pre_level": [P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, D, D, D, P, ctypes.c_int32, ctypes.c_int32,
+                      P, P, P, P, P, P, P],
+    "svp_image_downsample": [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P, ctypes.c_int32, ctypes.c_int32,
+                             ctypes.c_int32, P],
+    "svp_field_prolong": [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P, ctypes.c_int32, ctypes.c_int32,
+                          ctypes.c_int32, P, P, P],
     "svp_gradient": [P, P, P, P, I32, P, P],
     "svp_outer_gradients": [P, P, P, P, P, P, P, P],
     "svp_ggn_diagonal": [P, P, P, P, P],
     "svp_ggn_hvp": [P, P, P, P, P, P],
     "svp_node_min_jd": [P, P, P, P],
+    "svp_node_min_jd_extended": [P, P, ctypes.c_double, P, P, P],
     "svp_jd_root": [P, P, P, D, P, P, P],
     "svp_poisson_apply": [P, D, D, I32, P, P, D, P, P],
     "svp_dot": [P, P, I64, P, P],

@@ -21,7 +21,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=o
 FLAGS = {
     "certificate.cu": ["-fmad=false"],
 }
-SOURCES = ["capi.cu", "certificate.cu", "q1.cu", "dst.cu", "vec.cu", "pair.cu"]
+SOURCES = ["capi.cu", "certificate.cu", "q1.cu", "dst.cu", "vec.cu", "pair.cu", "preopt.cu"]
 
 
 def _headers():

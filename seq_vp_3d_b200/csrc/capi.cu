@@ -84,6 +84,37 @@ KernelTimer::~KernelTimer() {
     t.stop.push_back(e);
 }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created;
+            if ((e = cudaMemPoolCreate(&created, &props)) != cudaSuccess) return e;
+            uint64_t keep = 64ull << 20;     // keep up to 64 MB mapped between calls
+            cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+            g_pools[dev] = created;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+}
+
+cudaError_t scratch_free(void *ptr, cudaStream_t stream) { return cudaFreeAsync(ptr, stream); }
+
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 int fail(int code, const std::string &msg) {

@@ -845,9 +845,9 @@ extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const 
     long long warps = n < (long long)kSMs * 8 ? n : (long long)kSMs * 8;
     warps = (warps + 3) / 4 * 4;  // whole blocks of 4 warps
     char *scratch = nullptr;
-    SVP_CUDA(cudaMallocAsync((void **)&scratch, warp_scratch_bytes(slots) * warps, s));
+    SVP_CUDA(scratch_alloc((void **)&scratch, warp_scratch_bytes(slots) * warps, s));
     int rc = classify_launch(c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, warps, slots, s);
-    cudaError_t e = cudaFreeAsync(scratch, s);
+    cudaError_t e = scratch_free(scratch, s);
     if (rc != SVP_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
     return SVP_OK;

@@ -19,6 +19,7 @@ struct svp_pair {
     long long partial_cap = 0;                // in dd entries
     double *result = nullptr;                 // small device result area (64 doubles)
     long long *counter = nullptr;             // small device counters (8)
+    long long *cand = nullptr;                // candidate cells of the T69/T73 node JD extension (ncell)
     // DST-I Poisson metric
     double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
     int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)

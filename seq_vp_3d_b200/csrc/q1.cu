@@ -774,8 +774,12 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
 }
 
 // ============================================================================================== node JD measure
+// ext_act > 0 (T69/T73): cells whose closed27 Bernstein coefficients allow a value below min(m_c, ext_act) are
+// appended to cand (order of arrival; each is then estimated independently, so the order does not matter).
 __global__ void __launch_bounds__(CS) cell_min_jd_kernel(Q1Const q, const double *__restrict__ u,
-                                                         double *__restrict__ m) {
+                                                         double *__restrict__ m, double ext_act,
+                                                         unsigned long long *__restrict__ ncand,
+                                                         long long *__restrict__ cand) {
     extern __shared__ double smem[];
     double *J = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -808,6 +812,286 @@ __global__ void __launch_bounds__(CS) cell_min_jd_kernel(Q1Const q, const double
             if (a > 0 && b < 0 && -b < 2 * a) mn = fmin(mn, j0 - b * b / (4 * a));
         }
         m[c] = mn;
+        if (ext_act > 0.) {
+            // closed27 values -> Bernstein coefficients in place: per axis x, y, z the middle entry becomes
+            // 2 b - (a + c) / 2 (bernstein_barrier.py:26 to_bernstein)
+#pragma unroll 1
+            for (int axis = 0; axis < 3; axis++) {
+                const int st = axis == 0 ? 1 : (axis == 1 ? 3 : 9);
+#pragma unroll 1
+                for (int l = 0; l < 9; l++) {
+                    const int o = axis == 0 ? 3 * l : (axis == 1 ? (l / 3) * 9 + (l % 3) : l);
+                    const double v0 = J[o * T], v1 = J[(o + st) * T], v2 = J[(o + 2 * st) * T];
+                    J[(o + st) * T] = 2. * v1 - .5 * (v0 + v2);
+                }
+            }
+            double bmin = J[0];
+#pragma unroll 1
+            for (int k = 1; k < 27; k++) bmin = fmin(bmin, J[k * T]);
+            if (bmin < fmin(mn, ext_act)) cand[atomicAdd(ncand, 1ull)] = c;
+        }
+    }
+}
+
+// ---- T69/T73 face/interior estimate mu_c on candidate cells (solvers/jd_affine.py:45-150) ----
+// J on a cell is triquadratic; mu_c = min of its values on the 9^3 grid {0, 1/8, .., 1}^3 and of a bounded Newton
+// descent (30 iterations, halving backtracking <= 40, strict decrease only) from the 4 lowest grid points (stable
+// order).  A value J attains, so an estimate for the metric, never a bound.  One warp per candidate cell.
+struct Tri {
+    double c[27];    // monomial coefficients C[k][j][i] of z^k y^j x^i
+};
+// NumPy's add-reduce order for a contiguous length-27 axis (eight accumulators; jd_affine_compiled.py:_sum27)
+__device__ __forceinline__ double sum27(const double *a) {
+    double r[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) r[i] = a[i];
+#pragma unroll
+    for (int b = 8; b < 24; b += 8)
+#pragma unroll
+        for (int i = 0; i < 8; i++) r[i] += a[b + i];
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    res += a[24];
+    res += a[25];
+    res += a[26];
+    return 0.0 + res;
+}
+// sum C[k][j][i] (Z_k Y_j) X_i
+__device__ __forceinline__ double tri_e(const Tri &T, const double Z[3], const double Y[3], const double X[3]) {
+    double tmp[27];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const double zy = Z[k] * Y[j];
+#pragma unroll
+            for (int i = 0; i < 3; i++) tmp[9 * k + 3 * j + i] = T.c[9 * k + 3 * j + i] * (zy * X[i]);
+        }
+    return sum27(tmp);
+}
+__device__ __forceinline__ void tri_powers(double t, double P[3][3]) {
+    P[0][0] = 1.; P[0][1] = t; P[0][2] = t * t;
+    P[1][0] = 0.; P[1][1] = 1.; P[1][2] = 2. * t;
+    P[2][0] = 0.; P[2][1] = 0.; P[2][2] = 2.;
+}
+__device__ __forceinline__ double tri_value(const Tri &T, const double x[3]) {
+    double px[3][3], py[3][3], pz[3][3];
+    tri_powers(x[0], px); tri_powers(x[1], py); tri_powers(x[2], pz);
+    return tri_e(T, pz[0], py[0], px[0]);
+}
+__device__ __forceinline__ double clip01(double v) {
+    if (v != v) return v;
+    const double w = v > 0. ? v : 0.;
+    return w < 1. ? w : 1.;
+}
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations: A = Q diag(w) Q^T (columns of Q).
+__device__ void sym3_eigen(double A[3][3], double w[3], double Q[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) Q[i][j] = i == j ? 1. : 0.;
+#pragma unroll 1
+    for (int sweep = 0; sweep < 64; sweep++) {
+        const double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
+        const double dia = fabs(A[0][0]) + fabs(A[1][1]) + fabs(A[2][2]);
+        if (off == 0. || off <= 1e-300 + 1e-18 * dia) break;
+#pragma unroll 1
+        for (int pq = 0; pq < 3; pq++) {
+            const int p = pq == 2 ? 1 : 0, qq = pq == 0 ? 1 : 2;
+            const double apq = A[p][qq];
+            if (apq == 0.) continue;
+            // rotation zeroing A[p][q] (symmetric Schur decomposition of the 2x2 block)
+            const double tau = (A[qq][qq] - A[p][p]) / (2. * apq);
+            const double t = (tau >= 0. ? 1. : -1.) / (fabs(tau) + sqrt(1. + tau * tau));
+            const double cs = 1. / sqrt(1. + t * t), sn = t * cs;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {     // A <- A J
+                const double akp = A[k][p], akq = A[k][qq];
+                A[k][p] = cs * akp - sn * akq;
+                A[k][qq] = sn * akp + cs * akq;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; k++) {     // A <- J^T A
+                const double apk = A[p][k], aqk = A[qq][k];
+                A[p][k] = cs * apk - sn * aqk;
+                A[qq][k] = sn * apk + cs * aqk;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; k++) {     // Q <- Q J
+                const double qkp = Q[k][p], qkq = Q[k][qq];
+                Q[k][p] = cs * qkp - sn * qkq;
+                Q[k][qq] = sn * qkp + cs * qkq;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) w[i] = A[i][i];
+}
+// jd_affine.py:_bounded_newton for one start; returns the lowest value reached
+__device__ double bounded_newton(const Tri &T, double x[3], double best) {
+#pragma unroll 1
+    for (int it = 0; it < 30; it++) {
+        double px[3][3], py[3][3], pz[3][3];
+        tri_powers(x[0], px); tri_powers(x[1], py); tri_powers(x[2], pz);
+        double g[3], H[3][3];
+        g[0] = tri_e(T, pz[0], py[0], px[1]);
+        g[1] = tri_e(T, pz[0], py[1], px[0]);
+        g[2] = tri_e(T, pz[1], py[0], px[0]);
+        H[0][0] = tri_e(T, pz[0], py[0], px[2]);
+        H[1][1] = tri_e(T, pz[0], py[2], px[0]);
+        H[2][2] = tri_e(T, pz[2], py[0], px[0]);
+        H[0][1] = H[1][0] = tri_e(T, pz[0], py[1], px[1]);
+        H[0][2] = H[2][0] = tri_e(T, pz[1], py[0], px[1]);
+        H[1][2] = H[2][1] = tri_e(T, pz[1], py[1], px[0]);
+        bool free_[3];
+        double gf[3], Hf[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            free_[a] = !((x[a] <= 0. && g[a] > 0.) || (x[a] >= 1. && g[a] < 0.));
+            gf[a] = free_[a] ? g[a] : 0.;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                Hf[a][b] = (free_[a] && free_[b]) ? H[a][b] : (a == b && !free_[a] ? 1. : 0.);
+        double w[3], Q[3][3];
+        sym3_eigen(Hf, w, Q);
+        const double scale = fmax(1., fmax(fabs(w[0]), fmax(fabs(w[1]), fabs(w[2]))));
+        const bool ok = w[0] > 1e-12 * scale && w[1] > 1e-12 * scale && w[2] > 1e-12 * scale;
+        double d[3];
+        if (ok) {
+            double proj[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) proj[j] = (Q[0][j] * gf[0] + Q[1][j] * gf[1] + Q[2][j] * gf[2]) / w[j];
+#pragma unroll
+            for (int i = 0; i < 3; i++) d[i] = -(Q[i][0] * proj[0] + Q[i][1] * proj[1] + Q[i][2] * proj[2]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; i++) d[i] = -gf[i] / scale;
+        }
+        double step = 1.;
+        bool done = false;
+#pragma unroll 1
+        for (int bt = 0; bt < 40; bt++) {
+            double xt[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) xt[a] = clip01(x[a] + step * d[a]);
+            const double ft = tri_value(T, xt);
+            if (ft < best) {
+                x[0] = xt[0]; x[1] = xt[1]; x[2] = xt[2];
+                best = ft;
+                done = true;
+                break;
+            }
+            step = .5 * step;
+        }
+        if (!done) break;       // no strict decrease: converged to rounding (or stuck)
+    }
+    return best;
+}
+
+__device__ __forceinline__ double lagrange3(int a, double t) {
+    return a == 0 ? 2. * (t - .5) * (t - 1.) : (a == 1 ? -4. * t * (t - 1.) : 2. * t * (t - .5));
+}
+// (value, index) lexicographic order: the stable ascending sort of the grid values (NaN last)
+__device__ __forceinline__ bool vi_less(double v, int i, double w, int j) {
+    if (v < w) return true;
+    if (w != w && v == v) return true;
+    if (v == w || (v != v && w != w)) return i < j;
+    return false;
+}
+
+__global__ void __launch_bounds__(128) jd_extension_kernel(Q1Const q, const double *__restrict__ u,
+                                                           const unsigned long long *__restrict__ ncand,
+                                                           const long long *__restrict__ cand,
+                                                           double *__restrict__ m) {
+    __shared__ double sJ[4][27];
+    __shared__ Tri sT[4];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long n = (long long)*ncand;
+    for (long long w = blockIdx.x * 4LL + wib; w < n; w += (long long)gridDim.x * 4) {
+        const long long c = cand[w];
+        double E[3][4][3];
+        load_edges(u, cell_node0(c, q), q, E);
+        if (lane == 0)
+            sweep<true>(E, q, [&](int p, int, int, int, const double (&V)[3][3]) { sJ[wib][p] = det_only(V); });
+        __syncwarp();
+        // monomial coefficients C[k][j][i] = sum_cba J[c][b][a] M[c][k] M[b][j] M[a][i], M the Lagrange-to-power map
+        if (lane < 27) {
+            const double M[3][3] = {{1., -3., 2.}, {0., 4., -4.}, {0., -1., 2.}};
+            const int k = lane / 9, j = (lane / 3) % 3, i = lane % 3;
+            double acc = 0.;
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+                        acc += sJ[wib][9 * cc + 3 * b + a] * (M[cc][k] * (M[b][j] * M[a][i]));
+            sT[wib].c[lane] = acc;
+        }
+        __syncwarp();
+        // 9^3 grid values (z-major, x fastest), each lane keeping its 4 lowest in stable order
+        double tv[4];
+        int ti[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) { tv[r] = __longlong_as_double(0x7FF8000000000000LL); ti[r] = 0x7FFFFFFF; }
+        for (int pnt = lane; pnt < 729; pnt += 32) {
+            const int ix = pnt % 9, iy = (pnt / 9) % 9, iz = pnt / 81;
+            const double tx = .125 * ix, ty = .125 * iy, tz = .125 * iz;
+            double val = 0.;
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+                        val += sJ[wib][9 * cc + 3 * b + a] * (lagrange3(cc, tz) * (lagrange3(b, ty) * lagrange3(a, tx)));
+            if (vi_less(val, pnt, tv[3], ti[3])) {
+                int pos = 3;
+                while (pos > 0 && vi_less(val, pnt, tv[pos - 1], ti[pos - 1])) {
+                    tv[pos] = tv[pos - 1]; ti[pos] = ti[pos - 1];
+                    pos--;
+                }
+                tv[pos] = val; ti[pos] = pnt;
+            }
+        }
+        // butterfly merge of the lanes' sorted lists
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            double ov[4];
+            int oi[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                ov[r] = __shfl_xor_sync(0xFFFFFFFFu, tv[r], o);
+                oi[r] = __shfl_xor_sync(0xFFFFFFFFu, ti[r], o);
+            }
+            double nv[4];
+            int ni[4];
+            int a = 0, b = 0;
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                if (vi_less(tv[a], ti[a], ov[b], oi[b])) { nv[r] = tv[a]; ni[r] = ti[a]; a++; }
+                else { nv[r] = ov[b]; ni[r] = oi[b]; b++; }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) { tv[r] = nv[r]; ti[r] = ni[r]; }
+        }
+        // bounded Newton from the 4 lowest grid points, lanes 0..3
+        double found = __longlong_as_double(0x7FF0000000000000LL);
+        if (lane < 4) {
+            const int s0 = lane == 0 ? ti[0] : (lane == 1 ? ti[1] : (lane == 2 ? ti[2] : ti[3]));
+            double x[3] = {.125 * (s0 % 9), .125 * ((s0 / 9) % 9), .125 * (s0 / 81)};
+            found = bounded_newton(sT[wib], x, tri_value(sT[wib], x));
+        }
+#pragma unroll
+        for (int o = 2; o; o >>= 1) found = fmin(found, __shfl_xor_sync(0xFFFFFFFFu, found, o));
+        if (lane == 0) {
+            const double mu = fmin(tv[0], found);       // grid minimum and the Newton descents
+            const double mc = m[c];
+            m[c] = (mu < mc || mu != mu) ? mu : mc;     // np.minimum
+        }
+        __syncwarp();
     }
 }
 
@@ -1236,13 +1520,36 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
     return SVP_OK;
 }
 
-extern "C" int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream) {
+extern "C" int svp_node_min_jd_extended(svp_pair *p, const double *u, double extension_activation, double *node,
+                                        int64_t *candidates, void *stream) {
     SVP_REQUIRE(p && u && node, "svp_node_min_jd: null argument");
+    SVP_REQUIRE(!(extension_activation < 0.) && extension_activation == extension_activation,
+                "svp_node_min_jd: extension activation must be >= 0 (0: no extension)");
     cudaStream_t s = (cudaStream_t)stream;
-    { svp::KernelTimer _t("cell_min_jd_kernel", s); SVP_LAUNCH(cell_min_jd_kernel<<<slice_blocks(p), CS, slice_bytes(27), s>>>(p->q, u, p->cellbuf)); }
+    const bool ext = extension_activation > 0.;
+    if (ext && !p->cand) SVP_CUDA(cudaMalloc((void **)&p->cand, sizeof(long long) * p->q.ncell));
+    unsigned long long *ncand = (unsigned long long *)(p->counter + 4);
+    if (ext) SVP_CUDA(cudaMemsetAsync(ncand, 0, sizeof(unsigned long long), s));
+    { svp::KernelTimer _t("cell_min_jd_kernel", s); SVP_LAUNCH(cell_min_jd_kernel<<<slice_blocks(p), CS, slice_bytes(27), s>>>(p->q, u, p->cellbuf, ext ? extension_activation : 0., ncand, p->cand)); }
+    if (ext) {
+        svp::KernelTimer _t("jd_extension_kernel", s);
+        SVP_LAUNCH(jd_extension_kernel<<<148 * 4, 128, 0, s>>>(p->q, u, ncand, p->cand, p->cellbuf));
+    }
     SVP_LAUNCH(node_min_kernel<<<node_blocks(p->q.nnode), 256, 0, s>>>(p->q, p->cellbuf, node));
     SVP_LAUNCH_CHECK("node_min_jd");
+    if (candidates) {
+        unsigned long long nc = 0;
+        if (ext) {
+            SVP_CUDA(cudaMemcpyAsync(&nc, ncand, sizeof nc, cudaMemcpyDeviceToHost, s));
+            SVP_CUDA(cudaStreamSynchronize(s));
+        }
+        *candidates = (int64_t)nc;
+    }
     return SVP_OK;
+}
+
+extern "C" int svp_node_min_jd(svp_pair *p, const double *u, double *node, void *stream) {
+    return svp_node_min_jd_extended(p, u, 0., node, nullptr, stream);
 }
 
 extern "C" int svp_jd_root(svp_pair *p, const double *u, const double *pvec, double limit, double *root,

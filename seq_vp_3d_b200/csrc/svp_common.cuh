@@ -12,6 +12,10 @@ void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t err, const char *what);
 void count_launch();
+// Stream-ordered scratch from the library's own memory pool on the current device (it keeps its memory between
+// calls, so the small per-call reductions never map new pages): cudaMallocFromPoolAsync / cudaFreeAsync.
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream);
+cudaError_t scratch_free(void *ptr, cudaStream_t stream);
 
 // Opt-in per-kernel CUDA-event timing (svp_timers_enable): a scope records an event pair on its stream around the
 // launches inside it; svp_timer_read resolves and sums them.

@@ -163,14 +163,14 @@ extern "C" int svp_bb2_dots(const double *theta, const double *theta_old, const 
     cudaStream_t s = (cudaStream_t)stream;
     unsigned nb = blocks_for(n, 256, 4);
     dd *part = nullptr;
-    SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * 4 * nb + 4 * sizeof(double), s));
+    SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * 4 * nb + 4 * sizeof(double), s));
     double *res = (double *)(part + 4 * nb);
     SVP_LAUNCH(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
     SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res));
     cudaError_t le = cudaGetLastError();
     double host[4];
     cudaError_t ce = cudaMemcpyAsync(host, res, sizeof host, cudaMemcpyDeviceToHost, s);
-    cudaError_t fe = cudaFreeAsync(part, s);
+    cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "bb2 kernels");
     if (ce != cudaSuccess) return cuda_fail(ce, "bb2 copy");
     if (fe != cudaSuccess) return cuda_fail(fe, "bb2 free");
@@ -183,13 +183,13 @@ extern "C" int svp_max_abs_diff(const double *a, const double *b, int64_t n, dou
     SVP_REQUIRE(a && b && out2 && n >= 0, "svp_max_abs_diff: invalid argument");
     cudaStream_t s = (cudaStream_t)stream;
     long long *keys = nullptr;
-    SVP_CUDA(cudaMallocAsync((void **)&keys, 2 * sizeof(long long), s));
+    SVP_CUDA(scratch_alloc((void **)&keys, 2 * sizeof(long long), s));
     cudaError_t e0 = cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s);
     SVP_LAUNCH(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
     cudaError_t le = cudaGetLastError();
     long long host[2] = {0, 0};
     cudaError_t ce = cudaMemcpyAsync(host, keys, sizeof host, cudaMemcpyDeviceToHost, s);
-    cudaError_t fe = cudaFreeAsync(keys, s);
+    cudaError_t fe = scratch_free(keys, s);
     if (e0 != cudaSuccess) return cuda_fail(e0, "max abs init");
     if (le != cudaSuccess) return cuda_fail(le, "max_abs_diff_kernel");
     if (ce != cudaSuccess) return cuda_fail(ce, "max abs copy");
@@ -204,14 +204,14 @@ extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out,
     cudaStream_t s = (cudaStream_t)stream;
     unsigned nb = blocks_for(n, 256, 4);
     dd *part = nullptr;
-    SVP_CUDA(cudaMallocAsync((void **)&part, sizeof(dd) * nb + sizeof(double), s));
+    SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * nb + sizeof(double), s));
     double *res = (double *)(part + nb);
     SVP_LAUNCH(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
     SVP_LAUNCH(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res));
     cudaError_t le = cudaGetLastError();
     double host = 0.;
     cudaError_t ce = cudaMemcpyAsync(&host, res, sizeof host, cudaMemcpyDeviceToHost, s);
-    cudaError_t fe = cudaFreeAsync(part, s);
+    cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "dot kernels");
     if (ce != cudaSuccess) return cuda_fail(ce, "dot copy");
     if (fe != cudaSuccess) return cuda_fail(fe, "dot free");
@@ -247,14 +247,14 @@ extern "C" int svp_step_bound(const svp_grid *g, const double *u, const double *
     SVP_REQUIRE(grid_ok(g) && u && pvec && bound, "svp_step_bound: invalid argument");
     cudaStream_t s = (cudaStream_t)stream;
     long long *best = nullptr;
-    SVP_CUDA(cudaMallocAsync((void **)&best, sizeof(long long), s));
+    SVP_CUDA(scratch_alloc((void **)&best, sizeof(long long), s));
     long long init = kKeyPosInf, host = 0;
     cudaError_t e1 = cudaMemcpyAsync(best, &init, sizeof init, cudaMemcpyHostToDevice, s);
     SVP_LAUNCH(step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
                                                                     g->y0, g->z0, u, pvec, best));
     cudaError_t le = cudaGetLastError();
     cudaError_t e2 = cudaMemcpyAsync(&host, best, sizeof host, cudaMemcpyDeviceToHost, s);
-    cudaError_t e3 = cudaFreeAsync(best, s);
+    cudaError_t e3 = scratch_free(best, s);
     if (e1 != cudaSuccess) return cuda_fail(e1, "step bound init");
     if (le != cudaSuccess) return cuda_fail(le, "step_bound_kernel");
     if (e2 != cudaSuccess) return cuda_fail(e2, "step bound copy");

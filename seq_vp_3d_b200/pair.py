@@ -122,9 +122,18 @@ class DevicePair:
         _lib.call("svp_ggn_hvp", self._h, ptr(u), ptr(image_grad), ptr(to_device(p)), ptr(out), stream_ptr(stream))
         return out
 
-    def node_min_jd(self, u, stream=None):
+    def node_min_jd(self, u, extension_activation=None, stats=None, stream=None):
+        """Node JD measure (T62); with extension_activation, the T69/T73 face/interior extension on candidate cells
+        (stats, a dict, then receives the candidate count)."""
         out = self.node()
-        _lib.call("svp_node_min_jd", self._h, ptr(u), ptr(out), stream_ptr(stream))
+        if extension_activation is None:
+            _lib.call("svp_node_min_jd", self._h, ptr(u), ptr(out), stream_ptr(stream))
+            return out
+        cand = ctypes.c_int64()
+        _lib.call("svp_node_min_jd_extended", self._h, ptr(u), float(extension_activation), ptr(out),
+                  ctypes.byref(cand) if stats is not None else None, stream_ptr(stream))
+        if stats is not None:
+            stats["candidates"] = stats.get("candidates", 0) + int(cand.value)
         return out
 
     def jd_root(self, u, p, limit, stream=None):

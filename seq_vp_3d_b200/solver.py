@@ -20,6 +20,7 @@ import numpy as np
 import torch
 
 from . import certificate as cert_mod
+from .device import to_device
 from .pair import DevicePair, axpy, dot
 
 EPS = float(np.finfo(float).eps)
@@ -27,6 +28,9 @@ InvalidTrial = namedtuple("InvalidTrial", "reason detail count")
 FAST_COSINE_SCREEN = 1e-6
 JD_AFFINE_FLOOR = 1e-12
 T62_POLICY = "image_shift_ggn_equilibrated_jd_affine_v1"
+T69_POLICY = "image_shift_ggn_equilibrated_jd_affine_v2"   # T62 + face/interior extension once a certificate was uncertain
+T73_POLICY = "image_shift_ggn_equilibrated_jd_affine_v3"   # T62 + face/interior extension always (the native default)
+METRIC_POLICIES = (T62_POLICY, T69_POLICY, T73_POLICY)
 
 
 @dataclass(frozen=True)
@@ -41,10 +45,14 @@ class PGConfig3D:
     step_tol: float = 1e-12
     stall_steps: int = 5
     jd_step_safety: float = .9
-    metric_policy: str = T62_POLICY
+    metric_policy: str = T73_POLICY
     shift_factor: float = 1.
     jd_affine_activation: float = .25
     resolution_exit: bool = True
+
+    def __post_init__(self):
+        if self.metric_policy not in METRIC_POLICIES:
+            raise ValueError(f"metric_policy: one of {METRIC_POLICIES}")
 
 
 @dataclass(frozen=True)
@@ -120,7 +128,7 @@ class Registration:
         self.delta = self.config.delta
         self.weights = dict(lam=lam, mu=mu, nu=nu, kappa=kappa)
         self.activation = activation
-        u_ref = np.zeros(grid.shape + (3,)) if u_ref is None else u_ref
+        u_ref = torch.zeros(grid.shape + (3,), dtype=torch.float64, device="cuda") if u_ref is None else u_ref
         self.pair = DevicePair(grid, fixed, moving, u_ref, lam=lam, mu=mu, nu=nu, kappa=kappa,
                                activation=activation, delta=self.delta)
         self.certifier = cert_mod.certifier(grid, self.config)
@@ -128,7 +136,7 @@ class Registration:
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0
         self._reference_version = 0
-        ref = self.certify(torch.as_tensor(np.ascontiguousarray(u_ref, dtype=np.float64), device="cuda"))
+        ref = self.certify(to_device(u_ref))
         if ref.status != "certified_feasible":
             raise ValueError(f"u_ref: not certified feasible ({ref.reason})")
         self.reference_certificate = ref
@@ -214,7 +222,7 @@ class Registration:
         _lib.call("svp_max_abs_diff", ptr(candidate), ptr(theta), candidate.numel(), out, stream_ptr())
         return float(out[0] / max(self.length, out[1]))
 
-    def metric(self, base, config):
+    def metric(self, base, config, memory=None):
         """(a, b, S~) of the T62 conservative metric (solvers/poisson_gradient.py:400 _pg_metric_inverse)."""
         import ctypes
         from . import _lib
@@ -227,7 +235,10 @@ class Registration:
         inv_h2 = sum(1 / h ** 2 for h in self.grid.spacing)
         m = self.grid.omega * (a + b * (8 / 9) * inv_h2)
         d = self.pair.ggn_diagonal(base.u, base.image_grad)
-        node = self.pair.node_min_jd(base.u)
+        # solvers/poisson_gradient.py:486: T73 always, T69 once this level has seen an undetermined certificate
+        extend = config.metric_policy == T73_POLICY or (
+            config.metric_policy == T69_POLICY and memory is not None and memory.uncertain > 0)
+        node = self.pair.node_min_jd(base.u, config.jd_affine_activation if extend else None)
         scale = self.pair.free()
         bad = ctypes.c_int64()
         _lib.call("svp_pg_scale", self.pair._h, ptr(d), ptr(node), float(m), float(config.jd_affine_activation),
@@ -421,7 +432,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
             return finish("max_iterations", "ACCEPTED_STEP_BUDGET")
         if metric is None:
             try:
-                metric = reg.metric(base, config)
+                metric = reg.metric(base, config, memory)
             except FloatingPointError as exc:
                 return finish("nonfinite_evaluation", str(exc))
         a, b, scale = metric

@@ -18,7 +18,7 @@ q1.npz            spline coefficients/samples, energy terms, gradients, GGN diag
                   stable energy reductions of a small problem (residuals.py, linearization.py, poisson.py,
                   energy_comparison.py).
 
-Run:  python tests/golden/make_golden.py [--reference PATH] [--only certificate,cells,q1]
+Run:  python tests/golden/make_golden.py [--reference PATH] [--only certificate,cells,q1,seq,t73,preopt]
 """
 import argparse
 import os
@@ -334,7 +334,7 @@ def make_cells(out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", default="certificate,cells,q1,seq")
+    ap.add_argument("--only", default="certificate,cells,q1,seq,t73,preopt")
     args = ap.parse_args()
     import_reference(args.reference)
     only = set(args.only.split(","))
@@ -348,6 +348,12 @@ def main():
     if "seq" in only:
         from q1_golden import make_seq     # the full certified proximal loop on a small pair
         make_seq(HERE)
+    if "t73" in only:
+        from q1_golden import make_t73     # node JD measure with the T69/T73 face/interior extension
+        make_t73(HERE)
+    if "preopt" in only:
+        from preopt_golden import make_preopt   # the float32 pyramid pre-optimizer and its pieces
+        make_preopt(HERE)
 
 
 if __name__ == "__main__":

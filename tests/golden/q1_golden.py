@@ -137,8 +137,10 @@ def make_q1(out):
           "roots", data["jd_root0"], data["jd_root1"])
 
 
-def make_seq(out):
-    """The reference's full certified proximal loop (CPU, default PG route with the T62 metric) on a small pair."""
+def make_seq(out, policy="image_shift_ggn_equilibrated_jd_affine_v1", name="seq.npz", seed=3, outer_steps=6,
+             shape=(14, 13, 12), pair=None, theta0=None):
+    """The reference's full certified proximal loop (CPU, default PG route; T62 metric or the native T73) on a small
+    pair."""
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
     from seq_vp_3d_b200.synthetic import blob_pair, default_weights
@@ -147,8 +149,8 @@ def make_seq(out):
     from jd_curl.three_d.feasibility import PrescreenCertificateConfig
     from jd_curl.three_d.sequential import solve_sequential, SequentialReuseConfig3D
     from jd_curl.three_d.solvers.poisson_gradient import ConservativePGConfig3D
-    shape, spacing = (14, 13, 12), (1.0, 1.0, 1.0)
-    fixed, moving, u_gt = blob_pair(shape, spacing, seed=3)
+    spacing = (1.0, 1.0, 1.0)
+    fixed, moving, u_gt = blob_pair(shape, spacing, seed=seed) if pair is None else pair
     nz, ny, nx = shape
     grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=1., hy=1., hz=1., unit="mm")
     w = default_weights(shape, spacing)
@@ -157,10 +159,10 @@ def make_seq(out):
     problem = make_problem(grid=grid, fixed_image=fixed, moving_image=moving, u_ref=np.zeros(grid.shape + (3,)),
                            weights=weights, certificate_config=config, barrier_location="closed27_uniform",
                            barrier_activation=.05)
-    inner = ConservativePGConfig3D(max_iterations=5, metric_policy="image_shift_ggn_equilibrated_jd_affine_v1",
-                                   resolution_exit=True)
-    outer = SequentialReuseConfig3D(max_iterations=6, eta0=.01)
-    res = solve_sequential(problem, np.zeros(3 * grid.n_free_scalar), solver="pg", inner_config=inner, config=outer)
+    inner = ConservativePGConfig3D(max_iterations=5, metric_policy=policy, resolution_exit=True)
+    outer = SequentialReuseConfig3D(max_iterations=outer_steps, eta0=.01)
+    theta = np.zeros(3 * grid.n_free_scalar) if theta0 is None else theta0(grid)
+    res = solve_sequential(problem, theta, solver="pg", inner_config=inner, config=outer)
     rows = []
     attempts = []
     for k, row in enumerate(res.history):
@@ -172,9 +174,9 @@ def make_seq(out):
                              np.nan if a["actual_reduction"] is None else a["actual_reduction"],
                              a["energy_base"], a["gradient_norm"]])
     e = res.final_state.energy
-    np.savez_compressed(os.path.join(out, "seq.npz"), fixed=fixed, moving=moving, spacing=np.array(spacing),
+    np.savez_compressed(os.path.join(out, name), fixed=fixed, moving=moving, spacing=np.array(spacing),
                         weights=np.array([w["lam"], w["mu"], w["nu"], w["kappa"]]),
-                        status=np.array(res.status), reason=np.array(res.reason),
+                        status=np.array(res.status), reason=np.array(res.reason), theta0=theta,
                         theta=res.final_state.theta, rows=np.array(rows, dtype=np.float64),
                         attempts=np.array(attempts, dtype=np.float64),
                         inner_status=np.array([r["inner_status"] for r in res.history]),
@@ -182,5 +184,64 @@ def make_seq(out):
                         final_energy=np.array([e.image, e.proximity, e.jd, e.curl, e.barrier]),
                         gf=np.array([res.GF_initial, res.GF_final, res.GF_threshold]),
                         counts=np.array([res.counts["outer_accepted"], res.counts["inner_calls"]]))
-    print("seq.npz:", res.status, res.reason, "outer", res.counts["outer_accepted"], "rows", len(rows),
+    print(name + ":", res.status, res.reason, "outer", res.counts["outer_accepted"], "rows", len(rows),
           "attempts", len(attempts), "final E", e.total)
+
+
+def make_t73(out):
+    """Node JD measure with and without the T69/T73 face/interior extension (solvers/jd_affine.py:205) on a seeded
+    field with strongly curved J, so that the extension lowers many cells' minima; plus the seeded pair's full
+    loop with the native T73 metric policy."""
+    from jd_curl.three_d.grid import make_grid_3d
+    from jd_curl.three_d.problem import Weights3D, make_problem
+    from jd_curl.three_d.feasibility import PrescreenCertificateConfig
+    from jd_curl.three_d.solvers.jd_affine import node_min_jd
+    shape, spacing = (16, 15, 14), (1.0, 0.9, 1.1)
+    AMP = 0.2
+    nz, ny, nx = shape
+    grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=spacing[0], hy=spacing[1], hz=spacing[2], unit="mm")
+    fixed, moving = seeded_images(shape, 11)
+    rng = np.random.default_rng(12)
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    u = np.zeros(shape + (3,))
+    for r, h in enumerate(spacing):
+        for _ in range(4):
+            k = rng.uniform(0.6, 1.6, size=3)
+            u[..., r] += AMP * h * np.sin(k[0] * xx + k[1] * yy + k[2] * zz + rng.uniform(0, 6))
+    u[[0, -1]] = 0.; u[:, [0, -1]] = 0.; u[:, :, [0, -1]] = 0.
+    u = np.ascontiguousarray(u)
+    weights = Weights3D(lam=0.1, mu=0.03, nu=0.03, kappa=0.002)
+    config = PrescreenCertificateConfig(delta=0., max_depth=48, max_boxes=255, tile_size=65536, fallback_workers=2)
+    problem = make_problem(grid=grid, fixed_image=fixed, moving_image=moving, u_ref=np.zeros(grid.shape + (3,)),
+                           weights=weights, certificate_config=config, barrier_location="closed27_uniform",
+                           barrier_activation=.05)
+
+    class State:
+        pass
+    st = State()
+    st.u = u
+    node62 = node_min_jd(problem, st)
+    stats = {}
+    node73 = node_min_jd(problem, st, extension_activation=0.25, stats=stats)
+    inner = node73[1:-1, 1:-1, 1:-1] < node62[1:-1, 1:-1, 1:-1]
+    np.savez_compressed(os.path.join(out, "t73.npz"), u=u, spacing=np.array(spacing), node62=node62, node73=node73,
+                        candidates=np.array(stats.get("candidates", 0)), lowered=np.array(stats.get("lowered_cells", 0)),
+                        lowered_any=np.array(stats.get("lowered_cells_any", 0)))
+    print("t73.npz: candidates", stats.get("candidates", 0), "lowered", stats.get("lowered_cells", 0), "lowered nodes",
+          int(inner.sum()), "min", float(node62.min()), float(node73.min()))
+    # the full loop with the native T73 policy on a pair whose ground truth compresses strongly (min JD >= 0.15),
+    # so the face/interior extension meets candidate cells during the solve
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    from seq_vp_3d_b200 import synthetic as syn
+    pshape, psp = (16, 15, 14), (1., 1., 1.)
+    prng = np.random.default_rng(21)
+    fixed2 = syn.blob_pair(pshape, psp, seed=21)[0]
+    u_gt = syn._ground_truth(pshape, psp, prng, 3, 2.5, 2.2, 0.15)
+    moving2 = syn._resample(fixed2, u_gt, psp)
+    def start(grid):       # a certified start with a strong local compression (J ~ 0.12 near the centre)
+        from jd_curl.three_d.boundary import restrict_free
+        u0 = compressed_field(grid, 0.88, (8, 7, 7), 22, amp=0.05)
+        return restrict_free(u0, grid)
+    make_seq(out, policy="image_shift_ggn_equilibrated_jd_affine_v3", name="seq_t73.npz", outer_steps=8,
+             shape=pshape, pair=(fixed2, moving2, u_gt), theta0=start)

@@ -79,6 +79,23 @@ def test_poisson_and_metric(fx):
     assert rel(-scale * Q.poisson_apply(g, a, b, scale * d["grad/total"]), d["direction"]) < TOL
 
 
+def test_node_measure_face_interior_extension():
+    """The oracle's T69/T73 estimator against the reference's node_min_jd(extension_activation=.25) (t73.npz)."""
+    d = np.load(os.path.join(GOLDEN, "t73.npz"))
+    u = d["u"]
+    nz, ny, nx = u.shape[:3]
+    g = Q.make_grid((nz, ny, nx), tuple(d["spacing"]))
+    z = np.zeros((nz, ny, nx))
+    P = Q.make_problem(g, z, z, np.zeros_like(u), .1, .03, .03, .002)
+    inner = (slice(1, -1),) * 3
+    n62 = Q.node_min_jd(P, u)
+    n73, ncand = Q.node_min_jd(P, u, .25)
+    assert rel(n62[inner], d["node62"][inner]) < TOL
+    assert ncand == int(d["candidates"]) and np.sum(n73[inner] < n62[inner]) > 0
+    err = np.abs(n73[inner] - d["node73"][inner]) / np.abs(d["node73"][inner])
+    assert err.max() < 1e-12, err.max()
+
+
 def test_node_measure_and_root(fx):
     d, g, P, w1, ig1 = fx
     n62 = Q.node_min_jd(P, d["u1"])

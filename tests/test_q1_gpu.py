@@ -123,6 +123,31 @@ def test_node_measure_and_root(gold):
         assert (r is None and np.isnan(root)) or abs(r - root) <= 1e-12 * root, (r, root)
 
 
+def test_node_measure_face_interior_extension():
+    """T69/T73 (solvers/jd_affine.py:173 extend_minima): the same candidate cells as the reference and its node
+    measure within 1e-12 on a field whose extension lowers several cells' minima (metric estimate, not a bound)."""
+    from seq_vp_3d_b200.grid import make_grid_3d
+    from seq_vp_3d_b200.pair import DevicePair
+    d = np.load(os.path.join(GOLDEN, "t73.npz"))
+    u = d["u"]
+    nz, ny, nx = u.shape[:3]
+    hx, hy, hz = (float(v) for v in d["spacing"])
+    grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=hx, hy=hy, hz=hz, unit="mm")
+    z = np.zeros((nz, ny, nx))
+    P = DevicePair(grid, z, z, np.zeros_like(u), lam=.1, mu=.03, nu=.03, kappa=.002)
+    ud = dev(u)
+    ref62, ref73 = d["node62"], d["node73"]
+    inner = (slice(1, -1),) * 3
+    assert np.sum(ref73[inner] < ref62[inner]) > 0          # the extension matters on this field
+    got62 = P.node_min_jd(ud).cpu().numpy()
+    assert rel(got62[inner], ref62[inner]) < TOL
+    stats = {}
+    got73 = P.node_min_jd(ud, 0.25, stats).cpu().numpy()
+    assert stats["candidates"] == int(d["candidates"])
+    err = np.abs(got73[inner] - ref73[inner]) / np.maximum(np.abs(ref73[inner]), 1e-300)
+    assert err.max() <= 1e-12, err.max()
+
+
 # ------------------------------------------------------------------------------------------ larger, vs the oracle
 def seeded_problem(shape, spacing, seed):
     rng = np.random.default_rng(seed)

@@ -1,5 +1,6 @@
 """End-to-end: the device-resident certified proximal loop against the reference's own solve_sequential on the same
-seeded pair (golden seq.npz: default conservative PG route with the T62 metric, 6 outer steps).
+seeded pairs (golden seq.npz: conservative PG route with the T62 metric, 6 outer steps from u = 0; seq_t73.npz: the
+native T73 metric, 8 outer steps from a certified start with a strong local compression).
 
 Discrete decisions (statuses, accepted flags, attempt counts) must be identical; the continuous trajectory agrees
 to the precision that the 1e-12 kernel parity propagates through 30 BB2 steps."""
@@ -14,16 +15,25 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def run():
+# (fixture, metric policy, outer steps): the T62 metric from u = 0, and the native T73 metric from a certified start
+# with a strong local compression
+CASES = [("seq.npz", "image_shift_ggn_equilibrated_jd_affine_v1", 6),
+         ("seq_t73.npz", "image_shift_ggn_equilibrated_jd_affine_v3", 8)]
+
+
+@pytest.fixture(scope="module", params=CASES, ids=["t62", "t73"])
+def run(request):
     from seq_vp_3d_b200.grid import make_grid_3d
     from seq_vp_3d_b200.solver import PGConfig3D, Registration, SequentialConfig3D, solve_sequential
-    d = np.load(os.path.join(GOLDEN, "seq.npz"))
+    name, policy, outer = request.param
+    d = np.load(os.path.join(GOLDEN, name))
     nz, ny, nx = d["fixed"].shape
     grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=1., hy=1., hz=1., unit="mm")
     lam, mu, nu, kappa = (float(v) for v in d["weights"])
     reg = Registration(grid, d["fixed"], d["moving"], lam=lam, mu=mu, nu=nu, kappa=kappa)
-    res = solve_sequential(reg, config=SequentialConfig3D(max_iterations=6), inner_config=PGConfig3D())
+    theta0 = torch.from_numpy(np.ascontiguousarray(d["theta0"])).cuda() if "theta0" in d.files else None
+    res = solve_sequential(reg, theta0, config=SequentialConfig3D(max_iterations=outer),
+                           inner_config=PGConfig3D(metric_policy=policy))
     return d, res
 
 
