@@ -26,7 +26,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "certified pairs/hour @160x192x224 (plain FP64 form, 1 GPU per pair)"
+METRIC = "certified pairs/hour @160x192x224 ({} form, 1 B200 per pair)"
 SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -42,7 +42,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--outer", type=int, default=200, help="outer steps per registration (config 2: 200)")
-    ap.add_argument("--preopt", action=argparse.BooleanOptionalAction, default=False,
+    ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
+                    help="plain: float64 throughout; mixed: float32 search direction (gradient, GGN diagonal, DST-I) "
+                         "with float64 energies, decisions and certificate")
+    ap.add_argument("--preopt", action=argparse.BooleanOptionalAction, default=True,
                     help="config-2 route: float32 8/4/2/1 pyramid pre-optimizer + certified transfer before the "
                          "native steps")
     ap.add_argument("--shape", default="160,192,224", help="nx,ny,nz")
@@ -151,6 +154,9 @@ def kernel_counts(shape):
         "cell_grad_kernel": (2 * 24 * nn + 192 * nc, c("cell_grad_kernel")),
         "gather_kernel": (192 * nc + nn * (24 + 24 + 8 + 8 + 24) + 3 * 8 * nf, None),
         "cell_ggn_diag_kernel": (24 * nn + 192 * nc, c("cell_ggn_diag_kernel")),
+        # mixed form: the same float64 inputs, float32 locals out (the FLOP counts above are float32 operations here)
+        "cell_grad32_kernel": (2 * 24 * nn + 96 * nc, None),
+        "cell_ggn_diag32_kernel": (24 * nn + 96 * nc, None),
         "edge_hull_kernel": (24 * nn + 9 * nc, None),
         # trial u, base u, base warped, fixed, u_ref in; warped (+ gradient) out; coefficients cache resident
         "warp_trial_kernel_grad": ((24 + 24 + 8 + 8 + 24 + 8 + 24) * nn, None),
@@ -236,7 +242,8 @@ def main():
     config = {"workload": f"head phantom pair {nx}x{ny}x{nz} (x fastest), 1 mm, float64, certified proximal loop "
                           f"{start} {args.outer} outer steps x 5 PG steps (T73 metric)",
               "grid_nodes": nx * ny * nz, "outer_steps": args.outer, "inner_steps": 5,
-              "form": "plain FP64", "l2_policy": "inputs larger than L2 (6.9M-node fields, 55-165 MB each)"}
+              "form": "plain FP64" if args.form == "plain" else "mixed (float32 direction, float64 decisions)",
+              "l2_policy": "inputs larger than L2 (6.9M-node fields, 55-165 MB each)"}
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -249,7 +256,7 @@ def main():
             v, cores, samples, _ = cpu_baseline(shape, fixed, moving, weights, args.cpu_slab, args.outer)
             vals.append(v)
         value = float(np.mean(vals))
-        line = dict(metric=METRIC, value=value, unit="pairs/hour", n_gpus=args.gpus, steps=args.steps,
+        line = dict(metric=METRIC.format(args.form), value=value, unit="pairs/hour", n_gpus=args.gpus, steps=args.steps,
                     warmup=args.warmup, ms_per_step=3.6e6 / value, higher_is_better=True, scaling="weak",
                     vs_baseline=None, dtype="f64", data="synthetic", config=config, impl="reference",
                     cpu_baseline=dict(value=value, unit="pairs/hour", cores=cores, kind="port", sample=samples),
@@ -279,10 +286,11 @@ def main():
     def step(f, m):
         if args.preopt:
             from seq_vp_3d_b200.preopt import register_pair
-            res, _ = register_pair(f, m, grid, weights, outer=args.outer, inner_config=inner_cfg)
+            res, _ = register_pair(f, m, grid, weights, outer=args.outer, inner_config=inner_cfg,
+                                   precision=args.form)
             reg = None
         else:
-            reg = Registration(grid, f, m, **weights)
+            reg = Registration(grid, f, m, **weights, precision=args.form)
             res = solve_sequential(reg, config=outer_cfg, inner_config=inner_cfg)
         if not res.certified:
             raise RuntimeError(f"registration ended without a certified state: {res.status}")
@@ -382,7 +390,7 @@ def main():
             v, cores, sample, _ = cpu_baseline(shape, fixed, moving, weights, args.cpu_slab, args.outer)
             cpu = dict(value=v, unit="pairs/hour", cores=cores, kind="port", sample=sample)
         r = results[-1]
-        line = dict(metric=METRIC, value=value, unit="pairs/hour", n_gpus=world, steps=args.steps,
+        line = dict(metric=METRIC.format(args.form), value=value, unit="pairs/hour", n_gpus=world, steps=args.steps,
                     warmup=args.warmup, ms_per_step=seconds * 1e3 / args.steps, higher_is_better=True,
                     scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", config=config,
                     e2e=dict(value=e2e_value, unit="pairs/hour", h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h),

@@ -153,6 +153,16 @@ int svp_pair_destroy(svp_pair *p);
 /* Copy of the spline coefficients (nz, ny, nx) into out (device). */
 int svp_pair_spline_coefficients(const svp_pair *p, double *out, void *stream);
 
+/* Arithmetic of the search direction.  SVP_PRECISION_PLAIN (the default): everything in float64, the reference's
+ * binary64 results within 1e-12.  SVP_PRECISION_MIXED: svp_gradient, svp_outer_gradients, svp_ggn_diagonal and
+ * svp_poisson_apply compute in float32 (edge differences, grad u, cofactors, fluxes, the folded DST-I passes), with
+ * the localized barrier evaluated in float64 wherever the float32 J comes within 1e-3 of the activation, and their
+ * sums and outputs in float64; energies, stable differences, the certificate, the node JD measure and the JD root
+ * stay float64, so every acceptance decision is taken on float64 values (the north star's mixed form). */
+#define SVP_PRECISION_PLAIN 0
+#define SVP_PRECISION_MIXED 1
+int svp_pair_set_precision(svp_pair *p, int32_t precision);
+
 /* Moving image at X + u (and its physical xyz gradient when image_grad != NULL) at every node.
  * Replaces interpolation.py:72 sample_points / :109 sample_value_gradient and backends/spline.py:81 TorchSpline.
  * warped: (nz, ny, nx); image_grad: (nz, ny, nx, 3).  The caller certifies the sampling domain first. */
@@ -247,6 +257,15 @@ int svp_bb2_dots(const double *theta, const double *theta_old, const double *g, 
 /* out2 (host) = (max |a - b|, max |b|), NaN-propagating (fast_checks.py:120 _max_abs_diff, :111 _max_abs):
  * the inputs of the relative step max|candidate - theta| / max(L, max|theta|) (solvers/common.py:70 step_ratio). */
 int svp_max_abs_diff(const double *a, const double *b, int64_t n, double *out2, void *stream);
+
+/* Deferred forms of svp_dot, svp_bb2_dots, svp_max_abs_diff and svp_step_bound: the same values written to device
+ * memory (out_dev: 1, 4, 2 and 1 doubles), stream-ordered and without synchronisation, so that a caller gathers the
+ * scalars of a whole step with one copy. */
+int svp_dot_dev(const double *a, const double *b, int64_t n, double *out_dev, void *stream);
+int svp_bb2_dots_dev(const double *theta, const double *theta_old, const double *g, const double *g_old,
+                     const double *p_old, const double *pvec, int64_t n, double *out4_dev, void *stream);
+int svp_max_abs_diff_dev(const double *a, const double *b, int64_t n, double *out2_dev, void *stream);
+int svp_step_bound_dev(const svp_grid *g, const double *u, const double *pvec, double *bound_dev, void *stream);
 
 /* Image-curvature shift alpha = factor * mean over free nodes of (q/omega) |grad I(X+u)|^2 / 3
  * (solvers/poisson_gradient.py:269 image_curvature_shift).  alpha: host. */

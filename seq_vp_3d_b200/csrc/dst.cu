@@ -117,56 +117,62 @@ __global__ void __launch_bounds__(256) gemm_right_kernel(const double *__restric
 // output rows of one parity need only half the columns, against the folded input u_k = x_k + x_(n-1-k) (even i;
 // u_mid = x_mid when n is odd) or v_k = x_k - x_(n-1-k) (odd i): half the FLOPs of the dense product.  The folded
 // half matrices are stored per parity, H0 (ceil(n/2) x ceil(n/2)) then H1 (floor(n/2) x floor(n/2)), row-major.
-struct HalfDst {
-    const double *h0, *h1;
+// TC: the arithmetic type of a pass (double in the plain form, float in the mixed form); inputs and outputs may be
+// either (the mixed form reads the float64 right-hand side and writes the float64 direction).
+template <class TC>
+struct HalfDstT {
+    const TC *h0, *h1;
     int n, k0, k1;     // n, ceil(n/2), floor(n/2)
 };
-__device__ __forceinline__ double folded(const double *__restrict__ x, const double *__restrict__ pre, long long a,
-                                         long long b, int g) {
-    double xa = pre ? pre[a] * x[a] : x[a];
-    if (a == b) return xa;
-    double xb = pre ? pre[b] * x[b] : x[b];
-    return g ? xa - xb : xa + xb;
+using HalfDst = HalfDstT<double>;
+// the fold is formed in float64 and rounded once to the pass's type
+template <class TC, class TI>
+__device__ __forceinline__ TC folded(const TI *__restrict__ x, const double *__restrict__ pre, long long a,
+                                     long long b, int g) {
+    double xa = pre ? pre[a] * (double)x[a] : (double)x[a];
+    if (a == b) return (TC)xa;
+    double xb = pre ? pre[b] * (double)x[b] : (double)x[b];
+    return (TC)(g ? xa - xb : xa + xb);
 }
 
 // Left pass: C[b][i][w] = sum_k S[i][k] X[b][k][w] (rows of length W, stride ldx, batch stride bs).  blockIdx.y
 // enumerates the 64-row tiles of parity 0, then of parity 1.  EPI 1 divides by den[flat % per], EPI 2 multiplies
 // by sign * post[flat] (the same operation order as the separate elementwise passes).
-template <int EPI>
-__global__ void __launch_bounds__(256) dst_left_kernel(HalfDst D, const double *__restrict__ X, long long W,
-                                                       long long ldx, long long bs, double *__restrict__ C,
+template <int EPI, class TC, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long W,
+                                                       long long ldx, long long bs, TO *__restrict__ C,
                                                        const double *__restrict__ den, long long per,
                                                        const double *__restrict__ post, double sign) {
-    __shared__ double sM[TK][TM + 1];
-    __shared__ double sX[TK][TN];
+    __shared__ TC sM[TK][TM + 1];
+    __shared__ TC sX[TK][TN];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     const int t0 = (D.k0 + TM - 1) / TM;
     const int g = blockIdx.y < t0 ? 0 : 1;
     const int rows = g ? D.k1 : D.k0, K = rows;
-    const double *H = g ? D.h1 : D.h0;
+    const TC *H = g ? D.h1 : D.h0;
     const int i0 = (g ? blockIdx.y - t0 : blockIdx.y) * TM;
     const long long b = blockIdx.z;
     const long long w0 = (long long)blockIdx.x * TN;
-    const double *Xb = X + b * bs;
-    double acc[4][4] = {};
+    const TI *Xb = X + b * bs;
+    TC acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += TK) {
         for (int e = threadIdx.x; e < TK * TM; e += 256) {
             int kk = e % TK, ii = e / TK;
             int i = i0 + ii, k = k0 + kk;
-            sM[kk][ii] = (i < rows && k < K) ? H[(long long)i * K + k] : 0.;
+            sM[kk][ii] = (i < rows && k < K) ? H[(long long)i * K + k] : TC(0);
         }
         for (int e = threadIdx.x; e < TK * TN; e += 256) {
             int ww = e % TN, kk = e / TN;
             long long w = w0 + ww;
             int k = k0 + kk;
-            sX[kk][ww] = (k < K && w < W) ? folded(Xb, nullptr, (long long)k * ldx + w,
-                                                   (long long)(D.n - 1 - k) * ldx + w, g)
-                                          : 0.;
+            sX[kk][ww] = (k < K && w < W) ? folded<TC>(Xb, nullptr, (long long)k * ldx + w,
+                                                       (long long)(D.n - 1 - k) * ldx + w, g)
+                                          : TC(0);
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < TK; kk++) {
-            double a[4], x[4];
+            TC a[4], x[4];
 #pragma unroll
             for (int r = 0; r < 4; r++) a[r] = sM[kk][ty + 16 * r];
 #pragma unroll
@@ -188,44 +194,45 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDst D, const double *
             long long w = w0 + tx + 16 * c;
             if (w >= W) continue;
             long long o = b * bs + i * ldx + w;
-            double v = acc[r][c];
+            double v = (double)acc[r][c];
             if (EPI == 1) v = v / den[o % per];
             if (EPI == 2) v = sign * (post[o] * v);
-            C[o] = v;
+            C[o] = (TO)v;
         }
     }
 }
 
 // Right pass over contiguous rows of length n: C[r][i] = sum_k X[r][k] S[i][k]; pre (optional) scales X first.
-__global__ void __launch_bounds__(256) dst_right_kernel(HalfDst D, const double *__restrict__ X, long long R,
-                                                        const double *__restrict__ pre, double *__restrict__ C) {
-    __shared__ double sX[TK][TM + 1];
-    __shared__ double sM[TK][TN + 1];
+template <class TC, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long R,
+                                                        const double *__restrict__ pre, TO *__restrict__ C) {
+    __shared__ TC sX[TK][TM + 1];
+    __shared__ TC sM[TK][TN + 1];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     const int t0 = (D.k0 + TN - 1) / TN;
     const int g = blockIdx.y < t0 ? 0 : 1;
     const int cols = g ? D.k1 : D.k0, K = cols;
-    const double *H = g ? D.h1 : D.h0;
+    const TC *H = g ? D.h1 : D.h0;
     const int i0 = (g ? blockIdx.y - t0 : blockIdx.y) * TN;
     const long long r0 = (long long)blockIdx.x * TM;
     const int n = D.n;
-    double acc[4][4] = {};
+    TC acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += TK) {
         for (int e = threadIdx.x; e < TK * TM; e += 256) {
             int kk = e % TK, rr = e / TK;
             long long r = r0 + rr;
             int k = k0 + kk;
-            sX[kk][rr] = (r < R && k < K) ? folded(X, pre, r * n + k, r * n + (n - 1 - k), g) : 0.;
+            sX[kk][rr] = (r < R && k < K) ? folded<TC>(X, pre, r * n + k, r * n + (n - 1 - k), g) : TC(0);
         }
         for (int e = threadIdx.x; e < TK * TN; e += 256) {
             int kk = e % TK, ii = e / TK;
             int i = i0 + ii, k = k0 + kk;
-            sM[kk][ii] = (i < cols && k < K) ? H[(long long)i * K + k] : 0.;
+            sM[kk][ii] = (i < cols && k < K) ? H[(long long)i * K + k] : TC(0);
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < TK; kk++) {
-            double a[4], m[4];
+            TC a[4], m[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) a[q] = sX[kk][ty + 16 * q];
 #pragma unroll
@@ -244,7 +251,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDst D, const double 
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             int ii = i0 + tx + 16 * c;
-            if (ii < cols) C[r * n + 2 * ii + g] = acc[q][c];
+            if (ii < cols) C[r * n + 2 * ii + g] = (TO)acc[q][c];
         }
     }
 }
@@ -294,27 +301,31 @@ std::vector<double> dst1_matrix(int n);
 
 // One DST-I pass along `axis` of (3, n2, n1, n0) fields with the folded half matrices; see dst_left_kernel for
 // pre / EPI.
-static int dst_pass(const svp_pair *p, int axis, const double *in, double *out, const double *pre, int epi,
-                    double sign, const double *post, cudaStream_t s) {
+template <class TC, class TI, class TO>
+static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const double *pre, int epi, double sign,
+                    const double *post, cudaStream_t s) {
     const long long n0 = p->q.fx, n1 = p->q.fy, n2 = p->q.fz;
-    HalfDst D{p->dst_half[axis], p->dst_half[axis] + (size_t)((p->dst_n[axis] + 1) / 2) * ((p->dst_n[axis] + 1) / 2),
-              p->dst_n[axis], (p->dst_n[axis] + 1) / 2, p->dst_n[axis] / 2};
+    const TC *h = nullptr;
+    if constexpr (sizeof(TC) == 8) h = p->dst_half[axis];
+    else h = p->dst_half32[axis];
+    HalfDstT<TC> D{h, h + (size_t)((p->dst_n[axis] + 1) / 2) * ((p->dst_n[axis] + 1) / 2), p->dst_n[axis],
+                   (p->dst_n[axis] + 1) / 2, p->dst_n[axis] / 2};
     const unsigned tiles = (unsigned)(div_up(D.k0, TM) + div_up(D.k1, TM));
     const long long nf = p->q.nfree;
     if (axis == 0) {
         SVP_REQUIRE(epi == 0, "dst_pass: x pass has no epilogue");
         long long R = 3 * n2 * n1;
         dim3 grid((unsigned)div_up(R, TM), tiles);
-        { svp::KernelTimer _t("dst_right_kernel", s); SVP_LAUNCH(dst_right_kernel<<<grid, 256, 0, s>>>(D, in, R, pre, out)); }
+        { svp::KernelTimer _t("dst_right_kernel", s); SVP_LAUNCH((dst_right_kernel<TC, TI, TO><<<grid, 256, 0, s>>>(D, in, R, pre, out))); }
     } else {
         SVP_REQUIRE(!pre, "dst_pass: pre-scale only on the x pass");
         long long W = axis == 1 ? n0 : n1 * n0;
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
         dim3 grid((unsigned)div_up(W, TN), tiles, (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
-        if (epi == 0) SVP_LAUNCH(dst_left_kernel<0><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.));
-        else if (epi == 1) SVP_LAUNCH(dst_left_kernel<1><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.));
-        else SVP_LAUNCH(dst_left_kernel<2><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign));
+        if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
+        else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
+        else SVP_LAUNCH((dst_left_kernel<2, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
     }
     SVP_LAUNCH_CHECK("dst pass");
     return SVP_OK;
@@ -353,6 +364,9 @@ int pair_dst_setup(svp_pair *p) {
         std::vector<double> H = dst1_half((int)f[k]);
         SVP_CUDA(cudaMalloc((void **)&p->dst_half[k], sizeof(double) * H.size()));
         SVP_CUDA(cudaMemcpy(p->dst_half[k], H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice));
+        std::vector<float> H32(H.begin(), H.end());      // the mixed form's matrices (rounded once)
+        SVP_CUDA(cudaMalloc((void **)&p->dst_half32[k], sizeof(float) * H32.size()));
+        SVP_CUDA(cudaMemcpy(p->dst_half32[k], H32.data(), sizeof(float) * H32.size(), cudaMemcpyHostToDevice));
         p->dst_n[k] = (int)f[k];
     }
     SVP_CUDA(cudaMalloc((void **)&p->dst_tmp, sizeof(double) * 2 * 3 * p->q.nfree));
@@ -407,15 +421,29 @@ extern "C" int svp_poisson_apply(svp_pair *p, double a, double b, int32_t metric
     int rc = set_denominator(p, a, b, metric, s);
     if (rc) return rc;
     const long long n3 = 3 * p->q.nfree;
+    if (p->precision == SVP_PRECISION_MIXED) {
+        // the same six passes in float32 (the fold and the epilogues formed in float64, rounded once)
+        float *f0 = (float *)p->dst_tmp, *f1 = f0 + n3;
+        if ((rc = dst_pass<float>(p, 0, rhs, f0, scale, 0, 1., nullptr, s))) return rc;
+        if ((rc = dst_pass<float>(p, 1, f0, f1, nullptr, 0, 1., nullptr, s))) return rc;
+        if ((rc = dst_pass<float>(p, 2, f1, f0, nullptr, 1, 1., nullptr, s))) return rc;
+        if ((rc = dst_pass<float>(p, 0, f0, f1, nullptr, 0, 1., nullptr, s))) return rc;
+        if ((rc = dst_pass<float>(p, 1, f1, f0, nullptr, 0, 1., nullptr, s))) return rc;
+        if (scale) return dst_pass<float>(p, 2, f0, out, nullptr, 2, sign, scale, s);
+        if ((rc = dst_pass<float>(p, 2, f0, out, nullptr, 0, 1., nullptr, s))) return rc;
+        SVP_LAUNCH(scale_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(out, nullptr, sign, n3, out));
+        SVP_LAUNCH_CHECK("scale_kernel");
+        return SVP_OK;
+    }
     double *t0 = p->dst_tmp, *t1 = p->dst_tmp + n3;
     // scale -> DST(x, y, z) -> / den -> DST(x, y, z) -> sign * scale; the elementwise steps ride in the passes
-    if ((rc = dst_pass(p, 0, rhs, t0, scale, 0, 1., nullptr, s))) return rc;
-    if ((rc = dst_pass(p, 1, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
-    if ((rc = dst_pass(p, 2, t1, t0, nullptr, 1, 1., nullptr, s))) return rc;
-    if ((rc = dst_pass(p, 0, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
-    if ((rc = dst_pass(p, 1, t1, t0, nullptr, 0, 1., nullptr, s))) return rc;
-    if (scale) return dst_pass(p, 2, t0, out, nullptr, 2, sign, scale, s);
-    if ((rc = dst_pass(p, 2, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
+    if ((rc = dst_pass<double>(p, 0, rhs, t0, scale, 0, 1., nullptr, s))) return rc;
+    if ((rc = dst_pass<double>(p, 1, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
+    if ((rc = dst_pass<double>(p, 2, t1, t0, nullptr, 1, 1., nullptr, s))) return rc;
+    if ((rc = dst_pass<double>(p, 0, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
+    if ((rc = dst_pass<double>(p, 1, t1, t0, nullptr, 0, 1., nullptr, s))) return rc;
+    if (scale) return dst_pass<double>(p, 2, t0, out, nullptr, 2, sign, scale, s);
+    if ((rc = dst_pass<double>(p, 2, t0, t1, nullptr, 0, 1., nullptr, s))) return rc;
     unsigned eb = blocks_for(n3, 256, 8);
     SVP_LAUNCH(scale_kernel<<<eb, 256, 0, s>>>(t1, nullptr, sign, n3, out));
     SVP_LAUNCH_CHECK("scale_kernel");

@@ -23,6 +23,8 @@ struct svp_pair {
     // DST-I Poisson metric
     double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
     int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)
+    float *dst_half32[3] = {nullptr, nullptr, nullptr};     // the same, rounded to float32 (mixed form)
+    int precision = 0;                                      // SVP_PRECISION_PLAIN or SVP_PRECISION_MIXED
     double *dst_tmp = nullptr;                          // 2 * 3 * nfree scratch
     double *den = nullptr;                              // (nz-2, ny-2, nx-2) omega (a + b lambda)
     double den_a = -1, den_b = -1;

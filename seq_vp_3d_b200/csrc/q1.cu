@@ -187,11 +187,13 @@ __device__ __forceinline__ void load_edges(const double *__restrict__ u, long lo
     load_cell(u, n0, q, v);
     cell_edges(v, E);
 }
-__device__ __forceinline__ void zero_slice(double *sl, int T, int n) {
-    for (int k = 0; k < n; k++) sl[k * T] = 0.;
+template <class R>
+__device__ __forceinline__ void zero_slice(R *sl, int T, int n) {
+    for (int k = 0; k < n; k++) sl[k * T] = R(0);
 }
 // S[j][s][t][r] += f[r][j] at point (ix, iy, iz): j = 0 -> (iy, iz), j = 1 -> (ix, iz), j = 2 -> (ix, iy)
-__device__ __forceinline__ void add_flux(double *sl, int T, int ix, int iy, int iz, const double f[3][3]) {
+template <class R>
+__device__ __forceinline__ void add_flux(R *sl, int T, int ix, int iy, int iz, const R f[3][3]) {
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         sl[((iy * 3 + iz) * 3 + r) * T] += f[r][0];
@@ -200,26 +202,27 @@ __device__ __forceinline__ void add_flux(double *sl, int T, int ix, int iy, int 
     }
 }
 // adjoint of the edge interpolation (scatter_edges) reading S from the slice
-__device__ __forceinline__ void scatter_slice(const double *sl, int T, const double n[3], const double m[3],
-                                              const double ih[3], double L[8][3]) {
+template <class R, class C>
+__device__ __forceinline__ void scatter_slice(const R *sl, int T, const C n[3], const C m[3], const double ih[3],
+                                              R L[8][3]) {
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-            double e[4] = {0., 0., 0., 0.};
+            R e[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
             for (int s = 0; s < 3; s++) {
-                double t0 = 0., t1 = 0.;
+                R t0 = R(0), t1 = R(0);
 #pragma unroll
                 for (int t = 0; t < 3; t++) {
-                    double v = sl[(27 * j + (s * 3 + t) * 3 + r) * T] * ih[j];
-                    t0 += m[t] * v;
-                    t1 += n[t] * v;
+                    R v = sl[(27 * j + (s * 3 + t) * 3 + r) * T] * (R)ih[j];
+                    t0 += (R)m[t] * v;
+                    t1 += (R)n[t] * v;
                 }
-                e[0] += m[s] * t0;
-                e[1] += n[s] * t0;
-                e[2] += m[s] * t1;
-                e[3] += n[s] * t1;
+                e[0] += (R)m[s] * t0;
+                e[1] += (R)n[s] * t0;
+                e[2] += (R)m[s] * t1;
+                e[3] += (R)n[s] * t1;
             }
 #pragma unroll
             for (int k = 0; k < 4; k++) {
@@ -291,8 +294,8 @@ __global__ void __launch_bounds__(CS) cell_energy_kernel(Q1Const q, const double
 }
 
 // Per-cell vertex values -> SoA locals L[(a * 3 + r) * ncell + c].
-__device__ __forceinline__ void store_locals(double *__restrict__ L, long long c, long long ncell,
-                                             const double v[8][3]) {
+template <class R>
+__device__ __forceinline__ void store_locals(R *__restrict__ L, long long c, long long ncell, const R v[8][3]) {
 #pragma unroll
     for (int a = 0; a < 8; a++)
 #pragma unroll
@@ -385,8 +388,9 @@ struct GatherSpec {
 };
 
 // Free node (z, y, x): sum of the 8 cells' vertex values in fixed order a = 0..7, plus node terms.
-__global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, const double *__restrict__ L1,
-                                                     const double *__restrict__ L2, const double *__restrict__ u,
+template <class LT>
+__global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, const LT *__restrict__ L1,
+                                                     const LT *__restrict__ L2, const double *__restrict__ u,
                                                      const double *__restrict__ uref,
                                                      const double *__restrict__ warped,
                                                      const double *__restrict__ fixed,
@@ -403,8 +407,8 @@ __global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, co
             long long c = ((z - (a >> 2)) * q.cy + (y - ((a >> 1) & 1))) * q.cx + (x - (a & 1));
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                if (L1) s1[r] += L1[(long long)(a * 3 + r) * q.ncell + c];
-                if (L2) s2[r] += L2[(long long)(a * 3 + r) * q.ncell + c];
+                if (L1) s1[r] += (double)L1[(long long)(a * 3 + r) * q.ncell + c];
+                if (L2) s2[r] += (double)L2[(long long)(a * 3 + r) * q.ncell + c];
             }
         }
 #pragma unroll
@@ -550,7 +554,8 @@ __global__ void __launch_bounds__(CS) cell_ggn_hvp_kernel(Q1Const q, const doubl
 }
 
 // node part of the GGN: q |b|^2 + lambda q (diagonal) or q b (b . v) + lambda q v (action)
-__global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const double *__restrict__ L,
+template <class LT>
+__global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const LT *__restrict__ L,
                                                        const double *__restrict__ image_grad,
                                                        const double *__restrict__ vv, double *__restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
@@ -563,7 +568,7 @@ __global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const double *
         for (int a = 0; a < 8; a++) {
             long long c = ((z - (a >> 2)) * q.cy + (y - ((a >> 1) & 1))) * q.cx + (x - (a & 1));
 #pragma unroll
-            for (int r = 0; r < 3; r++) s[r] += L[(long long)(a * 3 + r) * q.ncell + c];
+            for (int r = 0; r < 3; r++) s[r] += (double)L[(long long)(a * 3 + r) * q.ncell + c];
         }
         const double *b = image_grad + 3 * node;
         if (vv) {
@@ -575,6 +580,185 @@ __global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const double *
 #pragma unroll
             for (int r = 0; r < 3; r++) out[r * q.nfree + i] = (qw * b[r] * b[r] + q.lam * qw) + s[r];
         }
+    }
+}
+
+// ============================================================================================== mixed form
+// The direction pipeline in float32 (gradient, GGN diagonal): edge differences formed in float64 from the float64
+// state and rounded once, grad u, cofactors, fluxes and the separable adjoint in float32, float32 locals gathered in
+// float64.  The localized barrier stays float64: wherever the float32 J of a closed27 point comes within
+// kBarrierGuard of the activation, that point's grad u is recomputed in float64 (bitwise the plain form's value) and
+// the barrier and its derivatives are evaluated there.
+constexpr float kBarrierGuard = 1e-3f;
+
+__device__ __forceinline__ void load_edges_f32(const double *__restrict__ u, long long n0, const Q1Const &q,
+                                               float E[3][4][3]) {
+    double v[8][3];
+    load_cell(u, n0, q, v);
+    double E64[3][4][3];
+    cell_edges(v, E64);
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) E[j][e][r] = (float)E64[j][e][r];
+}
+// grad u at closed27 point (ix, iy, iz) of the cell in float64, as the plain form's sweep evaluates it
+__device__ __noinline__ void closed_point_f64(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
+                                              int iy, int iz, double V[3][3]) {
+    double E[3][4][3];
+    load_edges(u, n0, q, E);
+    const double nx = rule_n<true>(q, ix), mx = rule_m<true>(q, ix), ny = rule_n<true>(q, iy), my = rule_m<true>(q, iy);
+    const double nz = rule_n<true>(q, iz), mz = rule_m<true>(q, iz);
+    double X[3], Y[3], Z[3];
+    column<0>(E, my, ny, mz, nz, q.ih[0], X);
+    column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
+    column<2>(E, mx, nx, my, ny, q.ih[2], Z);
+#pragma unroll
+    for (int r = 0; r < 3; r++) { V[r][0] = X[r]; V[r][1] = Y[r]; V[r][2] = Z[r]; }
+}
+
+__global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
+                                                         const double *__restrict__ uref, double mu_scale,
+                                                         double nu_scale, bool barrier, bool split,
+                                                         float *__restrict__ L1, float *__restrict__ L2) {
+    extern __shared__ float smemf[];
+    float *sl = smemf + threadIdx.x;
+    const int T = blockDim.x;
+    const float cn[3] = {0.f, .5f, 1.f}, cm[3] = {1.f, .5f, 0.f};
+    const float mu = (float)(q.mu * mu_scale), nu = (float)(q.nu * nu_scale);
+    const float guard = (float)q.act + kBarrierGuard;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        float E[3][4][3], L[8][3];
+        load_edges_f32(u, n0, q, E);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) L[a][r] = 0.f;
+        if (mu != 0.f || nu != 0.f) {
+            float Er[3][4][3];
+            load_edges_f32(uref, n0, q, Er);
+            zero_slice(sl, T, 81);
+            sweep2<false, float>(E, Er, q, [&](int p, int ix, int iy, int iz, const float (&V)[3][3],
+                                               const float (&Vr)[3][3]) {
+                float A[3][3], J, C[3], Cr[3];
+                cofactor_det(V, A, J);
+                float Jr = det_only(Vr);
+                curl_of(V, C);
+                curl_of(Vr, Cr);
+                const float gw = (float)q.gw[p];
+                float jd = mu * gw * (J - Jr);
+                float k0 = nu * gw * (C[0] - Cr[0]), k1 = nu * gw * (C[1] - Cr[1]), k2 = nu * gw * (C[2] - Cr[2]);
+                float f[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++) f[r][jj] = A[r][jj] * jd;
+                f[2][1] += k0; f[1][2] -= k0;
+                f[0][2] += k1; f[2][0] -= k1;
+                f[1][0] += k2; f[0][1] -= k2;
+                add_flux(sl, T, ix, iy, iz, f);
+            });
+            scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
+        }
+        bool any = false;
+        if (barrier) {
+            zero_slice(sl, T, 81);
+            sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
+                if (!(det_only(V) < guard)) return;
+                double V64[3][3];
+                closed_point_f64(u, n0, q, ix, iy, iz, V64);
+                if (!(det_only(V64) < q.act)) return;
+                double A[3][3], J, b, b1, b2;
+                cofactor_det(V64, A, J);
+                barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+                float f[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
+                add_flux(sl, T, ix, iy, iz, f);
+                any = true;
+            });
+        }
+        float Lb[8][3];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) Lb[a][r] = 0.f;
+        if (any) scatter_slice(sl, T, cn, cm, q.ih, Lb);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) L[a][r] += Lb[a][r];
+        store_locals(L1, c, q.ncell, L);
+        if (split) store_locals(L2, c, q.ncell, Lb);
+    }
+}
+
+// GGN diagonal contributions in float32 (Gauss JD/curl part); the closed27 barrier curvature b'' lc^2 in float64
+// at the points the guard selects (lc from the float64 cofactors).
+__global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const double *__restrict__ u,
+                                                             float *__restrict__ L) {
+    const float guard = (float)q.act + kBarrierGuard;
+    const float mu = (float)q.mu, nu = (float)q.nu;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const long long n0 = cell_node0(c, q);
+        float E[3][4][3], out[8][3];
+        load_edges_f32(u, n0, q, E);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] = 0.f;
+        sweep<false, float>(E, q, [&](int p, int ix, int iy, int iz, const float (&V)[3][3]) {
+            float A[3][3], J;
+            cofactor_det(V, A, J);
+            const float gw = (float)q.gw[p];
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                const int bx = a & 1, by = (a >> 1) & 1, bz = (a >> 2) & 1;
+                const float fx = (float)(bx ? rule_n<false>(q, ix) : rule_m<false>(q, ix));
+                const float fy = (float)(by ? rule_n<false>(q, iy) : rule_m<false>(q, iy));
+                const float fz = (float)(bz ? rule_n<false>(q, iz) : rule_m<false>(q, iz));
+                float D[3];
+                D[0] = (float)(bx ? q.ih[0] : -q.ih[0]) * fy * fz;
+                D[1] = (float)(by ? q.ih[1] : -q.ih[1]) * fx * fz;
+                D[2] = (float)(bz ? q.ih[2] : -q.ih[2]) * fx * fy;
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    float lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
+                    float cs = 0.f;
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        if (j != r) cs += D[j] * D[j];
+                    out[a][r] += gw * (mu * lj * lj + nu * cs);
+                }
+            }
+        });
+        sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
+            if (!(det_only(V) < guard)) return;
+            double V64[3][3];
+            closed_point_f64(u, n0, q, ix, iy, iz, V64);
+            if (!(det_only(V64) < q.act)) return;
+            double A[3][3], J, b, b1, b2;
+            cofactor_det(V64, A, J);
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                double D[3];
+                point_D<true>(q, ix, iy, iz, a, D);
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    double lc = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
+                    out[a][r] += (float)(b2 * lc * lc);
+                }
+            }
+        });
+        store_locals(L, c, q.ncell, out);
     }
 }
 
@@ -1302,6 +1486,13 @@ int pair_locals(svp_pair *p, int n) {
 
 using namespace svp;
 
+extern "C" int svp_pair_set_precision(svp_pair *p, int32_t precision) {
+    SVP_REQUIRE(p && (precision == SVP_PRECISION_PLAIN || precision == SVP_PRECISION_MIXED),
+                "svp_pair_set_precision: SVP_PRECISION_PLAIN or SVP_PRECISION_MIXED");
+    p->precision = precision;
+    return SVP_OK;
+}
+
 extern "C" int svp_warp(const svp_pair *p, const double *u, double *warped, double *image_grad, void *stream) {
     SVP_REQUIRE(p && u && warped, "svp_warp: null argument");
     cudaStream_t s = (cudaStream_t)stream;
@@ -1442,9 +1633,10 @@ extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double 
     return SVP_OK;
 }
 
-static int run_gather(svp_pair *p, const GatherSpec &g, const double *L1, const double *L2, const double *u,
+template <class LT>
+static int run_gather(svp_pair *p, const GatherSpec &g, const LT *L1, const LT *L2, const double *u,
                       const double *uref, const double *warped, const double *image_grad, cudaStream_t s) {
-    { svp::KernelTimer _t("gather_kernel", s); SVP_LAUNCH(gather_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, g, L1, L2, u, uref, warped, p->fixed, image_grad)); }
+    { svp::KernelTimer _t("gather_kernel", s); SVP_LAUNCH(gather_kernel<LT><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, g, L1, L2, u, uref, warped, p->fixed, image_grad)); }
     SVP_LAUNCH_CHECK("gather_kernel");
     return SVP_OK;
 }
@@ -1456,11 +1648,18 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
     bool img = terms & SVP_TERM_IMAGE;
     SVP_REQUIRE(!img || (warped && image_grad), "svp_gradient: the image term needs warped and image_grad");
     cudaStream_t s = (cudaStream_t)stream;
+    const bool mixed = p->precision == SVP_PRECISION_MIXED;
     bool cellwork = terms & (SVP_TERM_JD | SVP_TERM_CURL | SVP_TERM_BARRIER);
     if (cellwork) {
         int rc = pair_locals(p, 1);
         if (rc) return rc;
-        { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
+        if (mixed) {
+            svp::KernelTimer _t("cell_grad32_kernel", s);
+            SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
+                                                       (terms & SVP_TERM_CURL) ? 1. : 0.,
+                                                       (terms & SVP_TERM_BARRIER) != 0, false, (float *)p->loc1, nullptr));
+        } else {
+            svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
                                                        (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr)); }
         SVP_LAUNCH_CHECK("cell_grad_kernel");
@@ -1471,8 +1670,11 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
     g.cp[0] = (terms & SVP_TERM_PROXIMITY) ? 1. : 0.;
     g.c1[0] = cellwork ? 1. : 0.;
     g.out[0] = out;
-    return run_gather(p, g, cellwork ? p->loc1 : nullptr, nullptr, u, p->u_ref, img ? warped : nullptr,
-                      img ? image_grad : nullptr, s);
+    if (mixed)
+        return run_gather<float>(p, g, cellwork ? (const float *)p->loc1 : nullptr, nullptr, u, p->u_ref,
+                                 img ? warped : nullptr, img ? image_grad : nullptr, s);
+    return run_gather<double>(p, g, cellwork ? p->loc1 : nullptr, nullptr, u, p->u_ref, img ? warped : nullptr,
+                              img ? image_grad : nullptr, s);
 }
 
 extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, const double *image_grad,
@@ -1481,7 +1683,12 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 2);
     if (rc) return rc;
-    { svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
+    const bool mixed = p->precision == SVP_PRECISION_MIXED;
+    if (mixed) {
+        svp::KernelTimer _t("cell_grad32_kernel", s);
+        SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, 1., 1., true, true, (float *)p->loc1, (float *)p->loc2));
+    } else {
+        svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
     GatherSpec g{};
     g.nout = 3;
@@ -1489,7 +1696,8 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     g.ci[0] = 1.; g.cp[0] = 0.; g.c1[0] = 0.; g.c2[0] = 1.; g.out[0] = gF;
     g.ci[1] = 1.; g.cp[1] = 0.; g.c1[1] = 0.; g.c2[1] = 0.; g.out[1] = gD;
     g.ci[2] = 1.; g.cp[2] = 1.; g.c1[2] = 1.; g.c2[2] = 0.; g.out[2] = gE;
-    return run_gather(p, g, p->loc1, p->loc2, u, p->u_ref, warped, image_grad, s);
+    if (mixed) return run_gather<float>(p, g, (const float *)p->loc1, (const float *)p->loc2, u, p->u_ref, warped, image_grad, s);
+    return run_gather<double>(p, g, p->loc1, p->loc2, u, p->u_ref, warped, image_grad, s);
 }
 
 extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out,
@@ -1498,8 +1706,13 @@ extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *imag
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 1);
     if (rc) return rc;
-    { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1)); }
-    SVP_LAUNCH(ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out));
+    if (p->precision == SVP_PRECISION_MIXED) {
+        { svp::KernelTimer _t("cell_ggn_diag32_kernel", s); SVP_LAUNCH(cell_ggn_diag32_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, (float *)p->loc1)); }
+        SVP_LAUNCH(ggn_node_kernel<float><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, (const float *)p->loc1, image_grad, nullptr, out));
+    } else {
+        { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1)); }
+        SVP_LAUNCH(ggn_node_kernel<double><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out));
+    }
     SVP_LAUNCH_CHECK("ggn diagonal");
     return SVP_OK;
 }
@@ -1515,7 +1728,7 @@ extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_gra
     rc = svp_inject(&p->grid, pvec, vv, stream);
     if (rc) return rc;
     { svp::KernelTimer _t("cell_ggn_hvp_kernel", s); SVP_LAUNCH(cell_ggn_hvp_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, vv, p->loc1)); }
-    SVP_LAUNCH(ggn_node_kernel<<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out));
+    SVP_LAUNCH(ggn_node_kernel<double><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, vv, out));
     SVP_LAUNCH_CHECK("ggn hvp");
     return SVP_OK;
 }

@@ -154,51 +154,53 @@ __device__ __forceinline__ double rule_m(const Q1Const &q, int i) { return CLOSE
 // (iy, iz) and column y only on (ix, iz), so x is evaluated once per (iy, iz) and y once per (ix, iz): 45 column
 // evaluations instead of 81, each bitwise the one of column<J> at that point.  Fields: one (sweep) or two
 // (sweep2, same points); body(p, ix, iy, iz, V[, V2]).
-template <bool CLOSED, class Body>
-__device__ __forceinline__ void sweep(const double E[3][4][3], const Q1Const &q, Body &&body) {
+template <bool CLOSED, class R = double, class Body>
+__device__ __forceinline__ void sweep(const R E[3][4][3], const Q1Const &q, Body &&body) {
+    const R ih0 = (R)q.ih[0], ih1 = (R)q.ih[1], ih2 = (R)q.ih[2];
 #pragma unroll 1
     for (int iz = 0; iz < 3; iz++) {
-        const double nz = rule_n<CLOSED>(q, iz), mz = rule_m<CLOSED>(q, iz);
-        double Y[3][3];
+        const R nz = (R)rule_n<CLOSED>(q, iz), mz = (R)rule_m<CLOSED>(q, iz);
+        R Y[3][3];
 #pragma unroll
-        for (int ix = 0; ix < 3; ix++) column<1>(E, rule_m<CLOSED>(q, ix), rule_n<CLOSED>(q, ix), mz, nz, q.ih[1], Y[ix]);
+        for (int ix = 0; ix < 3; ix++)
+            column<1>(E, (R)rule_m<CLOSED>(q, ix), (R)rule_n<CLOSED>(q, ix), mz, nz, ih1, Y[ix]);
 #pragma unroll 1
         for (int iy = 0; iy < 3; iy++) {
-            const double ny = rule_n<CLOSED>(q, iy), my = rule_m<CLOSED>(q, iy);
-            double X[3];
-            column<0>(E, my, ny, mz, nz, q.ih[0], X);
+            const R ny = (R)rule_n<CLOSED>(q, iy), my = (R)rule_m<CLOSED>(q, iy);
+            R X[3];
+            column<0>(E, my, ny, mz, nz, ih0, X);
 #pragma unroll
             for (int ix = 0; ix < 3; ix++) {
-                double Z[3];
-                column<2>(E, rule_m<CLOSED>(q, ix), rule_n<CLOSED>(q, ix), my, ny, q.ih[2], Z);
-                double V[3][3] = {{X[0], Y[ix][0], Z[0]}, {X[1], Y[ix][1], Z[1]}, {X[2], Y[ix][2], Z[2]}};
+                R Z[3];
+                column<2>(E, (R)rule_m<CLOSED>(q, ix), (R)rule_n<CLOSED>(q, ix), my, ny, ih2, Z);
+                R V[3][3] = {{X[0], Y[ix][0], Z[0]}, {X[1], Y[ix][1], Z[1]}, {X[2], Y[ix][2], Z[2]}};
                 body(9 * iz + 3 * iy + ix, ix, iy, iz, V);
             }
         }
     }
 }
-template <bool CLOSED, class Body>
-__device__ __forceinline__ void sweep2(const double E[3][4][3], const double E2[3][4][3], const Q1Const &q,
-                                       Body &&body) {
+template <bool CLOSED, class R = double, class Body>
+__device__ __forceinline__ void sweep2(const R E[3][4][3], const R E2[3][4][3], const Q1Const &q, Body &&body) {
+    const R ih0 = (R)q.ih[0], ih1 = (R)q.ih[1], ih2 = (R)q.ih[2];
 #pragma unroll 1
     for (int iz = 0; iz < 3; iz++) {
-        const double nz = rule_n<CLOSED>(q, iz), mz = rule_m<CLOSED>(q, iz);
+        const R nz = (R)rule_n<CLOSED>(q, iz), mz = (R)rule_m<CLOSED>(q, iz);
 #pragma unroll 1
         for (int iy = 0; iy < 3; iy++) {
-            const double ny = rule_n<CLOSED>(q, iy), my = rule_m<CLOSED>(q, iy);
-            double X[3], X2[3];
-            column<0>(E, my, ny, mz, nz, q.ih[0], X);
-            column<0>(E2, my, ny, mz, nz, q.ih[0], X2);
+            const R ny = (R)rule_n<CLOSED>(q, iy), my = (R)rule_m<CLOSED>(q, iy);
+            R X[3], X2[3];
+            column<0>(E, my, ny, mz, nz, ih0, X);
+            column<0>(E2, my, ny, mz, nz, ih0, X2);
 #pragma unroll 1
             for (int ix = 0; ix < 3; ix++) {
-                const double nx = rule_n<CLOSED>(q, ix), mx = rule_m<CLOSED>(q, ix);
-                double Y[3], Z[3], Y2[3], Z2[3];
-                column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
-                column<2>(E, mx, nx, my, ny, q.ih[2], Z);
-                column<1>(E2, mx, nx, mz, nz, q.ih[1], Y2);
-                column<2>(E2, mx, nx, my, ny, q.ih[2], Z2);
-                double V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
-                double V2[3][3] = {{X2[0], Y2[0], Z2[0]}, {X2[1], Y2[1], Z2[1]}, {X2[2], Y2[2], Z2[2]}};
+                const R nx = (R)rule_n<CLOSED>(q, ix), mx = (R)rule_m<CLOSED>(q, ix);
+                R Y[3], Z[3], Y2[3], Z2[3];
+                column<1>(E, mx, nx, mz, nz, ih1, Y);
+                column<2>(E, mx, nx, my, ny, ih2, Z);
+                column<1>(E2, mx, nx, mz, nz, ih1, Y2);
+                column<2>(E2, mx, nx, my, ny, ih2, Z2);
+                R V[3][3] = {{X[0], Y[0], Z[0]}, {X[1], Y[1], Z[1]}, {X[2], Y[2], Z[2]}};
+                R V2[3][3] = {{X2[0], Y2[0], Z2[0]}, {X2[1], Y2[1], Z2[1]}, {X2[2], Y2[2], Z2[2]}};
                 body(9 * iz + 3 * iy + ix, ix, iy, iz, V, V2);
             }
         }

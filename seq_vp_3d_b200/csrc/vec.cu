@@ -152,10 +152,72 @@ __global__ void max_abs_diff_kernel(const double *__restrict__ a, const double *
     }
 }
 
+// order keys -> doubles in place (the deferred form of the step-bound reduction)
+__global__ void keys_to_double_kernel(long long *keys, int n) {
+    if (threadIdx.x < n) keys[threadIdx.x] = __double_as_longlong(key_value(keys[threadIdx.x]));
+}
+__global__ void set_key_kernel(long long *key, long long value) { *key = value; }
+
 }  // namespace
 }  // namespace svp
 
 using namespace svp;
+
+// ---- deferred forms: results into device memory, no synchronisation (gather several scalars with one copy) ----
+extern "C" int svp_dot_dev(const double *a, const double *b, int64_t n, double *out_dev, void *stream) {
+    SVP_REQUIRE(a && b && out_dev && n >= 0, "svp_dot_dev: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = blocks_for(n, 256, 4);
+    dd *part = nullptr;
+    SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * nb, s));
+    SVP_LAUNCH(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
+    SVP_LAUNCH(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, out_dev));
+    cudaError_t le = cudaGetLastError();
+    cudaError_t fe = scratch_free(part, s);
+    if (le != cudaSuccess) return cuda_fail(le, "dot kernels");
+    if (fe != cudaSuccess) return cuda_fail(fe, "dot free");
+    return SVP_OK;
+}
+
+extern "C" int svp_bb2_dots_dev(const double *theta, const double *theta_old, const double *g, const double *g_old,
+                                const double *p_old, const double *pvec, int64_t n, double *out4_dev, void *stream) {
+    SVP_REQUIRE(theta && theta_old && g && g_old && p_old && pvec && out4_dev && n >= 0, "svp_bb2_dots_dev: invalid");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = blocks_for(n, 256, 4);
+    dd *part = nullptr;
+    SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * 4 * nb, s));
+    SVP_LAUNCH(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
+    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, out4_dev));
+    cudaError_t le = cudaGetLastError();
+    cudaError_t fe = scratch_free(part, s);
+    if (le != cudaSuccess) return cuda_fail(le, "bb2 kernels");
+    if (fe != cudaSuccess) return cuda_fail(fe, "bb2 free");
+    return SVP_OK;
+}
+
+extern "C" int svp_max_abs_diff_dev(const double *a, const double *b, int64_t n, double *out2_dev, void *stream) {
+    SVP_REQUIRE(a && b && out2_dev && n >= 0, "svp_max_abs_diff_dev: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long *keys = (long long *)out2_dev;
+    SVP_CUDA(cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s));
+    // the keys are the bits of the nonnegative maxima (NaN canonical): already the doubles
+    SVP_LAUNCH(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
+    SVP_LAUNCH_CHECK("max_abs_diff");
+    return SVP_OK;
+}
+
+extern "C" int svp_step_bound_dev(const svp_grid *g, const double *u, const double *pvec, double *bound_dev,
+                                  void *stream) {
+    SVP_REQUIRE(grid_ok(g) && u && pvec && bound_dev, "svp_step_bound_dev: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long *best = (long long *)bound_dev;
+    SVP_LAUNCH(set_key_kernel<<<1, 1, 0, s>>>(best, kKeyPosInf));
+    SVP_LAUNCH(step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
+                                                                    g->y0, g->z0, u, pvec, best));
+    SVP_LAUNCH(keys_to_double_kernel<<<1, 32, 0, s>>>(best, 1));
+    SVP_LAUNCH_CHECK("step_bound");
+    return SVP_OK;
+}
 
 extern "C" int svp_bb2_dots(const double *theta, const double *theta_old, const double *g, const double *g_old,
                             const double *p_old, const double *pvec, int64_t n, double *out4, void *stream) {

@@ -16,7 +16,10 @@ F64 = torch.float64
 
 
 class DevicePair:
-    def __init__(self, grid, fixed, moving, u_ref, *, lam, mu, nu, kappa, activation=.05, delta=0., stream=None):
+    PRECISIONS = {"plain": 0, "mixed": 1}
+
+    def __init__(self, grid, fixed, moving, u_ref, *, lam, mu, nu, kappa, activation=.05, delta=0., stream=None,
+                 precision="plain"):
         require_cuda()
         self.grid = grid
         self.weights = (float(lam), float(mu), float(nu), float(kappa), float(activation), float(delta))
@@ -30,6 +33,10 @@ class DevicePair:
                   ctypes.byref(h), stream_ptr(stream))
         self._h = h
         self.device = f.device
+        if precision not in self.PRECISIONS:
+            raise ValueError("precision: 'plain' (float64) or 'mixed' (float32 search direction)")
+        self.precision = precision
+        _lib.call("svp_pair_set_precision", self._h, self.PRECISIONS[precision])
         nz, ny, nx = grid.shape
         self.nnode, self.nfree = nz * ny * nx, (nz - 2) * (ny - 2) * (nx - 2)
 
@@ -178,3 +185,36 @@ def axpy(x, tau, p, out=None, stream=None):
     out = torch.empty_like(x) if out is None else out
     _lib.call("svp_axpy", ptr(x), float(tau), ptr(p), x.numel(), ptr(out), stream_ptr(stream))
     return out
+
+
+class Scalars:
+    """Device slots for the scalars of one step (dots, BB2 products, bounds), gathered with a single copy into pinned
+    host memory and one stream synchronisation (libsvp3d's *_dev entry points write the slots stream-ordered)."""
+
+    def __init__(self, n=16, device="cuda"):
+        self.dev = torch.zeros(n, dtype=torch.float64, device=device)
+        self.host = torch.zeros(n, dtype=torch.float64).pin_memory()
+
+    def slot(self, k):
+        return ctypes.c_void_p(self.dev.data_ptr() + 8 * k)
+
+    def dot(self, k, a, b, stream=None):
+        _lib.call("svp_dot_dev", ptr(a), ptr(b), a.numel(), self.slot(k), stream_ptr(stream))
+
+    def bb2(self, k, theta, theta_old, g, g_old, p_old, p, stream=None):
+        _lib.call("svp_bb2_dots_dev", ptr(theta), ptr(theta_old), ptr(g), ptr(g_old), ptr(p_old), ptr(p),
+                  theta.numel(), self.slot(k), stream_ptr(stream))
+
+    def max_abs_diff(self, k, a, b, stream=None):
+        _lib.call("svp_max_abs_diff_dev", ptr(a), ptr(b), a.numel(), self.slot(k), stream_ptr(stream))
+
+    def step_bound(self, k, pair, u, p, stream=None):
+        _lib.call("svp_step_bound_dev", ctypes.byref(pair._g), ptr(u), ptr(p), self.slot(k), stream_ptr(stream))
+
+    def fetch(self, stream=None):
+        """Copy every slot to the host and wait; returns a numpy copy."""
+        s = torch.cuda.current_stream() if stream is None else stream
+        with torch.cuda.stream(s):
+            self.host.copy_(self.dev, non_blocking=True)
+        s.synchronize()
+        return self.host.numpy().copy()

@@ -223,7 +223,7 @@ def transfer(seed, grid, certificate_config=None):
 
 
 def register_pair(fixed, moving, grid, weights, *, preopt=NATIVE_PREOPT, taper=NATIVE_TAPER, outer=200,
-                  inner_config=None, certificate_config=None):
+                  inner_config=None, certificate_config=None, precision="plain"):
     """The config-2 route: pyramid pre-optimization, boundary taper, certified transfer, then the certified native
     proximal solve from the transferred field (which is also its proximal reference).  Returns
     (SequentialResult, record).  Without a certified transfer the native solve starts from u = 0."""
@@ -234,8 +234,8 @@ def register_pair(fixed, moving, grid, weights, *, preopt=NATIVE_PREOPT, taper=N
         raw, record["preopt"] = preoptimize(fixed, moving, grid, preopt)
         seed, _ = boundary_taper(raw, grid, taper)
         field, record["transfer"] = transfer(seed.contiguous(), grid)
-    reg = Registration(grid, fixed, moving, **weights,
-                       u_ref=None if field is None else field, certificate_config=certificate_config)
+    reg = Registration(grid, fixed, moving, **weights, u_ref=None if field is None else field,
+                       certificate_config=certificate_config, precision=precision)
     theta0 = None if field is None else reg.pair.restrict(field)
     res = solve_sequential(reg, theta0, config=SequentialConfig3D(max_iterations=outer),
                            inner_config=PGConfig3D() if inner_config is None else inner_config)

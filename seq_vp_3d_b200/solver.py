@@ -21,7 +21,7 @@ import torch
 
 from . import certificate as cert_mod
 from .device import to_device
-from .pair import DevicePair, axpy, dot
+from .pair import DevicePair, Scalars, axpy, dot
 
 EPS = float(np.finfo(float).eps)
 InvalidTrial = namedtuple("InvalidTrial", "reason detail count")
@@ -122,7 +122,7 @@ class Registration:
     localized closed27 barrier (activation 0.05), the certificate configuration and the proximal reference."""
 
     def __init__(self, grid, fixed, moving, *, lam, mu, nu, kappa, activation=.05, u_ref=None,
-                 certificate_config=None):
+                 certificate_config=None, precision="plain"):
         self.grid = grid
         self.config = cert_mod.CertificateConfig(delta=0.) if certificate_config is None else certificate_config
         self.delta = self.config.delta
@@ -130,12 +130,13 @@ class Registration:
         self.activation = activation
         u_ref = torch.zeros(grid.shape + (3,), dtype=torch.float64, device="cuda") if u_ref is None else u_ref
         self.pair = DevicePair(grid, fixed, moving, u_ref, lam=lam, mu=mu, nu=nu, kappa=kappa,
-                               activation=activation, delta=self.delta)
+                               activation=activation, delta=self.delta, precision=precision)
         self.certifier = cert_mod.certifier(grid, self.config)
         self.q_sum = float(np.sum(grid.node_weights(), dtype=np.longdouble))
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0
         self._reference_version = 0
+        self.scalars = Scalars(16)
         ref = self.certify(to_device(u_ref))
         if ref.status != "certified_feasible":
             raise ValueError(f"u_ref: not certified feasible ({ref.reason})")
@@ -195,7 +196,11 @@ class Registration:
 
     # ------------------------------------------------------------------ derivatives
     def gnorm(self, g):
-        return float(np.sqrt(max(dot(g, g), 0.)) / np.sqrt(self.grid.omega))
+        return self.norm_of(dot(g, g))
+
+    def norm_of(self, gg):
+        """The norm sqrt(max(g.g, 0)) / sqrt(omega) from the dot product."""
+        return float(np.sqrt(max(float(gg), 0.)) / np.sqrt(self.grid.omega))
 
     def outer_norms(self, state):
         if state.norms is None:
@@ -358,11 +363,19 @@ def _bb2(reg, config, theta, g, p, previous):
     if previous is None:
         return _protect(config, config.initial_step), "initial"
     th0, g0, p0, tau0 = previous
-    fallback = _protect(config, 2 * min(tau0, config.step_max / 2))
     out = (ctypes.c_double * 4)()
     _lib.call("svp_bb2_dots", ptr(theta), ptr(th0), ptr(g), ptr(g0), ptr(p0), ptr(p), theta.numel(), out,
               stream_ptr())
-    sy, ss, yy2, yiy = out[:]
+    return _bb2_rule(config, previous, out[:])
+
+
+def _bb2_rule(config, previous, dots):
+    """The BB2 rule set on the secant products (s.y, s.s, y.y, y.iy) of svp_bb2_dots."""
+    if previous is None:
+        return _protect(config, config.initial_step), "initial"
+    tau0 = previous[3]
+    fallback = _protect(config, 2 * min(tau0, config.step_max / 2))
+    sy, ss, yy2, yiy = (float(v) for v in dots)
     if not all(np.isfinite([sy, ss, yy2, yiy])):
         return fallback, "fallback_nonfinite_secant"
     if sy <= 0:
@@ -411,39 +424,56 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
     def finish(status, reason):
         return InnerResult(base, status, reason, G, target, accepted_steps, history)
 
+    S = reg.scalars
     while True:
         final = accepted_steps >= config.max_iterations
-        try:
-            if final:
-                # the last gradient of the solve: the joint outer triple (same gE), reused by the outer norms
-                gF, gD, g = reg.pair.outer_gradients(base.u, base.warped, base.image_grad)
-                G = reg.gnorm(g)
-                base.norms = (reg.gnorm(gF), reg.gnorm(gD), G)
-            else:
-                g = reg.pair.gradient(base.u, base.warped, base.image_grad)
-                G = reg.gnorm(g)
-        except FloatingPointError as exc:
-            return finish("nonfinite_evaluation", str(exc))
-        if G <= target:
-            return finish("converged_gradient", "GRADIENT_TARGET")
-        if small_steps >= config.stall_steps:
-            return finish("stagnated", "SMALL_ACCEPTED_STEPS")
         if final:
+            # the last gradient of the solve: the joint outer triple (same gE), reused by the outer norms
+            gF, gD, g = reg.pair.outer_gradients(base.u, base.warped, base.image_grad)
+            S.dot(0, g, g)
+            S.dot(1, gF, gF)
+            S.dot(2, gD, gD)
+            v = S.fetch()
+            G = reg.norm_of(v[0])
+            base.norms = (reg.norm_of(v[1]), reg.norm_of(v[2]), G)
+            if G <= target:
+                return finish("converged_gradient", "GRADIENT_TARGET")
+            if small_steps >= config.stall_steps:
+                return finish("stagnated", "SMALL_ACCEPTED_STEPS")
             return finish("max_iterations", "ACCEPTED_STEP_BUDGET")
+        # One batch of device work and one synchronisation per step: the gradient and its norm, (the metric on the
+        # first step,) the direction, the slope, the BB2 secant products and the domain bound.  The decisions below
+        # are taken in the reference's order on the same values.
+        g = reg.pair.gradient(base.u, base.warped, base.image_grad)
+        S.dot(0, g, g)
+        metric_error = None
         if metric is None:
             try:
                 metric = reg.metric(base, config, memory)
             except FloatingPointError as exc:
-                return finish("nonfinite_evaluation", str(exc))
-        a, b, scale = metric
-        p = reg.pair.poisson_apply(a, b, g, scale=scale, sign=-1.)
-        slope = dot(g, p)
+                metric_error = exc
+        if metric_error is None:
+            a, b, scale = metric
+            p = reg.pair.poisson_apply(a, b, g, scale=scale, sign=-1.)
+            S.dot(1, g, p)
+            if previous is not None:
+                S.bb2(2, base.theta, previous[0], g, previous[1], previous[2], p)
+            S.step_bound(6, reg.pair, base.u, p)
+        v = S.fetch()
+        G = reg.norm_of(v[0])
+        if G <= target:
+            return finish("converged_gradient", "GRADIENT_TARGET")
+        if small_steps >= config.stall_steps:
+            return finish("stagnated", "SMALL_ACCEPTED_STEPS")
+        if metric_error is not None:
+            return finish("nonfinite_evaluation", str(metric_error))
+        slope = float(v[1])
         if not np.isfinite(slope):
             return finish("nonfinite_evaluation", "PG directional derivative")
         if slope >= 0:
             return finish("non_descent_direction", "NON_DESCENT_DIRECTION")
-        proposal, rule = _bb2(reg, config, base.theta, g, p, previous)
-        bound = reg.pair.step_bound(base.u, p)
+        proposal, rule = _bb2_rule(config, previous, v[2:6])
+        bound = float(v[6])
         if bound <= 0:
             return finish("domain_blocked", "NO_POSITIVE_DOMAIN_STEP")
         tau = min(proposal, .9 * bound)
