@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
                     help="plain: float64 throughout; mixed: float32 search direction (gradient, GGN diagonal, DST-I) "
                          "with float64 energies, decisions and certificate")
+    ap.add_argument("--concurrency", type=int, default=1,
+                    help="serving form: registrations in flight at once (each on its own stream); a step is one "
+                         "round of that many pairs, value = all pairs / time, with p50/p95/p99 latency")
     ap.add_argument("--preopt", action=argparse.BooleanOptionalAction, default=True,
                     help="config-2 route: float32 8/4/2/1 pyramid pre-optimizer + certified transfer before the "
                          "native steps")
@@ -228,6 +231,83 @@ def cpu_baseline(shape, fixed, moving, weights, slab, outer):
     return 3600. / seconds, cores, sample, sum(t.values())
 
 
+# ------------------------------------------------------------------------------------------ serving form
+def serving_bench(args, grid, weights, shape, config, world, rank, Clocks, local):
+    """--concurrency K: K registrations in flight through the serving form (own streams and threads); a step is one
+    round of K distinct pairs (seeds seed .. seed + K - 1).  value = pairs / device time of the timed rounds;
+    latency percentiles from submission to certified result; e2e = the same rounds from pinned host images with the
+    certified u copied back to pinned host memory."""
+    import torch
+    from seq_vp_3d_b200.preopt import NATIVE_PREOPT, register_pair
+    from seq_vp_3d_b200.serve import RegistrationServer
+    from seq_vp_3d_b200.solver import PGConfig3D
+    from seq_vp_3d_b200.synthetic import head_pair
+    nx, ny, nz = shape
+    K = args.concurrency
+    host = [head_pair((nz, ny, nx), (1., 1., 1.), seed=args.seed + rank * K + k)[:2] for k in range(K)]
+    dev = [(torch.from_numpy(f).cuda(), torch.from_numpy(m).cuda()) for f, m in host]
+    pinned = [(torch.from_numpy(f).pin_memory(), torch.from_numpy(m).pin_memory()) for f, m in host]
+    outs = [torch.empty(grid.shape + (3,), dtype=torch.float64).pin_memory() for _ in range(K)]
+
+    def run(fixed, moving, g, w, out=None):
+        res, _ = register_pair(fixed, moving, g, w, preopt=NATIVE_PREOPT if args.preopt else None,
+                               outer=args.outer, inner_config=PGConfig3D(), precision=args.form)
+        if out is not None:
+            out.copy_(res.final_state.u, non_blocking=True)
+        return res
+
+    def rounds(srv, n, inputs, copy_back):
+        results = []
+        for _ in range(n):
+            futs = [srv.submit(f, m, grid, dict(weights, **({"out": outs[k]} if copy_back else {})))
+                    for k, (f, m) in enumerate(inputs)]
+            results += [fu.result() for fu in futs]
+        return results
+
+    def runner(fixed, moving, g, w):
+        w = dict(w)
+        out = w.pop("out", None)
+        return run(fixed, moving, g, w, out)
+
+    stream = torch.cuda.current_stream()
+    with RegistrationServer(slots=K, run=runner) as srv:
+        rounds(srv, args.warmup, dev, False)
+        srv.latencies.clear()
+        torch.cuda.synchronize()
+        with Clocks(local) as clocks:
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            results = rounds(srv, args.steps, dev, False)
+            torch.cuda.synchronize()
+            end.record(stream)
+            end.synchronize()
+        seconds = start.elapsed_time(end) / 1e3
+        lat = srv.percentiles()
+        torch.cuda.synchronize()
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        rounds(srv, args.steps, pinned, True)
+        torch.cuda.synchronize()
+        e_end.record(stream)
+        e_end.synchronize()
+        e2e_seconds = e_start.elapsed_time(e_end) / 1e3
+    pairs = K * args.steps
+    if rank == 0:
+        r = results[-1]
+        line = dict(metric=METRIC.format(args.form) + f", serving {K} in flight", value=pairs / seconds * 3600.,
+                    unit="pairs/hour", n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=seconds * 1e3 / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64", data="synthetic", config=dict(config, concurrency=K, pairs_per_step=K),
+                    latency_s=lat,
+                    e2e=dict(value=pairs / e2e_seconds * 3600., unit="pairs/hour",
+                             h2d_bytes_per_step=K * 2 * host[0][0].nbytes,
+                             d2h_bytes_per_step=K * outs[0].numel() * 8),
+                    clocks=clocks.summary(), certified=all(x.certified for x in results),
+                    result=dict(status=r.status, outer_accepted=r.counts["outer_accepted"], final_mse=r.final_mse))
+        print(json.dumps(line))
+    return 0
+
+
 # ------------------------------------------------------------------------------------------ main
 def main():
     args = parse()
@@ -307,6 +387,9 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.concurrency > 1:
+        return serving_bench(args, grid, weights, shape, config, world, rank, Clocks, local)
 
     for _ in range(args.warmup):
         step(f_dev, m_dev)

@@ -125,11 +125,13 @@ _CERT_LOCK = threading.Lock()
 
 
 def certifier(grid, config):
-    key = (grid.grid_id, grid.shape, config, torch.cuda.current_device())
+    """The workspace of (grid, config) on the current device for the calling host thread: registrations that run
+    concurrently on their own threads and streams never share a certificate workspace."""
+    key = (grid.grid_id, grid.shape, config, torch.cuda.current_device(), threading.get_ident())
     with _CERT_LOCK:
         c = _CERTIFIERS.get(key)
         if c is None:
-            if len(_CERTIFIERS) > 8:
+            if len(_CERTIFIERS) > 16:
                 _CERTIFIERS.clear()
             c = _CERTIFIERS[key] = Certifier(grid, config)
     return c

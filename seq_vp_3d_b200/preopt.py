@@ -17,7 +17,7 @@ import torch
 
 from . import _lib
 from . import certificate as cert_mod
-from .device import ptr, require_cuda, stream_ptr
+from .device import ptr, require_cuda, stream_ptr, to_device
 from .grid import InputValidationError, make_grid_3d
 
 FACTORS = (8, 4, 2, 1)
@@ -141,8 +141,7 @@ def preoptimize(fixed, moving, grid, config=None, stream=None):
     require_cuda()
     config = PreoptConfig() if config is None else config
     dev = torch.device("cuda")
-    f64 = torch.as_tensor(np.ascontiguousarray(fixed, dtype=np.float64), device=dev) if not torch.is_tensor(fixed) else fixed
-    m64 = torch.as_tensor(np.ascontiguousarray(moving, dtype=np.float64), device=dev) if not torch.is_tensor(moving) else moving
+    f64, m64 = to_device(fixed), to_device(moving)
     started = perf_counter()
     grids = four_level_grids(grid)
     levels, u_mm, cap_total = [], None, 0
