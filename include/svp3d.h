@@ -191,6 +191,18 @@ int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warpe
                      double *trial_warped, double *trial_image_grad, double *terms5, double *diff2,
                      int64_t *barrier_violations, void *stream);
 
+/* The same two evaluations with per-cell barrier activity masks (uint8, one per cell: 1 where some closed27 J of
+ * the cell is below the barrier activation).  trial_active (optional) receives the trial's mask;
+ * svp_energy_difference_masked, given both states' masks, skips the closed27 sweep of cells inactive in both
+ * fields.  The results are bitwise those of svp_trial_energy / svp_energy_difference (the skipped points contribute
+ * nothing). */
+int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                            double *trial_warped, double *trial_image_grad, uint8_t *trial_active, double *terms5,
+                            double *diff2, int64_t *barrier_violations, void *stream);
+int svp_energy_difference_masked(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                                 const double *trial_warped, const uint8_t *base_active, const uint8_t *trial_active,
+                                 double *diff2, void *stream);
+
 /* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
 #define SVP_TERM_IMAGE 1
 #define SVP_TERM_PROXIMITY 2
@@ -207,6 +219,15 @@ int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, cons
                         double *gD, double *gE, void *stream);
 /* Exact diagonal of the frozen barrier GGN (linearization.py:357) and its action on a free vector p (:327). */
 int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out, void *stream);
+/* svp_gradient, svp_outer_gradients and svp_ggn_diagonal with the state's barrier activity mask (the mask
+ * svp_trial_energy_masked returned for this u, or NULL): cells inactive in it skip the closed27 barrier sweep, which
+ * contributes nothing there; the values are bitwise those of the unmasked calls. */
+int svp_gradient_masked(svp_pair *p, const double *u, const double *warped, const double *image_grad, int32_t terms,
+                        const uint8_t *active, double *out, void *stream);
+int svp_outer_gradients_masked(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                               const uint8_t *active, double *gF, double *gD, double *gE, void *stream);
+int svp_ggn_diagonal_masked(svp_pair *p, const double *u, const double *image_grad, const uint8_t *active,
+                            double *out, void *stream);
 int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_grad, const double *pvec, double *out,
                 void *stream);
 

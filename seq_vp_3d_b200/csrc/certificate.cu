@@ -56,14 +56,13 @@ __device__ __forceinline__ int edge_start(int j, int e) {
 
 // ============================================================================================== 1. edge hull
 // F_rj interval: hull of the 4 edge differences (from +inf / -inf in edge order), outward, /h, outward, + identity.
-__device__ __forceinline__ bool hull_entry(const double *__restrict__ u, long long base, long long ny, long long nx,
-                                           int j, int r, double h, double &lo, double &hi) {
+__device__ __forceinline__ bool hull_entry_v(const double v[8][3], int j, int r, double h, double &lo, double &hi) {
     bool ok = true;
     double lower = __longlong_as_double(0x7FF0000000000000LL), upper = -lower;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
         int a = edge_start(j, e), b = a | (1 << j);
-        double d = rsub(__ldg(u + 3 * vnode(base, b, ny, nx) + r), __ldg(u + 3 * vnode(base, a, ny, nx) + r));
+        double d = rsub(v[b][r], v[a][r]);
         ok &= finite64(d);
         lower = nmin(lower, d);
         upper = nmax(upper, d);
@@ -81,12 +80,17 @@ __global__ void __launch_bounds__(256) edge_hull_kernel(const double *__restrict
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long base = cell_base(c, g);
+        double v[8][3];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) v[a][r] = __ldg(u + 3 * vnode(base, a, g.ny, g.nx) + r);
         double fl[3][3], fh[3][3];
         bool ok = true;
 #pragma unroll
         for (int j = 0; j < 3; j++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) ok &= hull_entry(u, base, g.ny, g.nx, j, r, g.h[j], fl[r][j], fh[r][j]);
+            for (int r = 0; r < 3; r++) ok &= hull_entry_v(v, j, r, g.h[j], fl[r][j], fh[r][j]);
         double jl, jh, ml, mh;
         ok &= idet(fl, fh, jl, jh);
         ok &= iout(rsub(jl, delta), rsub(jh, delta), ml, mh);

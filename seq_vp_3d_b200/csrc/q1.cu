@@ -187,6 +187,21 @@ __device__ __forceinline__ void load_edges(const double *__restrict__ u, long lo
     load_cell(u, n0, q, v);
     cell_edges(v, E);
 }
+// grad u at closed27 point (ix, iy, iz) of the cell in float64, as the plain form's sweep evaluates it
+__device__ __noinline__ void closed_point_f64(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
+                                              int iy, int iz, double V[3][3]) {
+    double E[3][4][3];
+    load_edges(u, n0, q, E);
+    const double nx = rule_n<true>(q, ix), mx = rule_m<true>(q, ix), ny = rule_n<true>(q, iy), my = rule_m<true>(q, iy);
+    const double nz = rule_n<true>(q, iz), mz = rule_m<true>(q, iz);
+    double X[3], Y[3], Z[3];
+    column<0>(E, my, ny, mz, nz, q.ih[0], X);
+    column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
+    column<2>(E, mx, nx, my, ny, q.ih[2], Z);
+#pragma unroll
+    for (int r = 0; r < 3; r++) { V[r][0] = X[r]; V[r][1] = Y[r]; V[r][2] = Z[r]; }
+}
+
 template <class R>
 __device__ __forceinline__ void zero_slice(R *sl, int T, int n) {
     for (int k = 0; k < n; k++) sl[k * T] = R(0);
@@ -307,7 +322,8 @@ __device__ __forceinline__ void store_locals(R *__restrict__ L, long long c, lon
 __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *__restrict__ u,
                                                        const double *__restrict__ uref, double mu_scale,
                                                        double nu_scale, bool barrier, bool split,
-                                                       double *__restrict__ L1, double *__restrict__ L2) {
+                                                       double *__restrict__ L1, double *__restrict__ L2,
+                                                       const uint8_t *__restrict__ active) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -349,7 +365,8 @@ __global__ void __launch_bounds__(CS) cell_grad_kernel(Q1Const q, const double *
             scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
         }
         bool any = false;
-        if (barrier) {
+        // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term
+        if (barrier && (!active || active[c])) {
             zero_slice(sl, T, 81);
             sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
                 if (!(det_only(V) < q.act)) return;
@@ -437,7 +454,8 @@ __device__ __forceinline__ void point_D(const Q1Const &q, int ix, int iy, int iz
 }
 
 __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const double *__restrict__ u,
-                                                           double *__restrict__ L) {
+                                                           double *__restrict__ L,
+                                                           const uint8_t *__restrict__ active) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         double E[3][4][3], out[8][3];
@@ -465,6 +483,7 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
                 }
             }
         });
+        if (!active || active[c])
         sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
             if (!(det_only(V) < q.act)) return;
             double A[3][3], J, b, b1, b2;
@@ -604,25 +623,11 @@ __device__ __forceinline__ void load_edges_f32(const double *__restrict__ u, lon
 #pragma unroll
             for (int r = 0; r < 3; r++) E[j][e][r] = (float)E64[j][e][r];
 }
-// grad u at closed27 point (ix, iy, iz) of the cell in float64, as the plain form's sweep evaluates it
-__device__ __noinline__ void closed_point_f64(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
-                                              int iy, int iz, double V[3][3]) {
-    double E[3][4][3];
-    load_edges(u, n0, q, E);
-    const double nx = rule_n<true>(q, ix), mx = rule_m<true>(q, ix), ny = rule_n<true>(q, iy), my = rule_m<true>(q, iy);
-    const double nz = rule_n<true>(q, iz), mz = rule_m<true>(q, iz);
-    double X[3], Y[3], Z[3];
-    column<0>(E, my, ny, mz, nz, q.ih[0], X);
-    column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
-    column<2>(E, mx, nx, my, ny, q.ih[2], Z);
-#pragma unroll
-    for (int r = 0; r < 3; r++) { V[r][0] = X[r]; V[r][1] = Y[r]; V[r][2] = Z[r]; }
-}
-
 __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
                                                          const double *__restrict__ uref, double mu_scale,
                                                          double nu_scale, bool barrier, bool split,
-                                                         float *__restrict__ L1, float *__restrict__ L2) {
+                                                         float *__restrict__ L1, float *__restrict__ L2,
+                                                       const uint8_t *__restrict__ active) {
     extern __shared__ float smemf[];
     float *sl = smemf + threadIdx.x;
     const int T = blockDim.x;
@@ -665,7 +670,8 @@ __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const dou
             scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
         }
         bool any = false;
-        if (barrier) {
+        // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term
+        if (barrier && (!active || active[c])) {
             zero_slice(sl, T, 81);
             sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
                 if (!(det_only(V) < guard)) return;
@@ -702,7 +708,8 @@ __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const dou
 // GGN diagonal contributions in float32 (Gauss JD/curl part); the closed27 barrier curvature b'' lc^2 in float64
 // at the points the guard selects (lc from the float64 cofactors).
 __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const double *__restrict__ u,
-                                                             float *__restrict__ L) {
+                                                             float *__restrict__ L,
+                                                           const uint8_t *__restrict__ active) {
     const float guard = (float)q.act + kBarrierGuard;
     const float mu = (float)q.mu, nu = (float)q.nu;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
@@ -739,6 +746,7 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
                 }
             }
         });
+        if (!active || active[c])
         sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
             if (!(det_only(V) < guard)) return;
             double V64[3][3];
@@ -814,7 +822,9 @@ __device__ __forceinline__ void acc_add(dd &acc, dd t) {
 }
 __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *__restrict__ ua,
                                                        const double *__restrict__ ub,
-                                                       const double *__restrict__ uref, dd *partial) {
+                                                       const double *__restrict__ uref, dd *partial,
+                                                       const uint8_t *__restrict__ act_a,
+                                                       const uint8_t *__restrict__ act_b) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -840,10 +850,12 @@ __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *
             }
         });
         double sb = 0.;
-        sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
-            double ja = det_only(Va), jb = det_only(Vb);
-            if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
-        });
+        // with both masks, a cell inactive in both fields has no barrier difference at all
+        if (!(act_a && act_b && !act_a[c] && !act_b[c]))
+            sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
+                double ja = det_only(Va), jb = det_only(Vb);
+                if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
+            });
         acc_add(acc[2], dd{q.bw * sb, 0.});
     }
 #pragma unroll
@@ -897,10 +909,12 @@ __global__ void __launch_bounds__(256) warp_trial_kernel(Q1Const q, SplineRef S,
     block_reduce_dd<2>(dif, pd);
 }
 
+// Barrier activity mask: act[c] = 1 when some closed27 J of cell c is below the activation; trial_act (optional)
+// receives the trial's mask, which later calls on that state use to skip barrier sweeps that contribute nothing.
 __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double *__restrict__ ua,
                                                         const double *__restrict__ ub,
                                                         const double *__restrict__ uref, dd *pe, dd *pd,
-                                                        unsigned long long *bad) {
+                                                        unsigned long long *bad, uint8_t *__restrict__ trial_act) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -933,9 +947,11 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
             sj += w * dj * dj;
             sc += w * (cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
         });
+        bool active = false;
         sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
             double ja = det_only(Va), jb = det_only(Vb);
             if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+            active |= jb < q.act;
             if (!(jb > q.delta)) { nbad++; return; }
             if (jb < q.act) {
                 double b, b1, b2;
@@ -943,6 +959,7 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
                 sb += b;
             }
         });
+        if (trial_act) trial_act[c] = active ? 1 : 0;
         acc[0] = dd_add_d(acc[0], sj);
         acc[1] = dd_add_d(acc[1], sc);
         acc[2] = dd_add_d(acc[2], sb);
@@ -1551,9 +1568,10 @@ extern "C" int svp_energy(svp_pair *p, const double *u, const double *warped, do
     return SVP_OK;
 }
 
-extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped,
-                                     const double *trial_u, const double *trial_warped, double *diff2,
-                                     void *stream) {
+extern "C" int svp_energy_difference_masked(svp_pair *p, const double *base_u, const double *base_warped,
+                                            const double *trial_u, const double *trial_warped,
+                                            const uint8_t *base_active, const uint8_t *trial_active, double *diff2,
+                                            void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && diff2, "svp_energy_difference: null");
     cudaStream_t s = (cudaStream_t)stream;
     unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
@@ -1564,7 +1582,7 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
     { svp::KernelTimer _t("node_diff_kernel", s); SVP_LAUNCH(node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
                                         p->partial)); }
     dd *pc = p->partial + (long long)nb * 2;
-    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pc)); }
+    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pc, base_active, trial_active)); }
     SVP_LAUNCH_CHECK("difference kernels");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4));
@@ -1580,9 +1598,17 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
     return SVP_OK;
 }
 
-extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warped,
-                                const double *trial_u, double *trial_warped, double *trial_image_grad,
-                                double *terms5, double *diff2, int64_t *barrier_violations, void *stream) {
+extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped,
+                                     const double *trial_u, const double *trial_warped, double *diff2,
+                                     void *stream) {
+    return svp_energy_difference_masked(p, base_u, base_warped, trial_u, trial_warped, nullptr, nullptr, diff2,
+                                        stream);
+}
+
+extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *base_warped,
+                                       const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                       uint8_t *trial_active, double *terms5, double *diff2,
+                                       int64_t *barrier_violations, void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && terms5 && diff2,
                 "svp_trial_energy: null argument");
     cudaStream_t s = (cudaStream_t)stream;
@@ -1603,7 +1629,7 @@ extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double 
                                                                  p->u_ref, trial_warped, nullptr, pne, pnd));
     }
     SVP_LAUNCH_CHECK("warp_trial_kernel");
-    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter)); }
+    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter, trial_active)); }
     SVP_LAUNCH_CHECK("cell_trial_kernel");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
@@ -1633,6 +1659,13 @@ extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double 
     return SVP_OK;
 }
 
+extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warped,
+                                const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                double *terms5, double *diff2, int64_t *barrier_violations, void *stream) {
+    return svp_trial_energy_masked(p, base_u, base_warped, trial_u, trial_warped, trial_image_grad, nullptr, terms5,
+                                   diff2, barrier_violations, stream);
+}
+
 template <class LT>
 static int run_gather(svp_pair *p, const GatherSpec &g, const LT *L1, const LT *L2, const double *u,
                       const double *uref, const double *warped, const double *image_grad, cudaStream_t s) {
@@ -1641,8 +1674,8 @@ static int run_gather(svp_pair *p, const GatherSpec &g, const LT *L1, const LT *
     return SVP_OK;
 }
 
-extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, const double *image_grad,
-                            int32_t terms, double *out, void *stream) {
+extern "C" int svp_gradient_masked(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                                   int32_t terms, const uint8_t *active, double *out, void *stream) {
     SVP_REQUIRE(p && u && out, "svp_gradient: null argument");
     SVP_REQUIRE((terms & ~SVP_TERM_TOTAL) == 0 && terms, "svp_gradient: invalid term mask");
     bool img = terms & SVP_TERM_IMAGE;
@@ -1657,11 +1690,11 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
             svp::KernelTimer _t("cell_grad32_kernel", s);
             SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
-                                                       (terms & SVP_TERM_BARRIER) != 0, false, (float *)p->loc1, nullptr));
+                                                       (terms & SVP_TERM_BARRIER) != 0, false, (float *)p->loc1, nullptr, active));
         } else {
             svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
-                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr)); }
+                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr, active)); }
         SVP_LAUNCH_CHECK("cell_grad_kernel");
     }
     GatherSpec g{};
@@ -1677,8 +1710,9 @@ extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, 
                               img ? image_grad : nullptr, s);
 }
 
-extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, const double *image_grad,
-                                   double *gF, double *gD, double *gE, void *stream) {
+extern "C" int svp_outer_gradients_masked(svp_pair *p, const double *u, const double *warped,
+                                          const double *image_grad, const uint8_t *active, double *gF, double *gD,
+                                          double *gE, void *stream) {
     SVP_REQUIRE(p && u && warped && image_grad && gF && gD && gE, "svp_outer_gradients: null argument");
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 2);
@@ -1686,9 +1720,9 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     const bool mixed = p->precision == SVP_PRECISION_MIXED;
     if (mixed) {
         svp::KernelTimer _t("cell_grad32_kernel", s);
-        SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, 1., 1., true, true, (float *)p->loc1, (float *)p->loc2));
+        SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, 1., 1., true, true, (float *)p->loc1, (float *)p->loc2, active));
     } else {
-        svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2)); }
+        svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2, active)); }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
     GatherSpec g{};
     g.nout = 3;
@@ -1700,21 +1734,34 @@ extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *w
     return run_gather<double>(p, g, p->loc1, p->loc2, u, p->u_ref, warped, image_grad, s);
 }
 
-extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out,
-                                void *stream) {
+extern "C" int svp_ggn_diagonal_masked(svp_pair *p, const double *u, const double *image_grad,
+                                       const uint8_t *active, double *out, void *stream) {
     SVP_REQUIRE(p && u && image_grad && out, "svp_ggn_diagonal: null argument");
     cudaStream_t s = (cudaStream_t)stream;
     int rc = pair_locals(p, 1);
     if (rc) return rc;
     if (p->precision == SVP_PRECISION_MIXED) {
-        { svp::KernelTimer _t("cell_ggn_diag32_kernel", s); SVP_LAUNCH(cell_ggn_diag32_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, (float *)p->loc1)); }
+        { svp::KernelTimer _t("cell_ggn_diag32_kernel", s); SVP_LAUNCH(cell_ggn_diag32_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, (float *)p->loc1, active)); }
         SVP_LAUNCH(ggn_node_kernel<float><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, (const float *)p->loc1, image_grad, nullptr, out));
     } else {
-        { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1)); }
+        { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1, active)); }
         SVP_LAUNCH(ggn_node_kernel<double><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out));
     }
     SVP_LAUNCH_CHECK("ggn diagonal");
     return SVP_OK;
+}
+
+extern "C" int svp_gradient(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                            int32_t terms, double *out, void *stream) {
+    return svp_gradient_masked(p, u, warped, image_grad, terms, nullptr, out, stream);
+}
+extern "C" int svp_outer_gradients(svp_pair *p, const double *u, const double *warped, const double *image_grad,
+                                   double *gF, double *gD, double *gE, void *stream) {
+    return svp_outer_gradients_masked(p, u, warped, image_grad, nullptr, gF, gD, gE, stream);
+}
+extern "C" int svp_ggn_diagonal(svp_pair *p, const double *u, const double *image_grad, double *out,
+                                void *stream) {
+    return svp_ggn_diagonal_masked(p, u, image_grad, nullptr, out, stream);
 }
 
 extern "C" int svp_ggn_hvp(svp_pair *p, const double *u, const double *image_grad, const double *pvec,

@@ -88,40 +88,46 @@ class DevicePair:
         _lib.call("svp_energy", self._h, ptr(u), ptr(warped), t, ctypes.byref(bad), stream_ptr(stream))
         return np.array(t[:]), int(bad.value)
 
-    def energy_difference(self, base_u, base_w, trial_u, trial_w, stream=None):
-        """(E(trial) - E(base), F(trial) - F(base)), cancellation-free."""
+    def energy_difference(self, base_u, base_w, trial_u, trial_w, base_active=None, trial_active=None, stream=None):
+        """(E(trial) - E(base), F(trial) - F(base)), cancellation-free; the optional barrier activity masks of the
+        two states only skip work (same values)."""
         d = (ctypes.c_double * 2)()
-        _lib.call("svp_energy_difference", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(trial_w), d,
-                  stream_ptr(stream))
+        _lib.call("svp_energy_difference_masked", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(trial_w),
+                  ptr(base_active), ptr(trial_active), d, stream_ptr(stream))
         return d[0], d[1]
+
+    def cell_mask(self):
+        return torch.empty(self.grid.n_cells, dtype=torch.uint8, device=self.device)
 
     def trial_energy(self, base_u, base_w, trial_u, with_gradient=True, stream=None):
         """Warp and evaluate a trial against its base in one pass: (warped, image_grad or None, terms[5],
-        barrier violations, (E(trial) - E(base), F(trial) - F(base)))."""
+        barrier violations, (E(trial) - E(base), F(trial) - F(base)), the trial's barrier activity mask)."""
         w = self.node()
         g = self.node(3) if with_gradient else None
+        act = self.cell_mask()
         t = (ctypes.c_double * 5)()
         d = (ctypes.c_double * 2)()
         bad = ctypes.c_int64()
-        _lib.call("svp_trial_energy", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g), t, d,
-                  ctypes.byref(bad), stream_ptr(stream))
-        return w, g, np.array(t[:]), int(bad.value), (d[0], d[1])
+        _lib.call("svp_trial_energy_masked", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g),
+                  ptr(act), t, d, ctypes.byref(bad), stream_ptr(stream))
+        return w, g, np.array(t[:]), int(bad.value), (d[0], d[1]), act
 
-    def gradient(self, u, warped, image_grad, term="total", out=None, stream=None):
+    def gradient(self, u, warped, image_grad, term="total", out=None, active=None, stream=None):
         out = self.free() if out is None else out
-        _lib.call("svp_gradient", self._h, ptr(u), ptr(warped), ptr(image_grad), _lib.TERMS[term], ptr(out),
-                  stream_ptr(stream))
+        _lib.call("svp_gradient_masked", self._h, ptr(u), ptr(warped), ptr(image_grad), _lib.TERMS[term],
+                  ptr(active), ptr(out), stream_ptr(stream))
         return out
 
-    def outer_gradients(self, u, warped, image_grad, stream=None):
+    def outer_gradients(self, u, warped, image_grad, active=None, stream=None):
         gF, gD, gE = self.free(), self.free(), self.free()
-        _lib.call("svp_outer_gradients", self._h, ptr(u), ptr(warped), ptr(image_grad), ptr(gF), ptr(gD), ptr(gE),
-                  stream_ptr(stream))
+        _lib.call("svp_outer_gradients_masked", self._h, ptr(u), ptr(warped), ptr(image_grad), ptr(active), ptr(gF),
+                  ptr(gD), ptr(gE), stream_ptr(stream))
         return gF, gD, gE
 
-    def ggn_diagonal(self, u, image_grad, stream=None):
+    def ggn_diagonal(self, u, image_grad, active=None, stream=None):
         out = self.free()
-        _lib.call("svp_ggn_diagonal", self._h, ptr(u), ptr(image_grad), ptr(out), stream_ptr(stream))
+        _lib.call("svp_ggn_diagonal_masked", self._h, ptr(u), ptr(image_grad), ptr(active), ptr(out),
+                  stream_ptr(stream))
         return out
 
     def ggn_hvp(self, u, image_grad, p, stream=None):
@@ -210,6 +216,19 @@ class Scalars:
 
     def step_bound(self, k, pair, u, p, stream=None):
         _lib.call("svp_step_bound_dev", ctypes.byref(pair._g), ptr(u), ptr(p), self.slot(k), stream_ptr(stream))
+
+    def copy_async(self, stream=None):
+        """Start the copy of every slot to the host; values() waits for it (usually already done by then, when a
+        later call synchronized the stream)."""
+        s = torch.cuda.current_stream() if stream is None else stream
+        with torch.cuda.stream(s):
+            self.host.copy_(self.dev, non_blocking=True)
+            self._done = torch.cuda.Event()
+            self._done.record(s)
+
+    def values(self):
+        self._done.synchronize()
+        return self.host.numpy().copy()
 
     def fetch(self, stream=None):
         """Copy every slot to the host and wait; returns a numpy copy."""

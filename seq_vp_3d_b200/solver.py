@@ -75,6 +75,7 @@ class State:
     image_grad: torch.Tensor = None    # set by promotion
     norms: tuple = None                # (GF, GD, GE) when computed with the final gradient
     differences: tuple = None          # ((base eval_id, reference version), (dE, dF)) from the one-pass trial
+    active: object = None              # per-cell barrier activity mask (from the state's own trial evaluation)
 
     @property
     def total(self):
@@ -159,16 +160,16 @@ class Registration:
             reason = ("NONFINITE_STATE" if c.reason == "NONFINITE_STATE" else
                       "FEASIBILITY_UNCERTAIN" if c.status == "uncertain" else c.reason)
             return InvalidTrial(reason, "trial not certified: " + c.reason, c.n_uncertain + c.n_infeasible)
-        grad = diff = None
+        grad = diff = active = None
         if base is None:
             warped, _ = self.pair.warp(u)
             terms, bad = self.pair.energy(u, warped)
         else:
-            warped, grad, terms, bad, diff = self.pair.trial_energy(base.u, base.warped, u)
+            warped, grad, terms, bad, diff, active = self.pair.trial_energy(base.u, base.warped, u)
         if bad or not np.all(np.isfinite(terms)):
             return InvalidTrial("NONFINITE_STATE", "floating barrier-point evaluation contradicts feasible certificate", 1)
         self._eval += 1
-        state = State(theta, u, warped, terms, c, self._eval, image_grad=grad)
+        state = State(theta, u, warped, terms, c, self._eval, image_grad=grad, active=active)
         if diff is not None:
             state.differences = ((base.eval_id, self._reference_version), diff)
         return state
@@ -204,7 +205,7 @@ class Registration:
 
     def outer_norms(self, state):
         if state.norms is None:
-            gF, gD, gE = self.pair.outer_gradients(state.u, state.warped, state.image_grad)
+            gF, gD, gE = self.pair.outer_gradients(state.u, state.warped, state.image_grad, state.active)
             state.norms = (self.gnorm(gF), self.gnorm(gD), self.gnorm(gE))
         return state.norms
 
@@ -214,7 +215,8 @@ class Registration:
         if cached is not None and cached[0] == (base.eval_id, self._reference_version):
             dE, dF = cached[1]
         else:
-            dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped)
+            dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active,
+                                                 trial.active)
         rE = 16 * EPS * max(base.total, trial.total)
         rF = 16 * EPS * max(base.outer, trial.outer)
         return (-dE, rE), (-dF, rF)
@@ -239,7 +241,7 @@ class Registration:
         a, b = lam + alpha.value, mu / 2 + nu / 2
         inv_h2 = sum(1 / h ** 2 for h in self.grid.spacing)
         m = self.grid.omega * (a + b * (8 / 9) * inv_h2)
-        d = self.pair.ggn_diagonal(base.u, base.image_grad)
+        d = self.pair.ggn_diagonal(base.u, base.image_grad, base.active)
         # solvers/poisson_gradient.py:486: T73 always, T69 once this level has seen an undetermined certificate
         extend = config.metric_policy == T73_POLICY or (
             config.metric_policy == T69_POLICY and memory is not None and memory.uncertain > 0)
@@ -429,7 +431,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         final = accepted_steps >= config.max_iterations
         if final:
             # the last gradient of the solve: the joint outer triple (same gE), reused by the outer norms
-            gF, gD, g = reg.pair.outer_gradients(base.u, base.warped, base.image_grad)
+            gF, gD, g = reg.pair.outer_gradients(base.u, base.warped, base.image_grad, base.active)
             S.dot(0, g, g)
             S.dot(1, gF, gF)
             S.dot(2, gD, gD)
@@ -444,7 +446,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         # One batch of device work and one synchronisation per step: the gradient and its norm, (the metric on the
         # first step,) the direction, the slope, the BB2 secant products and the domain bound.  The decisions below
         # are taken in the reference's order on the same values.
-        g = reg.pair.gradient(base.u, base.warped, base.image_grad)
+        g = reg.pair.gradient(base.u, base.warped, base.image_grad, active=base.active)
         S.dot(0, g, g)
         metric_error = None
         if metric is None:
@@ -486,11 +488,15 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         for attempt in range(config.max_backtracks + 1):
             candidate = axpy(base.theta, tau, p)
             required = -config.c1 * tau * slope
+            # the step ratio's maxima ride along: their copy completes under the trial's own synchronisations
+            S.max_abs_diff(7, candidate, base.theta)
+            S.copy_async()
             trial = reg.evaluate_trial(candidate, observer=memory.certificate, base=base)
             valid = not isinstance(trial, InvalidTrial)
             actual = resolution = None
             if valid:
-                relative = reg.step_ratio(candidate, base.theta)
+                v = S.values()
+                relative = float(v[7] / max(reg.length, v[8]))
                 (actual, resolution), _ = reg.stable_reductions(base, trial)
                 certified = actual - resolution
                 accepted = certified > 0 and certified >= required

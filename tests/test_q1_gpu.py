@@ -92,12 +92,23 @@ def test_one_pass_trial_matches_separate_passes(gold):
     w2, g2 = P.warp(u2, with_gradient=True)
     terms, bad = P.energy(u2, w2)
     diff = P.energy_difference(u1, w1, u2, w2)
-    tw, tg, tterms, tbad, tdiff = P.trial_energy(u1, w1, u2)
+    tw, tg, tterms, tbad, tdiff, act2 = P.trial_energy(u1, w1, u2)
     assert torch.equal(tw, w2) and torch.equal(tg, g2)
     assert same_bits(tterms, terms) and tbad == bad
     assert same_bits(np.array(tdiff), np.array(diff))
-    tw, none, tterms, tbad, tdiff = P.trial_energy(u1, w1, u2, with_gradient=False)
+    tw, none, tterms, tbad, tdiff, _ = P.trial_energy(u1, w1, u2, with_gradient=False)
     assert none is None and torch.equal(tw, w2) and same_bits(tterms, terms)
+    # barrier activity masks only skip work: with the states' masks (from their own evaluations as trials) the
+    # values are bitwise the same; u1 has active cells (the fixture's barrier is active) and inactive ones
+    act1 = P.trial_energy(u2, w2, u1)[5]
+    assert 0 < int(act1.sum()) < act1.numel()
+    assert same_bits(np.array(P.energy_difference(u1, w1, u2, w2, act1, act2)), np.array(diff))
+    # the gradient, the outer triple and the GGN diagonal with u1's mask: bitwise the unmasked values
+    for term in ("total", "barrier"):
+        assert torch.equal(P.gradient(u1, w1, g1, term, active=act1), P.gradient(u1, w1, g1, term))
+    for a, b in zip(P.outer_gradients(u1, w1, g1, act1), P.outer_gradients(u1, w1, g1)):
+        assert torch.equal(a, b)
+    assert torch.equal(P.ggn_diagonal(u1, g1, act1), P.ggn_diagonal(u1, g1))
 
 
 def test_poisson_metric_direction(gold):
