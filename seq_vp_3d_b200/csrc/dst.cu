@@ -117,6 +117,15 @@ __global__ void __launch_bounds__(256) gemm_right_kernel(const double *__restric
 // output rows of one parity need only half the columns, against the folded input u_k = x_k + x_(n-1-k) (even i;
 // u_mid = x_mid when n is odd) or v_k = x_k - x_(n-1-k) (odd i): half the FLOPs of the dense product.  The folded
 // half matrices are stored per parity, H0 (ceil(n/2) x ceil(n/2)) then H1 (floor(n/2) x floor(n/2)), row-major.
+// FP64 tensor-core product D = A B + D on one 8x8x4 tile (mma.sync m8n8k4 f64): lane (g = lane / 4, t = lane % 4)
+// holds A[g][t], B[t][g] and D[g][2t], D[g][2t + 1].  FP64 has no tcgen05 kind on sm_100a; this is B200's FP64
+// tensor path, one instruction per 256 fused multiply-adds.
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
 // TC: the arithmetic type of a pass (double in the plain form, float in the mixed form); inputs and outputs may be
 // either (the mixed form reads the float64 right-hand side and writes the float64 direction).
 template <class TC>
@@ -135,24 +144,28 @@ __device__ __forceinline__ TC folded(const TI *__restrict__ x, const double *__r
     return (TC)(g ? xa - xb : xa + xb);
 }
 
-// Left pass: C[b][i][w] = sum_k S[i][k] X[b][k][w] (rows of length W, stride ldx, batch stride bs).  blockIdx.y
-// enumerates the 64-row tiles of parity 0, then of parity 1.  EPI 1 divides by den[flat % per], EPI 2 multiplies
+// Left pass: C[b][i][w] = sum_k S[i][k] X[b][k][w] (rows of length W, stride ldx, batch stride bs).  blockIdx.x
+// enumerates the 64-row tiles of parity 0, then of parity 1 (the blocks that read the same X run together).  EPI 1 divides by den[flat % per], EPI 2 multiplies
 // by sign * post[flat] (the same operation order as the separate elementwise passes).
 template <int EPI, class TC, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long W,
                                                        long long ldx, long long bs, TO *__restrict__ C,
                                                        const double *__restrict__ den, long long per,
                                                        const double *__restrict__ post, double sign) {
-    __shared__ TC sM[TK][TM + 1];
-    __shared__ TC sX[TK][TN];
+    __shared__ TC sM[TK][TM + 4];
+    __shared__ TC sX[TK][TN + 4];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    constexpr bool kTensor = sizeof(TC) == 8;    // float64 passes on the FP64 tensor path
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;   // a warp's 16 x 32 block of the 64 x 64 tile
+    double dacc[2][4][2] = {};
     const int t0 = (D.k0 + TM - 1) / TM;
-    const int g = blockIdx.y < t0 ? 0 : 1;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
     const int rows = g ? D.k1 : D.k0, K = rows;
     const TC *H = g ? D.h1 : D.h0;
-    const int i0 = (g ? blockIdx.y - t0 : blockIdx.y) * TM;
+    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
     const long long b = blockIdx.z;
-    const long long w0 = (long long)blockIdx.x * TN;
+    const long long w0 = (long long)blockIdx.y * TN;
     const TI *Xb = X + b * bs;
     TC acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += TK) {
@@ -170,35 +183,56 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
                                           : TC(0);
         }
         __syncthreads();
+        if constexpr (kTensor) {
 #pragma unroll
-        for (int kk = 0; kk < TK; kk++) {
-            TC a[4], x[4];
+            for (int kb = 0; kb < TK; kb += 4) {
+                double a[2], x[4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) a[r] = sM[kk][ty + 16 * r];
+                for (int fr = 0; fr < 2; fr++) a[fr] = sM[kb + tig][wr + 8 * fr + gid];
 #pragma unroll
-            for (int c = 0; c < 4; c++) x[c] = sX[kk][tx + 16 * c];
+                for (int fc = 0; fc < 4; fc++) x[fc] = sX[kb + tig][wc + 8 * fc + gid];
 #pragma unroll
-            for (int r = 0; r < 4; r++)
+                for (int fr = 0; fr < 2; fr++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], x[c], acc[r][c]);
+                    for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < TK; kk++) {
+                TC a[4], x[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) a[r] = sM[kk][ty + 16 * r];
+#pragma unroll
+                for (int c = 0; c < 4; c++) x[c] = sX[kk][tx + 16 * c];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], x[c], acc[r][c]);
+            }
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        int ii = i0 + ty + 16 * r;
-        if (ii >= rows) continue;
+    auto store = [&](int ii, long long w, double v) {
+        if (ii >= rows || w >= W) return;
         long long i = 2 * ii + g;
+        long long o = b * bs + i * ldx + w;
+        if (EPI == 1) v = v / den[o % per];
+        if (EPI == 2) v = sign * (post[o] * v);
+        C[o] = (TO)v;
+    };
+    if constexpr (kTensor) {
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            long long w = w0 + tx + 16 * c;
-            if (w >= W) continue;
-            long long o = b * bs + i * ldx + w;
-            double v = (double)acc[r][c];
-            if (EPI == 1) v = v / den[o % per];
-            if (EPI == 2) v = sign * (post[o] * v);
-            C[o] = (TO)v;
-        }
+        for (int fr = 0; fr < 2; fr++)
+#pragma unroll
+            for (int fc = 0; fc < 4; fc++)
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    store(i0 + wr + 8 * fr + gid, w0 + wc + 8 * fc + 2 * tig + e, dacc[fr][fc][e]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) store(i0 + ty + 16 * r, w0 + tx + 16 * c, (double)acc[r][c]);
     }
 }
 
@@ -206,15 +240,19 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
 template <class TC, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long R,
                                                         const double *__restrict__ pre, TO *__restrict__ C) {
-    __shared__ TC sX[TK][TM + 1];
-    __shared__ TC sM[TK][TN + 1];
+    __shared__ TC sX[TK][TM + 4];
+    __shared__ TC sM[TK][TN + 4];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    constexpr bool kTensor = sizeof(TC) == 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+    double dacc[2][4][2] = {};
     const int t0 = (D.k0 + TN - 1) / TN;
-    const int g = blockIdx.y < t0 ? 0 : 1;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
     const int cols = g ? D.k1 : D.k0, K = cols;
     const TC *H = g ? D.h1 : D.h0;
-    const int i0 = (g ? blockIdx.y - t0 : blockIdx.y) * TN;
-    const long long r0 = (long long)blockIdx.x * TM;
+    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
+    const long long r0 = (long long)blockIdx.y * TM;
     const int n = D.n;
     TC acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += TK) {
@@ -230,28 +268,56 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
             sM[kk][ii] = (i < cols && k < K) ? H[(long long)i * K + k] : TC(0);
         }
         __syncthreads();
+        if constexpr (kTensor) {
 #pragma unroll
-        for (int kk = 0; kk < TK; kk++) {
-            TC a[4], m[4];
+            for (int kb = 0; kb < TK; kb += 4) {
+                double a[2], m[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) a[q] = sX[kk][ty + 16 * q];
+                for (int fr = 0; fr < 2; fr++) a[fr] = sX[kb + tig][wr + 8 * fr + gid];
 #pragma unroll
-            for (int c = 0; c < 4; c++) m[c] = sM[kk][tx + 16 * c];
+                for (int fc = 0; fc < 4; fc++) m[fc] = sM[kb + tig][wc + 8 * fc + gid];
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+                for (int fr = 0; fr < 2; fr++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) acc[q][c] = fma(a[q], m[c], acc[q][c]);
+                    for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], m[fc]);
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < TK; kk++) {
+                TC a[4], m[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) a[q] = sX[kk][ty + 16 * q];
+#pragma unroll
+                for (int c = 0; c < 4; c++) m[c] = sM[kk][tx + 16 * c];
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[q][c] = fma(a[q], m[c], acc[q][c]);
+            }
         }
         __syncthreads();
     }
+    if constexpr (kTensor) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        long long r = r0 + ty + 16 * q;
-        if (r >= R) continue;
+        for (int fr = 0; fr < 2; fr++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            int ii = i0 + tx + 16 * c;
-            if (ii < cols) C[r * n + 2 * ii + g] = (TO)acc[q][c];
+            for (int fc = 0; fc < 4; fc++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const long long r = r0 + wr + 8 * fr + gid;
+                    const int ii = i0 + wc + 8 * fc + 2 * tig + e;
+                    if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)dacc[fr][fc][e];
+                }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            long long r = r0 + ty + 16 * q;
+            if (r >= R) continue;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                int ii = i0 + tx + 16 * c;
+                if (ii < cols) C[r * n + 2 * ii + g] = (TO)acc[q][c];
+            }
         }
     }
 }
@@ -315,13 +381,13 @@ static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const do
     if (axis == 0) {
         SVP_REQUIRE(epi == 0, "dst_pass: x pass has no epilogue");
         long long R = 3 * n2 * n1;
-        dim3 grid((unsigned)div_up(R, TM), tiles);
+        dim3 grid(tiles, (unsigned)div_up(R, TM));      // the blocks that share rows run together (L2 reuse)
         { svp::KernelTimer _t("dst_right_kernel", s); SVP_LAUNCH((dst_right_kernel<TC, TI, TO><<<grid, 256, 0, s>>>(D, in, R, pre, out))); }
     } else {
         SVP_REQUIRE(!pre, "dst_pass: pre-scale only on the x pass");
         long long W = axis == 1 ? n0 : n1 * n0;
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
-        dim3 grid((unsigned)div_up(W, TN), tiles, (unsigned)(axis == 1 ? 3 * n2 : 3));
+        dim3 grid(tiles, (unsigned)div_up(W, TN), (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
         if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
         else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
