@@ -176,6 +176,19 @@ def kernel_counts(shape):
     }
 
 
+def phase_summary(phases, timers, steps):
+    """Mean host-clock seconds per pair of the pre-optimizer, the transfer and the certified loop, the device time of
+    the FP64 kernels (all inside the certified loop) and the loop's remainder: host control, syncs and launch gaps."""
+    if not phases:
+        return None
+    mean = lambda key: (None if phases[0][key] is None else float(np.mean([p[key] for p in phases])))
+    out = {k: mean(k) for k in ("preopt_s", "transfer_s", "certified_loop_s")}
+    fp64 = sum(ms for name, (_, ms) in timers.items() if not name.startswith(("pre_", "adam"))) / 1e3 / steps
+    out["fp64_kernels_s"] = fp64
+    out["loop_host_gap_s"] = out["certified_loop_s"] - fp64
+    return out
+
+
 # ------------------------------------------------------------------------------------------ CPU baseline
 def cpu_baseline(shape, fixed, moving, weights, slab, outer):
     """Time the oracle (the reference's CPU algorithm restated) per component on a z-slab of the pair and extrapolate
@@ -363,17 +376,23 @@ def main():
     outer_cfg, inner_cfg = SequentialConfig3D(max_iterations=args.outer), PGConfig3D()
     stream = torch.cuda.current_stream()
 
+    phases = []
+
     def step(f, m):
         if args.preopt:
             from seq_vp_3d_b200.preopt import register_pair
-            res, _ = register_pair(f, m, grid, weights, outer=args.outer, inner_config=inner_cfg,
-                                   precision=args.form)
+            res, record = register_pair(f, m, grid, weights, outer=args.outer, inner_config=inner_cfg,
+                                        precision=args.form)
             reg = None
         else:
             reg = Registration(grid, f, m, **weights, precision=args.form)
-            res = solve_sequential(reg, config=outer_cfg, inner_config=inner_cfg)
+            res, record = solve_sequential(reg, config=outer_cfg, inner_config=inner_cfg), {}
         if not res.certified:
             raise RuntimeError(f"registration ended without a certified state: {res.status}")
+        # host-clock phases of the pair (the certified loop's figure includes its host control)
+        phases.append(dict(preopt_s=record.get("preopt", {}).get("seconds"),
+                           transfer_s=record.get("transfer", {}).get("elapsed_seconds"),
+                           certified_loop_s=res.elapsed_seconds))
         return reg, res
 
     def barrier():
@@ -393,6 +412,7 @@ def main():
 
     for _ in range(args.warmup):
         step(f_dev, m_dev)
+    phases.clear()
     # ---------------------------------------------------------------- timed: device-resident inputs
     launches0 = ctypes.c_int64()
     _lib.call("svp_counters", ctypes.byref(launches0))
@@ -417,6 +437,7 @@ def main():
             timers[name] = (cnt.value, ms.value)
     _lib.call("svp_timers_enable", 0)
     value = world * args.steps / seconds * 3600.
+    timed_phases = phases[:args.steps]
     # ---------------------------------------------------------------- e2e: public API from pinned host buffers
     f_host = torch.from_numpy(fixed).pin_memory()
     m_host = torch.from_numpy(moving).pin_memory()
@@ -481,7 +502,8 @@ def main():
                     clocks=clocks.summary(),
                     result=dict(status=r.status, certified=bool(r.certified), outer_accepted=r.counts["outer_accepted"],
                                 trials=r.counts["trials"], native_mse=r.native_mse, final_mse=r.final_mse,
-                                GF_initial=r.GF_initial, GF_final=r.GF_final))
+                                GF_initial=r.GF_initial, GF_final=r.GF_final),
+                    phases=phase_summary(timed_phases, timers, args.steps))
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

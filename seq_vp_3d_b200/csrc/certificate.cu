@@ -1006,6 +1006,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     if (acc.invalid) { out->status = ST_INFEASIBLE; out->reason = R_DOMAIN; return SVP_OK; }
     long long n1 = counts[0], n2 = n1;
     const long long *list2 = c->list1;
+    const bool staged = n1 != 0;   // a later stage updates acc; with no flagged cell the copy above is final
     if (c->cfg.prescreen && n1) {
         { svp::KernelTimer _t("prescreen_kernel", s); SVP_LAUNCH(prescreen_kernel<<<blocks_for(n1, 128, 8), 128, 0, s>>>(u, c->cg, c->list1, n1, c->pk, c->lower)); }
         SVP_LAUNCH_CHECK("prescreen_kernel");
@@ -1046,8 +1047,10 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
             SVP_LAUNCH_CHECK("verdict stage");
         }
     }
-    SVP_CUDA(cudaMemcpyAsync(&acc, c->acc, sizeof acc, cudaMemcpyDeviceToHost, s));
-    SVP_CUDA(cudaStreamSynchronize(s));
+    if (staged) {
+        SVP_CUDA(cudaMemcpyAsync(&acc, c->acc, sizeof acc, cudaMemcpyDeviceToHost, s));
+        SVP_CUDA(cudaStreamSynchronize(s));
+    }
     // the record (feasibility.py:755-771)
     long long fallback = n2;
     long long unknown = (long long)acc.unknown, bad = (long long)acc.bad;

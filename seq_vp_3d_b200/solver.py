@@ -222,12 +222,14 @@ class Registration:
         return (-dE, rE), (-dF, rF)
 
     def step_ratio(self, candidate, theta):
+        """(max|candidate - theta| / max(length, max|theta|), whether the two vectors are equal): the maximum is
+        zero exactly when every entry is equal (finite vectors; -0 equals +0, as torch.equal has it)."""
         from . import _lib
         import ctypes
         from .device import ptr, stream_ptr
         out = (ctypes.c_double * 2)()
         _lib.call("svp_max_abs_diff", ptr(candidate), ptr(theta), candidate.numel(), out, stream_ptr())
-        return float(out[0] / max(self.length, out[1]))
+        return float(out[0] / max(self.length, out[1])), out[0] == 0.
 
     def metric(self, base, config, memory=None):
         """(a, b, S~) of the T62 conservative metric (solvers/poisson_gradient.py:400 _pg_metric_inverse)."""
@@ -596,11 +598,10 @@ def solve_sequential(reg, theta0=None, *, config=None, inner_config=None, budget
         total = fixed = None
         if True:
             GFa, GDa, GEa = reg.outer_norms(candidate)
-            relative = reg.step_ratio(candidate.theta, start.theta)
+            relative, same = reg.step_ratio(candidate.theta, start.theta)
             total, fixed = reg.stable_reductions(start, candidate)
             cert = (total[0] - total[1]) > 0 and (fixed[0] - fixed[1]) > 0
             eligible = inner.status in ("converged_gradient", "max_iterations", "stagnated")
-            same = bool(torch.equal(candidate.theta, start.theta))
             accepted = bool(eligible and cert and not same)
             reason = ("ACCEPTED" if accepted else "INNER_FAILED_NOT_COMMITTED" if not eligible
                       else "NO_PROGRESS" if same else "DESCENT_CERTIFICATE_FAILED")
