@@ -176,6 +176,12 @@ def kernel_counts(shape):
     }
 
 
+# kernels timed for the profile and the phase split only: their work depends on the state (the certificate stages
+# run on the cells the edge hull leaves unproven, the node-measure extension on candidate cells)
+STATE_DEPENDENT_KERNELS = ("prescreen_kernel", "fallback_grid_kernel", "classify_kernel", "jd_extension_kernel",
+                           "jd_root_kernel", "cell_ggn_hvp_kernel")
+
+
 def phase_summary(phases, timers, steps):
     """Mean host-clock seconds per pair of the pre-optimizer, the transfer and the certified loop, the device time of
     the FP64 kernels (all inside the certified loop) and the loop's remainder: host control, syncs and launch gaps."""
@@ -430,7 +436,7 @@ def main():
     launches1 = ctypes.c_int64()
     _lib.call("svp_counters", ctypes.byref(launches1))
     timers = {}
-    for name in kernel_counts(shape):
+    for name in (*kernel_counts(shape), *STATE_DEPENDENT_KERNELS):
         cnt, ms = ctypes.c_int64(), ctypes.c_double()
         _lib.call("svp_timer_read", name.encode(), ctypes.byref(cnt), ctypes.byref(ms))
         if cnt.value:
@@ -461,7 +467,8 @@ def main():
 
     if rank == 0:
         counts = kernel_counts(shape)
-        dominant = max(timers, key=lambda k: timers[k][1]) if timers else None
+        counted = {k: v for k, v in timers.items() if k in counts}
+        dominant = max(counted, key=lambda k: counted[k][1]) if counted else None
         hbm, kind = peaks()
         roofline = None
         if dominant:

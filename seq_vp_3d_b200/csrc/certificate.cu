@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "svp_common.cuh"
@@ -104,7 +105,21 @@ struct PrescreenConst {
     double D[3 * 27 * 8];  // closed27 Q1 derivative table (3, 27, 8), passed by value (constant bank)
     double g12, g6, g3, sq27, eta;
     int usable;            // 0: table not finite or has a subnormal entry -> every bound NaN
+    int sparse;            // 1: every structurally vanishing entry (table_nonzero false) is exactly zero
 };
+
+// D[j][p][a] = (+-1/h_j) f_k f_l over the two axes k, l != j, with f = c (vertex bit 1) or 1 - c (bit 0) and c in
+// {0, 1/2, 1} the point's coordinate: the entry vanishes exactly when some factor is 1 - 1 or 0.  Point
+// p = x + 3 y + 9 z, vertex a = x + 2 y + 4 z.
+__host__ __device__ constexpr bool table_nonzero(int j, int p, int a) {
+    const int c[3] = {p % 3, (p / 3) % 3, p / 9};
+    for (int k = 0; k < 3; k++) {
+        if (k == j) continue;
+        const int bit = (a >> k) & 1;
+        if ((bit == 1 && c[k] == 0) || (bit == 0 && c[k] == 2)) return false;
+    }
+    return true;
+}
 
 __device__ double prescreen_cell(const double *__restrict__ u, long long base, long long ny, long long nx,
                                  const PrescreenConst &k) {
@@ -172,14 +187,110 @@ __device__ double prescreen_cell(const double *__restrict__ u, long long base, l
     return finite ? rsub(low, bound) : __longlong_as_double(0x7FF8000000000000LL);
 }
 
+// The same bound with the 27 points unrolled and the vanishing table entries' terms left out of the 8-term sums
+// (about 55% of them).  For a finite u, bitwise prescreen_cell's value: a left-out term is a signed zero, so every
+// partial sum keeps its value (only the sign of a zero sum may differ), the magnitude sums add +0, and a zero's sign
+// cannot reach the bound (it enters products and sums that end in low - bound with bound > 0, and the min and max
+// compare -0 equal to +0).  certify_map runs the prescreen only on finite states.
+template <int P>
+__device__ __forceinline__ void prescreen_point(const double (&uv)[8][3], const PrescreenConst &k, double &b,
+                                                double &sigma, double &phi, double &big) {
+    double F[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double acc = 0., mag = 0.;
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                if (table_nonzero(j, P, a)) {
+                    double term = rmul(uv[a][r], k.D[(j * 27 + P) * 8 + a]);
+                    acc = radd(acc, term);
+                    mag = radd(mag, fabs(term));
+                }
+            }
+            F[r][j] = acc;
+            if (mag > sigma) sigma = mag;
+        }
+        F[r][r] = radd(F[r][r], 1.);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (fabs(F[r][j]) > phi) phi = fabs(F[r][j]);
+    double t0 = rmul(F[0][0], rsub(rmul(F[1][1], F[2][2]), rmul(F[1][2], F[2][1])));
+    double t1 = rmul(F[0][1], rsub(rmul(F[1][2], F[2][0]), rmul(F[1][0], F[2][2])));
+    double t2 = rmul(F[0][2], rsub(rmul(F[1][0], F[2][1]), rmul(F[1][1], F[2][0])));
+    double v = radd(radd(t0, t1), t2);
+    b = v;
+    if (fabs(v) > big) big = fabs(v);
+}
+template <int... Ps>
+__device__ __forceinline__ void prescreen_points(std::integer_sequence<int, Ps...>, const double (&uv)[8][3],
+                                                 const PrescreenConst &k, double *bs, int T, double &sigma,
+                                                 double &phi, double &big) {
+    double b;
+    ((prescreen_point<Ps>(uv, k, b, sigma, phi, big), bs[Ps * T] = b), ...);     // p = 0 .. 26 in order
+}
+// bs: the thread's 27-entry slice of shared memory (stride T), which holds the point values between the passes
+__device__ double prescreen_cell_sparse(const double *__restrict__ u, long long base, long long ny, long long nx,
+                                        const PrescreenConst &k, double *bs, int T) {
+    double uv[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        const long long off = (long long)(a >> 2) * ny * nx + (long long)((a >> 1) & 1) * nx + (a & 1);
+#pragma unroll
+        for (int r = 0; r < 3; r++) uv[a][r] = __ldg(u + 3 * (base + off) + r);
+    }
+    double sigma = 0., phi = 0., big = 0.;
+    prescreen_points(std::make_integer_sequence<int, 27>(), uv, k, bs, T, sigma, phi, big);
+    double b[27];
+#pragma unroll
+    for (int p = 0; p < 27; p++) b[p] = bs[p * T];
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        int stride = s == 0 ? 1 : (s == 1 ? 3 : 9);
+#pragma unroll
+        for (int p = 0; p < 27; p++)
+            if ((p / stride) % 3 == 1) b[p] = rsub(rmul(2., b[p]), rmul(.5, radd(b[p - stride], b[p + stride])));
+    }
+    double e = radd(rmul(k.g12, radd(sigma, phi)), k.eta);
+    double P = radd(phi, e);
+    double inner = radd(radd(rmul(rmul(3., P), P), rmul(rmul(3., P), e)), rmul(e, e));
+    double ej = radd(rmul(rmul(k.sq27, e), inner), rmul(rmul(rmul(rmul(6., k.g6), P), P), P));
+    double bound = radd(rmul(1.01, radd(rmul(27., ej), rmul(rmul(135., k.g3), big))), k.eta);
+    double low = __longlong_as_double(0x7FF0000000000000LL);
+    bool finite = true;
+#pragma unroll
+    for (int p = 0; p < 27; p++) {
+        double w = b[p];
+        if (!(w == w) || !finite64(w)) finite = false;
+        else if (w < low) low = w;
+    }
+    if (!(bound == bound) || !finite64(bound) || !(sigma == sigma) || !finite64(sigma)) finite = false;
+    return finite ? rsub(low, bound) : __longlong_as_double(0x7FF8000000000000LL);
+}
+
+template <bool SPARSE>
 __global__ void __launch_bounds__(128) prescreen_kernel(const double *__restrict__ u, CellGrid g,
                                                         const long long *__restrict__ cells, long long n,
                                                         const PrescreenConst k, double *__restrict__ out) {
+    __shared__ double slice[27 * 128];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
-        out[i] = k.usable ? prescreen_cell(u, cell_base(cells[i], g), g.ny, g.nx, k)
-                          : __longlong_as_double(0x7FF8000000000000LL);
+        const long long base = cell_base(cells[i], g);
+        out[i] = !k.usable ? __longlong_as_double(0x7FF8000000000000LL)
+                 : SPARSE  ? prescreen_cell_sparse(u, base, g.ny, g.nx, k, slice + threadIdx.x, blockDim.x)
+                           : prescreen_cell(u, base, g.ny, g.nx, k);
     }
+}
+void launch_prescreen(const double *u, const CellGrid &g, const long long *cells, long long n,
+                      const PrescreenConst &k, double *out, cudaStream_t s) {
+    if (k.sparse)
+        prescreen_kernel<true><<<blocks_for(n, 128, 8), 128, 0, s>>>(u, g, cells, n, k, out);
+    else
+        prescreen_kernel<false><<<blocks_for(n, 128, 8), 128, 0, s>>>(u, g, cells, n, k, out);
 }
 
 // ============================================================================================== 3a. fallback arrays
@@ -779,10 +890,12 @@ PrescreenConst prescreen_const(const double h[3]) {
     k.sq27 = 5.196152422706633;
     k.eta = 1e-290;
     k.usable = 1;
+    k.sparse = 1;
     for (int i = 0; i < 3 * 27 * 8; i++) {
         double x = k.D[i];
         if (!std::isfinite(x)) k.usable = 0;
         if (x != 0 && std::fabs(x) < 2.2250738585072014e-308) k.usable = 0;
+        if (x != 0 && !table_nonzero(i / 216, (i / 8) % 27, i % 8)) k.sparse = 0;
     }
     return k;
 }
@@ -808,8 +921,7 @@ extern "C" int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, co
     SVP_REQUIRE(u && cells && out, "svp_prescreen_lower_bounds: null pointer");
     CellGrid cg = cell_grid(g);
     PrescreenConst k = prescreen_const(cg.h);
-    { svp::KernelTimer _t("prescreen_kernel", (cudaStream_t)stream); SVP_LAUNCH(prescreen_kernel<<<blocks_for(n, 128, 8), 128, 0, (cudaStream_t)stream>>>(u, cg, (const long long *)cells, n, k,
-                                                                               out)); }
+    { svp::KernelTimer _t("prescreen_kernel", (cudaStream_t)stream); SVP_LAUNCH(launch_prescreen(u, cg, (const long long *)cells, n, k, out, (cudaStream_t)stream)); }
     SVP_LAUNCH_CHECK("prescreen_kernel");
     return SVP_OK;
 }
@@ -1008,7 +1120,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     const long long *list2 = c->list1;
     const bool staged = n1 != 0;   // a later stage updates acc; with no flagged cell the copy above is final
     if (c->cfg.prescreen && n1) {
-        { svp::KernelTimer _t("prescreen_kernel", s); SVP_LAUNCH(prescreen_kernel<<<blocks_for(n1, 128, 8), 128, 0, s>>>(u, c->cg, c->list1, n1, c->pk, c->lower)); }
+        { svp::KernelTimer _t("prescreen_kernel", s); SVP_LAUNCH(launch_prescreen(u, c->cg, c->list1, n1, c->pk, c->lower, s)); }
         SVP_LAUNCH_CHECK("prescreen_kernel");
         SVP_LAUNCH(prescreen_stage_kernel<<<blocks_for(n1, 256, 8), 256, 0, s>>>(c->lower, n1, delta, c->sel, c->acc));
         SVP_LAUNCH_CHECK("prescreen stage");

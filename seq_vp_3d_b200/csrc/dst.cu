@@ -134,26 +134,63 @@ struct HalfDstT {
     int n, k0, k1;     // n, ceil(n/2), floor(n/2)
 };
 using HalfDst = HalfDstT<double>;
-// the fold is formed in float64 and rounded once to the pass's type
-template <class TC, class TI>
-__device__ __forceinline__ TC folded(const TI *__restrict__ x, const double *__restrict__ pre, long long a,
-                                     long long b, int g) {
-    double xa = pre ? pre[a] * (double)x[a] : (double)x[a];
-    if (a == b) return (TC)xa;
-    double xb = pre ? pre[b] * (double)x[b] : (double)x[b];
-    return (TC)(g ? xa - xb : xa + xb);
+// Tile product of one K block held in shared memory: FP64 tensor path (8 warps x 16 x 32 outputs as 2 x 4 DMMA
+// tiles; A fragments from sA[k][row], B from sB[k][col]) or, for float, 256 threads x 4 x 4 FMA outputs.
+template <class TC>
+__device__ __forceinline__ void tile_product(const TC (*sA)[TM + 4], const TC (*sB)[TN + 4], int lane, int warp,
+                                             double (&dacc)[2][4][2], TC (&acc)[4][4]) {
+    if constexpr (sizeof(TC) == 8) {
+        const int gid = lane >> 2, tig = lane & 3;
+        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+#pragma unroll
+        for (int kb = 0; kb < TK; kb += 4) {
+            double a[2], x[4];
+#pragma unroll
+            for (int fr = 0; fr < 2; fr++) a[fr] = sA[kb + tig][wr + 8 * fr + gid];
+#pragma unroll
+            for (int fc = 0; fc < 4; fc++) x[fc] = sB[kb + tig][wc + 8 * fc + gid];
+#pragma unroll
+            for (int fr = 0; fr < 2; fr++)
+#pragma unroll
+                for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
+        }
+    } else {
+        const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+#pragma unroll
+        for (int kk = 0; kk < TK; kk++) {
+            TC a[4], x[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) a[r] = sA[kk][ty + 16 * r];
+#pragma unroll
+            for (int c = 0; c < 4; c++) x[c] = sB[kk][tx + 16 * c];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], x[c], acc[r][c]);
+        }
+    }
+}
+
+// One K block of the folded operand: the raw pair (x_k, x_(n-1-k)) of each of a thread's 4 entries is fetched into
+// registers one block ahead (the loads fly while the previous block's products run) and folded when it is stored
+// to shared memory.  fold = x_k (middle row of odd n), x_k + x_m (parity 0) or x_k - x_m (parity 1), formed in
+// float64 (with the optional pre-scale) and rounded once to the pass's type; entries outside the operand are +0.
+template <class TC>
+__device__ __forceinline__ TC fold_value(double xa, double xb, bool mid, int g) {
+    return (TC)(mid ? xa : (g ? xa - xb : xa + xb));
 }
 
 // Left pass: C[b][i][w] = sum_k S[i][k] X[b][k][w] (rows of length W, stride ldx, batch stride bs).  blockIdx.x
-// enumerates the 64-row tiles of parity 0, then of parity 1 (the blocks that read the same X run together).  EPI 1 divides by den[flat % per], EPI 2 multiplies
-// by sign * post[flat] (the same operation order as the separate elementwise passes).
+// enumerates the 64-row tiles of parity 0, then of parity 1 (the blocks that read the same X run together).  EPI 1
+// divides by den[flat % per], EPI 2 multiplies by sign * post[flat] (the same operation order as the separate
+// elementwise passes).  Two shared-memory buffers: block k + 1 is stored while block k is multiplied.
 template <int EPI, class TC, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long W,
                                                        long long ldx, long long bs, TO *__restrict__ C,
                                                        const double *__restrict__ den, long long per,
                                                        const double *__restrict__ post, double sign) {
-    __shared__ TC sM[TK][TM + 4];
-    __shared__ TC sX[TK][TN + 4];
+    __shared__ TC sM[2][TK][TM + 4];
+    __shared__ TC sX[2][TK][TN + 4];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     constexpr bool kTensor = sizeof(TC) == 8;    // float64 passes on the FP64 tensor path
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
@@ -168,49 +205,43 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
     const long long w0 = (long long)blockIdx.y * TN;
     const TI *Xb = X + b * bs;
     TC acc[4][4] = {};
+    TC rm[4];
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            {
+                const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
+                rm[t] = (i < rows && k < K) ? H[(long long)i * K + k] : TC(0);
+            }
+            const int ww = e % TN, kk = e / TN, k = k0 + kk;
+            const long long w = w0 + ww;
+            const bool ok = k < K && w < W;
+            ra[t] = ok ? (double)Xb[(long long)k * ldx + w] : 0.;
+            rb[t] = ok ? (double)Xb[(long long)(D.n - 1 - k) * ldx + w] : 0.;
+        }
+    };
+    auto stash = [&](int buf, int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            sM[buf][e % TK][e / TK] = rm[t];
+            const int ww = e % TN, kk = e / TN, k = k0 + kk;
+            sX[buf][kk][ww] = fold_value<TC>(ra[t], rb[t], k == D.n - 1 - k, g);
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
     for (int k0 = 0; k0 < K; k0 += TK) {
-        for (int e = threadIdx.x; e < TK * TM; e += 256) {
-            int kk = e % TK, ii = e / TK;
-            int i = i0 + ii, k = k0 + kk;
-            sM[kk][ii] = (i < rows && k < K) ? H[(long long)i * K + k] : TC(0);
-        }
-        for (int e = threadIdx.x; e < TK * TN; e += 256) {
-            int ww = e % TN, kk = e / TN;
-            long long w = w0 + ww;
-            int k = k0 + kk;
-            sX[kk][ww] = (k < K && w < W) ? folded<TC>(Xb, nullptr, (long long)k * ldx + w,
-                                                       (long long)(D.n - 1 - k) * ldx + w, g)
-                                          : TC(0);
-        }
+        const bool more = k0 + TK < K;
+        if (more) fetch(k0 + TK);
+        tile_product<TC>(sM[buf], sX[buf], lane, warp, dacc, acc);
+        if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
-        if constexpr (kTensor) {
-#pragma unroll
-            for (int kb = 0; kb < TK; kb += 4) {
-                double a[2], x[4];
-#pragma unroll
-                for (int fr = 0; fr < 2; fr++) a[fr] = sM[kb + tig][wr + 8 * fr + gid];
-#pragma unroll
-                for (int fc = 0; fc < 4; fc++) x[fc] = sX[kb + tig][wc + 8 * fc + gid];
-#pragma unroll
-                for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-                    for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
-            }
-        } else {
-#pragma unroll
-            for (int kk = 0; kk < TK; kk++) {
-                TC a[4], x[4];
-#pragma unroll
-                for (int r = 0; r < 4; r++) a[r] = sM[kk][ty + 16 * r];
-#pragma unroll
-                for (int c = 0; c < 4; c++) x[c] = sX[kk][tx + 16 * c];
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], x[c], acc[r][c]);
-            }
-        }
-        __syncthreads();
+        buf ^= 1;
     }
     auto store = [&](int ii, long long w, double v) {
         if (ii >= rows || w >= W) return;
@@ -240,8 +271,8 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
 template <class TC, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long R,
                                                         const double *__restrict__ pre, TO *__restrict__ C) {
-    __shared__ TC sX[TK][TM + 4];
-    __shared__ TC sM[TK][TN + 4];
+    __shared__ TC sX[2][TK][TM + 4];
+    __shared__ TC sM[2][TK][TN + 4];
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     constexpr bool kTensor = sizeof(TC) == 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
@@ -255,47 +286,44 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
     const long long r0 = (long long)blockIdx.y * TM;
     const int n = D.n;
     TC acc[4][4] = {};
+    TC rm[4];
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            {
+                const int kk = e % TK, rr = e / TK, k = k0 + kk;
+                const long long r = r0 + rr;
+                const bool ok = r < R && k < K;
+                const long long a = r * n + k, m = r * n + (n - 1 - k);
+                ra[t] = ok ? (pre ? pre[a] * (double)X[a] : (double)X[a]) : 0.;
+                rb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
+            }
+            const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
+            rm[t] = (i < cols && k < K) ? H[(long long)i * K + k] : TC(0);
+        }
+    };
+    auto stash = [&](int buf, int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            const int kk = e % TK, k = k0 + kk;
+            sX[buf][kk][e / TK] = fold_value<TC>(ra[t], rb[t], k == n - 1 - k, g);
+            sM[buf][kk][e / TK] = rm[t];
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
     for (int k0 = 0; k0 < K; k0 += TK) {
-        for (int e = threadIdx.x; e < TK * TM; e += 256) {
-            int kk = e % TK, rr = e / TK;
-            long long r = r0 + rr;
-            int k = k0 + kk;
-            sX[kk][rr] = (r < R && k < K) ? folded<TC>(X, pre, r * n + k, r * n + (n - 1 - k), g) : TC(0);
-        }
-        for (int e = threadIdx.x; e < TK * TN; e += 256) {
-            int kk = e % TK, ii = e / TK;
-            int i = i0 + ii, k = k0 + kk;
-            sM[kk][ii] = (i < cols && k < K) ? H[(long long)i * K + k] : TC(0);
-        }
+        const bool more = k0 + TK < K;
+        if (more) fetch(k0 + TK);
+        tile_product<TC>(sX[buf], sM[buf], lane, warp, dacc, acc);
+        if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
-        if constexpr (kTensor) {
-#pragma unroll
-            for (int kb = 0; kb < TK; kb += 4) {
-                double a[2], m[4];
-#pragma unroll
-                for (int fr = 0; fr < 2; fr++) a[fr] = sX[kb + tig][wr + 8 * fr + gid];
-#pragma unroll
-                for (int fc = 0; fc < 4; fc++) m[fc] = sM[kb + tig][wc + 8 * fc + gid];
-#pragma unroll
-                for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-                    for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], m[fc]);
-            }
-        } else {
-#pragma unroll
-            for (int kk = 0; kk < TK; kk++) {
-                TC a[4], m[4];
-#pragma unroll
-                for (int q = 0; q < 4; q++) a[q] = sX[kk][ty + 16 * q];
-#pragma unroll
-                for (int c = 0; c < 4; c++) m[c] = sM[kk][tx + 16 * c];
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc[q][c] = fma(a[q], m[c], acc[q][c]);
-            }
-        }
-        __syncthreads();
+        buf ^= 1;
     }
     if constexpr (kTensor) {
 #pragma unroll

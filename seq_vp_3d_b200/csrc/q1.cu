@@ -8,6 +8,7 @@
 // solvers/jd_affine.py, solvers/global_jd_step.py}.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "pair.cuh"
@@ -1468,13 +1469,23 @@ unsigned slice_blocks(const svp_pair *p) { return blocks_for(p->q.ncell, CS, 2 *
 // dynamic shared memory of the slice kernels: k doubles per thread
 constexpr size_t slice_bytes(int k) { return sizeof(double) * (size_t)k * CS; }
 int allow_slices() {
-    // the 108-value slices are above the 48 KB default; the attribute is per device context, so set it per call
+    // the 108-value slices are above the 48 KB default.  The attribute belongs to the device's context (the primary
+    // context torch and this library share), so it is set on the first call per device, not on every launch: a
+    // cudaFuncSetAttribute costs host time that the GPU then spends idle.
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    SVP_CUDA(cudaGetDevice(&dev));
+    SVP_REQUIRE(dev >= 0 && dev < 64, "allow_slices: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return SVP_OK;
     SVP_CUDA(cudaFuncSetAttribute(cell_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)slice_bytes(108)));
     SVP_CUDA(cudaFuncSetAttribute(cell_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)slice_bytes(108)));
     SVP_CUDA(cudaFuncSetAttribute(cell_trial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)slice_bytes(108)));
+    done[dev] = true;
     return SVP_OK;
 }
 unsigned node_blocks(long long n) { return blocks_for(n, 256, 8); }
