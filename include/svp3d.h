@@ -287,6 +287,11 @@ int svp_bb2_dots_dev(const double *theta, const double *theta_old, const double 
                      const double *p_old, const double *pvec, int64_t n, double *out4_dev, void *stream);
 int svp_max_abs_diff_dev(const double *a, const double *b, int64_t n, double *out2_dev, void *stream);
 int svp_step_bound_dev(const svp_grid *g, const double *u, const double *pvec, double *bound_dev, void *stream);
+/* One line-search trial point in one pass: candidate = fl(theta + fl(tau pvec)) exactly as svp_axpy, u = inject
+ * (candidate) exactly as svp_inject, and out2_dev (device) = (max |candidate - theta|, max |theta|) exactly as
+ * svp_max_abs_diff_dev(candidate, theta) (poisson_gradient.py:1245 trial theta; fast_checks.py:120 step ratio). */
+int svp_trial_point(const svp_grid *g, const double *theta, double tau, const double *pvec, double *candidate,
+                    double *u, double *out2_dev, void *stream);
 
 /* Image-curvature shift alpha = factor * mean over free nodes of (q/omega) |grad I(X+u)|^2 / 3
  * (solvers/poisson_gradient.py:269 image_curvature_shift).  alpha: host. */

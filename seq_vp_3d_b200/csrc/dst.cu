@@ -2,6 +2,8 @@
 // (jd_curl/three_d/poisson.py:99, scipy dstn type=1 norm='ortho') and the not-a-knot spline prefilter
 // (interpolation.py:29).  Each axis pass is a batched GEMM with a small square matrix.
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "pair.cuh"
@@ -452,10 +454,26 @@ std::vector<double> dst1_matrix(int n) {
     return S;
 }
 
+// The folded matrices depend only on n; registrations on one grid share them (n^2 long double sines per axis).
+static std::vector<double> cached_dst1_half(int n) {
+    static std::mutex mu;
+    static std::map<int, std::vector<double>> cache;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(n);
+        if (it != cache.end()) return it->second;
+    }
+    std::vector<double> H = dst1_half(n);
+    std::lock_guard<std::mutex> lock(mu);
+    if (cache.size() >= 32) cache.clear();
+    cache.emplace(n, H);
+    return H;
+}
+
 int pair_dst_setup(svp_pair *p) {
     const long long f[3] = {p->q.fx, p->q.fy, p->q.fz};
     for (int k = 0; k < 3; k++) {
-        std::vector<double> H = dst1_half((int)f[k]);
+        std::vector<double> H = cached_dst1_half((int)f[k]);
         SVP_CUDA(cudaMalloc((void **)&p->dst_half[k], sizeof(double) * H.size()));
         SVP_CUDA(cudaMemcpy(p->dst_half[k], H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice));
         std::vector<float> H32(H.begin(), H.end());      // the mixed form's matrices (rounded once)

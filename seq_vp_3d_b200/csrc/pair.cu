@@ -3,6 +3,8 @@
 // with the inverse collocation matrix (interpolation.py:29 build_image_sampler, SciPy make_interp_spline k=3).
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "pair.cuh"
@@ -79,6 +81,23 @@ std::vector<double> inverse_collocation(const std::vector<double> &x) {
     std::vector<double> out((size_t)n * n);
     for (size_t k = 0; k < out.size(); k++) out[k] = (double)I[k];
     return out;
+}
+
+// The inverse depends only on the axis nodes; registrations on one grid share it (it is O(n^3) in long double, tens
+// of milliseconds of host time per axis on a native grid).
+std::vector<double> cached_inverse_collocation(const std::vector<double> &x) {
+    static std::mutex mu;
+    static std::map<std::vector<double>, std::vector<double>> cache;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(x);
+        if (it != cache.end()) return it->second;
+    }
+    std::vector<double> inv = inverse_collocation(x);
+    std::lock_guard<std::mutex> lock(mu);
+    if (cache.size() >= 32) cache.clear();
+    cache.emplace(x, inv);
+    return inv;
 }
 
 Q1Const make_const(const svp_grid *g, const svp_weights *w) {
@@ -171,25 +190,32 @@ extern "C" int svp_pair_create(const svp_grid *g, const svp_weights *w, const do
             return bail(cuda_fail(e, "knots"));
         if ((e = cudaMemcpy(p->knots[k], t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(cuda_fail(e, "knots copy"));
-        inv[k] = inverse_collocation(x);
+        inv[k] = cached_inverse_collocation(x);
     }
+    // the prefilter's matrices and intermediate live in the stream-ordered scratch pool: freeing them does not
+    // synchronize the device (registrations on other streams keep running)
     double *mats[3] = {nullptr, nullptr, nullptr}, *tmp = nullptr;
-    for (int k = 0; k < 3; k++) {
-        if ((e = cudaMalloc((void **)&mats[k], sizeof(double) * inv[k].size())) != cudaSuccess)
-            return bail(cuda_fail(e, "prefilter matrix"));
-        cudaMemcpy(mats[k], inv[k].data(), sizeof(double) * inv[k].size(), cudaMemcpyHostToDevice);
+    int rc = SVP_OK;
+    for (int k = 0; k < 3 && !rc; k++) {
+        if ((e = scratch_alloc((void **)&mats[k], sizeof(double) * inv[k].size(), s)) != cudaSuccess)
+            rc = cuda_fail(e, "prefilter matrix");
+        else if ((e = cudaMemcpyAsync(mats[k], inv[k].data(), sizeof(double) * inv[k].size(), cudaMemcpyHostToDevice,
+                                      s)) != cudaSuccess)
+            rc = cuda_fail(e, "prefilter matrix copy");
     }
-    if ((e = cudaMalloc((void **)&tmp, sizeof(double) * nn)) != cudaSuccess) return bail(cuda_fail(e, "prefilter tmp"));
-    int rc = apply_axis(mats[2], 2, 1, g->nz, g->ny, g->nx, moving, tmp, s);
+    if (!rc && (e = scratch_alloc((void **)&tmp, sizeof(double) * nn, s)) != cudaSuccess)
+        rc = cuda_fail(e, "prefilter tmp");
+    if (!rc) rc = apply_axis(mats[2], 2, 1, g->nz, g->ny, g->nx, moving, tmp, s);
     if (!rc) rc = apply_axis(mats[1], 1, 1, g->nz, g->ny, g->nx, tmp, p->coeff, s);
     if (!rc) rc = apply_axis(mats[0], 0, 1, g->nz, g->ny, g->nx, p->coeff, tmp, s);
     if (!rc) {
         e = cudaMemcpyAsync(p->coeff, tmp, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) rc = cuda_fail(e, "coeff copy");
     }
-    cudaStreamSynchronize(s);
-    for (int k = 0; k < 3; k++) cudaFree(mats[k]);
-    cudaFree(tmp);
+    for (int k = 0; k < 3; k++)
+        if (mats[k]) scratch_free(mats[k], s);
+    if (tmp) scratch_free(tmp, s);
+    cudaStreamSynchronize(s);      // the host matrices above must outlive their copies
     if (rc) return bail(rc);
     if ((rc = pair_dst_setup(p))) return bail(rc);
     *out = p;

@@ -152,6 +152,47 @@ __global__ void max_abs_diff_kernel(const double *__restrict__ a, const double *
     }
 }
 
+// The trial point of a line-search attempt in one pass over the nodes: candidate = fl(theta + fl(tau p)) (axpy_kernel's
+// roundings), u = inject(candidate) (zero faces) and the keys of max |candidate - theta|, max |theta|
+// (max_abs_diff_kernel's), so the step ratio needs no second pass.
+__global__ void trial_point_kernel(long long nx, long long ny, long long nz, const double *__restrict__ theta,
+                                   double tau, const double *__restrict__ p, double *__restrict__ cand,
+                                   double *__restrict__ u, long long *keys) {
+    const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz, nn = nx * ny * nz;
+    long long k0 = 0, k1 = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
+        long long f = ((z - 1) * fy + (y - 1)) * fx + (x - 1);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (face) {
+                u[3 * i + r] = 0.;
+                continue;
+            }
+            const double t = theta[r * nf + f];
+            const double c = __dadd_rn(t, __dmul_rn(tau, p[r * nf + f]));
+            cand[r * nf + f] = c;
+            u[3 * i + r] = c;
+            double d = fabs(c - t), m = fabs(t);
+            long long kx = d != d ? 0x7FF8000000000000LL : __double_as_longlong(d);
+            long long ky = m != m ? 0x7FF8000000000000LL : __double_as_longlong(m);
+            k0 = kx > k0 ? kx : k0;
+            k1 = ky > k1 ? ky : k1;
+        }
+    }
+    for (int s = 16; s; s >>= 1) {
+        long long x = __shfl_xor_sync(0xFFFFFFFFu, k0, s), y = __shfl_xor_sync(0xFFFFFFFFu, k1, s);
+        k0 = x > k0 ? x : k0;
+        k1 = y > k1 ? y : k1;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(keys, k0);
+        atomicMax(keys + 1, k1);
+    }
+}
+
 // order keys -> doubles in place (the deferred form of the step-bound reduction)
 __global__ void keys_to_double_kernel(long long *keys, int n) {
     if (threadIdx.x < n) keys[threadIdx.x] = __double_as_longlong(key_value(keys[threadIdx.x]));
@@ -203,6 +244,18 @@ extern "C" int svp_max_abs_diff_dev(const double *a, const double *b, int64_t n,
     // the keys are the bits of the nonnegative maxima (NaN canonical): already the doubles
     SVP_LAUNCH(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
     SVP_LAUNCH_CHECK("max_abs_diff");
+    return SVP_OK;
+}
+
+extern "C" int svp_trial_point(const svp_grid *g, const double *theta, double tau, const double *pvec,
+                               double *candidate, double *u, double *out2_dev, void *stream) {
+    SVP_REQUIRE(grid_ok(g) && theta && pvec && candidate && u && out2_dev, "svp_trial_point: invalid argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    long long *keys = (long long *)out2_dev;
+    SVP_CUDA(cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s));
+    SVP_LAUNCH(trial_point_kernel<<<blocks_for(n_nodes(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, theta, tau, pvec,
+                                                                                candidate, u, keys));
+    SVP_LAUNCH_CHECK("trial_point_kernel");
     return SVP_OK;
 }
 

@@ -9,6 +9,9 @@ import hashlib
 import numpy as np
 
 
+_WEIGHT_TOTALS = {}
+
+
 class InputValidationError(ValueError):
     """A named input violates the numerical or layout contract (jd_curl.validation.InputValidationError)."""
 
@@ -46,6 +49,17 @@ class Grid3D:
     def node_weights(self):
         tx, ty, tz = self.trapezoid
         return self.omega * tz[:, None, None] * ty[None, :, None] * tx[None, None, :]
+
+    def node_weight_total(self):
+        """Sum of the node weights, accumulated in long double and rounded once; cached per grid id (it costs tens of
+        milliseconds on a native grid, and every registration on the grid needs it for its MSE)."""
+        total = _WEIGHT_TOTALS.get(self.grid_id)
+        if total is None:
+            total = float(np.sum(self.node_weights(), dtype=np.longdouble))
+            if len(_WEIGHT_TOTALS) >= 64:
+                _WEIGHT_TOTALS.clear()
+            _WEIGHT_TOTALS[self.grid_id] = total
+        return total
 
     def identity(self):
         x, y, z = self.axes

@@ -170,6 +170,16 @@ class DevicePair:
         _lib.call("svp_inject", ctypes.byref(self._g), ptr(theta), ptr(out), stream_ptr(stream))
         return out
 
+    def trial_point(self, theta, tau, p, maxima_dev, stream=None):
+        """(candidate, u) of a line-search trial in one pass: candidate = theta + tau p with axpy's roundings,
+        u = inject(candidate); maxima_dev (two device doubles, e.g. a Scalars slot pair) receives
+        (max |candidate - theta|, max |theta|)."""
+        cand = torch.empty_like(theta)
+        u = self.node(3)
+        _lib.call("svp_trial_point", ctypes.byref(self._g), ptr(theta), float(tau), ptr(p), ptr(cand), ptr(u),
+                  maxima_dev, stream_ptr(stream))
+        return cand, u
+
     def restrict(self, field, out=None, stream=None):
         out = self.free() if out is None else out
         _lib.call("svp_restrict", ctypes.byref(self._g), ptr(field), ptr(out), stream_ptr(stream))

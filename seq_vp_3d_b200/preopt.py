@@ -186,14 +186,19 @@ def preoptimize(fixed, moving, grid, config=None, stream=None):
 
 
 def boundary_taper(u, grid, L=4):
-    """preopt.py:617: nodes within L of a face scale linearly to zero on the face.  Returns (tapered u, weights)."""
+    """preopt.py:617: nodes within L of a face scale linearly to zero on the face.  Returns (tapered u, weights),
+    the weights on the input's side (a device u gets them formed on the device from the three axis profiles: the
+    same products in the same order as the host form)."""
     rs = []
     for n in grid.shape:
         k = np.arange(n)
         rs.append(np.minimum(np.minimum(k, n - 1 - k) / float(L), 1.))
-    w = rs[0][:, None, None] * rs[1][None, :, None] * rs[2][None, None, :]
-    wt = torch.as_tensor(w, device=u.device) if torch.is_tensor(u) else w
-    return (wt[..., None] * u), w
+    if torch.is_tensor(u):
+        r = [torch.as_tensor(a, device=u.device) for a in rs]
+        w = r[0][:, None, None] * r[1][None, :, None] * r[2][None, None, :]
+    else:
+        w = rs[0][:, None, None] * rs[1][None, :, None] * rs[2][None, None, :]
+    return (w[..., None] * u), w
 
 
 def transfer(seed, grid, certificate_config=None):

@@ -21,7 +21,7 @@ import torch
 
 from . import certificate as cert_mod
 from .device import to_device
-from .pair import DevicePair, Scalars, axpy, dot
+from .pair import DevicePair, Scalars, dot
 
 EPS = float(np.finfo(float).eps)
 InvalidTrial = namedtuple("InvalidTrial", "reason detail count")
@@ -133,7 +133,7 @@ class Registration:
         self.pair = DevicePair(grid, fixed, moving, u_ref, lam=lam, mu=mu, nu=nu, kappa=kappa,
                                activation=activation, delta=self.delta, precision=precision)
         self.certifier = cert_mod.certifier(grid, self.config)
-        self.q_sum = float(np.sum(grid.node_weights(), dtype=np.longdouble))
+        self.q_sum = grid.node_weight_total()
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0
         self._reference_version = 0
@@ -148,11 +148,12 @@ class Registration:
         rec = self.certifier.run(u)
         return cert_mod.result_from_record(rec, self.grid, self.config, None)
 
-    def evaluate_trial(self, theta, observer=None, base=None):
-        """Certify, warp and evaluate theta.  With the line search's base, the trial is warped (with its image
-        gradient, so promotion is free) and evaluated against the base in one pass, and the stable base -> trial
-        differences are kept for stable_reductions (bitwise the separate passes' values)."""
-        u = self.pair.inject(theta)
+    def evaluate_trial(self, theta, observer=None, base=None, u=None):
+        """Certify, warp and evaluate theta (u: its injected field, when the caller has it).  With the line search's
+        base, the trial is warped (with its image gradient, so promotion is free) and evaluated against the base in
+        one pass, and the stable base -> trial differences are kept for stable_reductions (bitwise the separate
+        passes' values)."""
+        u = self.pair.inject(theta) if u is None else u
         c = self.certify(u)
         if observer is not None:
             observer(c)
@@ -423,6 +424,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
     """One frozen-reference subproblem (solvers/poisson_gradient.py:1090)."""
     history, accepted_steps, small_steps = [], 0, 0
     previous, metric = None, None
+    pending = None          # the next step's gradient, launched as soon as its state was accepted
     G = None
 
     def finish(status, reason):
@@ -448,7 +450,9 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         # One batch of device work and one synchronisation per step: the gradient and its norm, (the metric on the
         # first step,) the direction, the slope, the BB2 secant products and the domain bound.  The decisions below
         # are taken in the reference's order on the same values.
-        g = reg.pair.gradient(base.u, base.warped, base.image_grad, active=base.active)
+        g = pending if pending is not None else reg.pair.gradient(base.u, base.warped, base.image_grad,
+                                                                  active=base.active)
+        pending = None
         S.dot(0, g, g)
         metric_error = None
         if metric is None:
@@ -488,12 +492,12 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         global_attempts = 0
         accepted = False
         for attempt in range(config.max_backtracks + 1):
-            candidate = axpy(base.theta, tau, p)
             required = -config.c1 * tau * slope
-            # the step ratio's maxima ride along: their copy completes under the trial's own synchronisations
-            S.max_abs_diff(7, candidate, base.theta)
+            # candidate, its field and the step ratio's maxima in one pass; the maxima's copy completes under the
+            # trial's own synchronisations
+            candidate, u_trial = reg.pair.trial_point(base.theta, tau, p, S.slot(7))
             S.copy_async()
-            trial = reg.evaluate_trial(candidate, observer=memory.certificate, base=base)
+            trial = reg.evaluate_trial(candidate, observer=memory.certificate, base=base, u=u_trial)
             valid = not isinstance(trial, InvalidTrial)
             actual = resolution = None
             if valid:
@@ -508,6 +512,10 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
                 reason = trial.reason
             if accepted:
                 reg.promote_trial(trial)
+                if accepted_steps + 1 < config.max_iterations:
+                    # the next iteration is not the final one, so it starts from this state's gradient: launch it
+                    # now, the bookkeeping below runs while the GPU computes it
+                    pending = reg.pair.gradient(trial.u, trial.warped, trial.image_grad, active=trial.active)
             exit_stop = False
             if (config.resolution_exit and not accepted and not reason.startswith("NONFINITE")
                     and global_attempts + 1 <= config.max_backtracks):

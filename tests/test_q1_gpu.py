@@ -227,6 +227,15 @@ def test_vector_kernels_bitwise(big):
         assert same_bits(got, theta + tau * p)
     assert torch.equal(P.inject(dev(theta)), dev(Q.inject(theta, OP.grid)))
     assert torch.equal(P.restrict(ud), dev(theta))
+    # the fused trial point: axpy's candidate, inject's field and max_abs_diff's maxima, bit for bit
+    S = pm.Scalars(4)
+    for tau in (0.37, 1e-3):
+        cand, uc = P.trial_point(dev(theta), tau, dev(p), S.slot(0))
+        S.max_abs_diff(2, pm.axpy(dev(theta), tau, dev(p)), dev(theta))
+        v = S.fetch()
+        assert same_bits(cand.cpu().numpy(), theta + tau * p)
+        assert torch.equal(uc, P.inject(cand))
+        assert same_bits(v[:2], v[2:4]) and v[0] == np.max(np.abs((theta + tau * p) - theta))
     assert abs(pm.dot(dev(theta), dev(p)) - float(np.dot(theta, p))) <= 1e-13 * np.abs(theta * p).sum()
     # step bound: exact min of the reference quotients
     v = p.reshape((3,) + OP.grid.interior_shape)
