@@ -23,9 +23,31 @@
 namespace svp {
 namespace {
 
+// Division by the spacing, x / h_j correctly rounded.  Where h_j is a power of two, 1/h_j is exact and x * (1/h_j) is
+// the same correctly rounded quotient (one rounding of the same exact value, subnormal and overflowing results
+// included), for a multiply instead of a division.
+struct AxisDiv {
+    double h[3], ih[3];
+    int pow2[3];
+};
+AxisDiv axis_div(const double h[3]) {
+    AxisDiv d;
+    for (int j = 0; j < 3; j++) {
+        int e = 0;
+        d.h[j] = h[j];
+        d.pow2[j] = std::isfinite(h[j]) && h[j] > 0 && std::frexp(h[j], &e) == .5 && e > -1000 && e < 1000;
+        d.ih[j] = d.pow2[j] ? 1. / h[j] : 0.;
+    }
+    return d;
+}
+__device__ __forceinline__ double div_axis(double x, const AxisDiv &d, int j) {
+    return d.pow2[j] ? rmul(x, d.ih[j]) : rdiv(x, d.h[j]);
+}
+
 struct CellGrid {
     long long nx, ny, nz, cx, cy, cz, ncell;
     double h[3];
+    AxisDiv div;
 };
 
 CellGrid cell_grid(const svp_grid *g) {
@@ -34,6 +56,7 @@ CellGrid cell_grid(const svp_grid *g) {
     c.cx = g->nx - 1; c.cy = g->ny - 1; c.cz = g->nz - 1;
     c.ncell = c.cx * c.cy * c.cz;
     c.h[0] = g->hx; c.h[1] = g->hy; c.h[2] = g->hz;
+    c.div = axis_div(c.h);
     return c;
 }
 
@@ -57,7 +80,8 @@ __device__ __forceinline__ int edge_start(int j, int e) {
 
 // ============================================================================================== 1. edge hull
 // F_rj interval: hull of the 4 edge differences (from +inf / -inf in edge order), outward, /h, outward, + identity.
-__device__ __forceinline__ bool hull_entry_v(const double v[8][3], int j, int r, double h, double &lo, double &hi) {
+__device__ __forceinline__ bool hull_entry_v(const double v[8][3], int j, int r, const AxisDiv &dv, double &lo,
+                                             double &hi) {
     bool ok = true;
     double lower = __longlong_as_double(0x7FF0000000000000LL), upper = -lower;
 #pragma unroll
@@ -70,7 +94,7 @@ __device__ __forceinline__ bool hull_entry_v(const double v[8][3], int j, int r,
     }
     double l, hh;
     ok &= iout(lower, upper, l, hh);
-    ok &= iout(rdiv(l, h), rdiv(hh, h), l, hh);
+    ok &= iout(div_axis(l, dv, j), div_axis(hh, dv, j), l, hh);
     double id = (r == j) ? 1.0 : 0.0;
     ok &= iadd(l, hh, id, id, lo, hi);
     return ok;
@@ -91,7 +115,7 @@ __global__ void __launch_bounds__(256) edge_hull_kernel(const double *__restrict
 #pragma unroll
         for (int j = 0; j < 3; j++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) ok &= hull_entry_v(v, j, r, g.h[j], fl[r][j], fh[r][j]);
+            for (int r = 0; r < 3; r++) ok &= hull_entry_v(v, j, r, g.div, fl[r][j], fh[r][j]);
         double jl, jh, ml, mh;
         ok &= idet(fl, fh, jl, jh);
         ok &= iout(rsub(jl, delta), rsub(jh, delta), ml, mh);
@@ -306,7 +330,7 @@ __device__ __forceinline__ double edge_weight(int j, int e, int p) {
 }
 
 // v: 24 vertex displacements (vertex-major); outputs with stride 1 (27 entries each); returns ok
-__device__ bool fallback_cell(const double v[24], const double h[3], double delta, double *plo, double *phi,
+__device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delta, double *plo, double *phi,
                               double *clo, double *chi, double *smp) {
     bool ok = true;
     double elo[3][4][3], ehi[3][4][3];
@@ -320,7 +344,7 @@ __device__ bool fallback_cell(const double v[24], const double h[3], double delt
                 double d = rsub(v[3 * b + r], v[3 * a + r]);
                 double sl, sh;
                 ok &= iout(d, d, sl, sh);
-                double x1 = rdiv(sl, h[j]), x2 = rdiv(sh, h[j]);
+                double x1 = div_axis(sl, dv, j), x2 = div_axis(sh, dv, j);
                 ok &= iout(nmin(nmin(nmin(x1, x1), x2), x2), nmax(nmax(nmax(x1, x1), x2), x2), elo[j][e][r],
                            ehi[j][e][r]);
             }
@@ -364,7 +388,17 @@ __device__ bool fallback_cell(const double v[24], const double h[3], double delt
         }
     }
     for (int p = 0; p < 27; p++) { clo[p] = blo[p]; chi[p] = bhi[p]; }
-    // float64 samples: F = I + sum_(j,e) ((v_b - v_a) / h) w, cofactors, ((0 + t0) + t1) + t2
+    // float64 samples: F = I + sum_(j,e) ((v_b - v_a) / h) w, cofactors, ((0 + t0) + t1) + t2; the 36 edge
+    // quotients do not depend on the point and are formed once
+    double dq[3][4][3];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            int a = edge_start(j, e), b = a | (1 << j);
+#pragma unroll
+            for (int r = 0; r < 3; r++) dq[j][e][r] = div_axis(rsub(v[3 * b + r], v[3 * a + r]), dv, j);
+        }
     for (int p = 0; p < 27; p++) {
         double fs[3][3];
 #pragma unroll
@@ -375,11 +409,9 @@ __device__ bool fallback_cell(const double v[24], const double h[3], double delt
         for (int j = 0; j < 3; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-                int a = edge_start(j, e), b = a | (1 << j);
                 double w = edge_weight(j, e, p);
 #pragma unroll
-                for (int r = 0; r < 3; r++)
-                    fs[r][j] = radd(fs[r][j], rmul(rdiv(rsub(v[3 * b + r], v[3 * a + r]), h[j]), w));
+                for (int r = 0; r < 3; r++) fs[r][j] = radd(fs[r][j], rmul(dq[j][e][r], w));
             }
         bool finite = true;
 #pragma unroll
@@ -408,15 +440,14 @@ __device__ bool fallback_cell(const double v[24], const double h[3], double delt
 
 // Standalone cells: vertices (n, 8, 3)
 __global__ void __launch_bounds__(64) fallback_vertices_kernel(const double *__restrict__ vertices, long long n,
-                                                               double hx, double hy, double hz, double delta,
+                                                               const AxisDiv dv, double delta,
                                                                double *plo, double *phi, double *clo, double *chi,
                                                                double *smp, uint8_t *ok) {
-    const double h[3] = {hx, hy, hz};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         double v[24];
         for (int k = 0; k < 24; k++) v[k] = vertices[24 * i + k];
-        ok[i] = fallback_cell(v, h, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+        ok[i] = fallback_cell(v, dv, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
     }
 }
 
@@ -431,7 +462,7 @@ __global__ void __launch_bounds__(64) fallback_grid_kernel(const double *__restr
         double v[24];
         for (int a = 0; a < 8; a++)
             for (int r = 0; r < 3; r++) v[3 * a + r] = __ldg(u + 3 * vnode(base, a, g.ny, g.nx) + r);
-        ok[i] = fallback_cell(v, g.h, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+        ok[i] = fallback_cell(v, g.div, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
     }
 }
 
@@ -932,8 +963,9 @@ extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const doub
     SVP_REQUIRE(n >= 0 && spacing3, "svp_fallback_arrays: invalid arguments");
     if (n == 0) return SVP_OK;
     SVP_REQUIRE(vertices && p_lo && p_hi && c_lo && c_hi && samples && ok, "svp_fallback_arrays: null pointer");
+    const AxisDiv dv = axis_div(spacing3);
     SVP_LAUNCH(fallback_vertices_kernel<<<blocks_for(n, 64, 16), 64, 0, (cudaStream_t)stream>>>(
-        vertices, n, spacing3[0], spacing3[1], spacing3[2], delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
+        vertices, n, dv, delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
     SVP_LAUNCH_CHECK("fallback_vertices_kernel");
     return SVP_OK;
 }
