@@ -329,9 +329,16 @@ __device__ __forceinline__ double edge_weight(int j, int e, int p) {
     return w;
 }
 
-// v: 24 vertex displacements (vertex-major); outputs with stride 1 (27 entries each); returns ok
-__device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delta, double *plo, double *phi,
-                              double *clo, double *chi, double *smp) {
+// One cell per warp (v: its 24 vertex displacements, vertex-major, in every lane; outputs with stride 1, 27 entries
+// each; sb: 54 doubles of the warp's shared memory).  Lane p < 27 evaluates closed27 point p: the interval J - delta
+// from the outward-rounded edge quotients, and the float sample.  The Lagrange -> Bernstein passes (x, y, z) update
+// the middle entries of each line on their own lanes, with a warp barrier between passes.  Bitwise the sequential
+// form: each point's arithmetic is the same, and a pass reads only entries it does not write.  Returns ok for the
+// whole cell (warp-uniform).
+__device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double delta, double *plo, double *phi,
+                                   double *clo, double *chi, double *smp, double *sb) {
+    const int p = threadIdx.x & 31;
+    const bool point = p < 27;
     bool ok = true;
     double elo[3][4][3], ehi[3][4][3];
 #pragma unroll
@@ -349,8 +356,7 @@ __device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delt
                            ehi[j][e][r]);
             }
         }
-    double blo[27], bhi[27];
-    for (int p = 0; p < 27; p++) {
+    if (point) {
         double fl[3][3], fh[3][3];
 #pragma unroll
         for (int j = 0; j < 3; j++)
@@ -370,36 +376,30 @@ __device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delt
         ok &= idet(fl, fh, jl, jh);
         ok &= isub(jl, jh, delta, delta, ml, mh);
         plo[p] = ml; phi[p] = mh;
-        blo[p] = ml; bhi[p] = mh;
+        sb[p] = ml; sb[27 + p] = mh;
     }
+    __syncwarp();
     // lagrange_to_bernstein: axes x, y, z; middle <- 2 b - (a + c) * .5, all outward
 #pragma unroll
     for (int s = 0; s < 3; s++) {
-        int stride = s == 0 ? 1 : (s == 1 ? 3 : 9);
-        for (int q = 0; q < 27; q++) {
-            if ((q / stride) % 3 != 1) continue;
-            int a0 = q - stride, a2 = q + stride;
-            double ml1, mh1, sl1, sh1, hl1, hh1, nl, nh;
-            ok &= imul(blo[q], bhi[q], 2., 2., ml1, mh1);
-            ok &= iadd(blo[a0], bhi[a0], blo[a2], bhi[a2], sl1, sh1);
+        const int stride = s == 0 ? 1 : (s == 1 ? 3 : 9);
+        const bool mid = point && (p / stride) % 3 == 1;
+        double nl = 0., nh = 0.;
+        if (mid) {
+            int a0 = p - stride, a2 = p + stride;
+            double ml1, mh1, sl1, sh1, hl1, hh1;
+            ok &= imul(sb[p], sb[27 + p], 2., 2., ml1, mh1);
+            ok &= iadd(sb[a0], sb[27 + a0], sb[a2], sb[27 + a2], sl1, sh1);
             ok &= imul(sl1, sh1, .5, .5, hl1, hh1);
             ok &= isub(ml1, mh1, hl1, hh1, nl, nh);
-            blo[q] = nl; bhi[q] = nh;
         }
+        __syncwarp();
+        if (mid) { sb[p] = nl; sb[27 + p] = nh; }
+        __syncwarp();
     }
-    for (int p = 0; p < 27; p++) { clo[p] = blo[p]; chi[p] = bhi[p]; }
-    // float64 samples: F = I + sum_(j,e) ((v_b - v_a) / h) w, cofactors, ((0 + t0) + t1) + t2; the 36 edge
-    // quotients do not depend on the point and are formed once
-    double dq[3][4][3];
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            int a = edge_start(j, e), b = a | (1 << j);
-#pragma unroll
-            for (int r = 0; r < 3; r++) dq[j][e][r] = div_axis(rsub(v[3 * b + r], v[3 * a + r]), dv, j);
-        }
-    for (int p = 0; p < 27; p++) {
+    if (point) {
+        clo[p] = sb[p]; chi[p] = sb[27 + p];
+        // float64 sample: F = I + sum_(j,e) ((v_b - v_a) / h) w, cofactors, ((0 + t0) + t1) + t2
         double fs[3][3];
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -409,9 +409,11 @@ __device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delt
         for (int j = 0; j < 3; j++)
 #pragma unroll
             for (int e = 0; e < 4; e++) {
+                int a = edge_start(j, e), b = a | (1 << j);
                 double w = edge_weight(j, e, p);
 #pragma unroll
-                for (int r = 0; r < 3; r++) fs[r][j] = radd(fs[r][j], rmul(dq[j][e][r], w));
+                for (int r = 0; r < 3; r++)
+                    fs[r][j] = radd(fs[r][j], rmul(div_axis(rsub(v[3 * b + r], v[3 * a + r]), dv, j), w));
             }
         bool finite = true;
 #pragma unroll
@@ -430,39 +432,50 @@ __device__ bool fallback_cell(const double v[24], const AxisDiv &dv, double delt
         finite = finite && finite64(a00) && finite64(a01) && finite64(a02) && finite64(a10) && finite64(a11) &&
                  finite64(a12) && finite64(a20) && finite64(a21) && finite64(a22);
         double t0 = rmul(fs[0][0], a00), t1 = rmul(fs[0][1], a01), t2 = rmul(fs[0][2], a02);
-        double s = radd(radd(radd(0., t0), t1), t2);
-        finite = finite && finite64(t0) && finite64(t1) && finite64(t2) && finite64(s);
-        smp[p] = s;
+        double sv = radd(radd(radd(0., t0), t1), t2);
+        finite = finite && finite64(t0) && finite64(t1) && finite64(t2) && finite64(sv);
+        smp[p] = sv;
         ok = ok && finite;
     }
-    return ok;
+    return __all_sync(0xFFFFFFFFu, ok);
 }
 
-// Standalone cells: vertices (n, 8, 3)
-__global__ void __launch_bounds__(64) fallback_vertices_kernel(const double *__restrict__ vertices, long long n,
-                                                               const AxisDiv dv, double delta,
-                                                               double *plo, double *phi, double *clo, double *chi,
-                                                               double *smp, uint8_t *ok) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+constexpr int kFallbackWarps = 4;   // cells per 128-thread block
+
+// Standalone cells: vertices (n, 8, 3), one warp per cell
+__global__ void __launch_bounds__(32 * kFallbackWarps) fallback_vertices_kernel(
+    const double *__restrict__ vertices, long long n, const AxisDiv dv, double delta, double *plo, double *phi,
+    double *clo, double *chi, double *smp, uint8_t *ok) {
+    __shared__ double sb[kFallbackWarps][54];
+    const int w = threadIdx.x >> 5;
+    for (long long i = blockIdx.x * (long long)kFallbackWarps + w; i < n; i += (long long)gridDim.x * kFallbackWarps) {
         double v[24];
+#pragma unroll
         for (int k = 0; k < 24; k++) v[k] = vertices[24 * i + k];
-        ok[i] = fallback_cell(v, dv, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+        bool good = fallback_cell_warp(v, dv, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i,
+                                       smp + 27 * i, sb[w]);
+        if ((threadIdx.x & 31) == 0) ok[i] = good;
+        __syncwarp();
     }
 }
 
-// Grid cells from a list: vertices gathered from u
-__global__ void __launch_bounds__(64) fallback_grid_kernel(const double *__restrict__ u, CellGrid g,
-                                                           const long long *__restrict__ cells, long long n,
-                                                           double delta, double *plo, double *phi, double *clo,
-                                                           double *chi, double *smp, uint8_t *ok) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+// Grid cells from a list: vertices gathered from u, one warp per cell
+__global__ void __launch_bounds__(32 * kFallbackWarps) fallback_grid_kernel(
+    const double *__restrict__ u, CellGrid g, const long long *__restrict__ cells, long long n, double delta,
+    double *plo, double *phi, double *clo, double *chi, double *smp, uint8_t *ok) {
+    __shared__ double sb[kFallbackWarps][54];
+    const int w = threadIdx.x >> 5;
+    for (long long i = blockIdx.x * (long long)kFallbackWarps + w; i < n; i += (long long)gridDim.x * kFallbackWarps) {
         long long base = cell_base(cells[i], g);
         double v[24];
+#pragma unroll
         for (int a = 0; a < 8; a++)
+#pragma unroll
             for (int r = 0; r < 3; r++) v[3 * a + r] = __ldg(u + 3 * vnode(base, a, g.ny, g.nx) + r);
-        ok[i] = fallback_cell(v, g.div, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i, smp + 27 * i);
+        bool good = fallback_cell_warp(v, g.div, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i,
+                                       smp + 27 * i, sb[w]);
+        if ((threadIdx.x & 31) == 0) ok[i] = good;
+        __syncwarp();
     }
 }
 
@@ -964,7 +977,8 @@ extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const doub
     if (n == 0) return SVP_OK;
     SVP_REQUIRE(vertices && p_lo && p_hi && c_lo && c_hi && samples && ok, "svp_fallback_arrays: null pointer");
     const AxisDiv dv = axis_div(spacing3);
-    SVP_LAUNCH(fallback_vertices_kernel<<<blocks_for(n, 64, 16), 64, 0, (cudaStream_t)stream>>>(
+    SVP_LAUNCH(fallback_vertices_kernel<<<blocks_for(div_up(n, kFallbackWarps), 1, 16), 32 * kFallbackWarps, 0,
+                                         (cudaStream_t)stream>>>(
         vertices, n, dv, delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
     SVP_LAUNCH_CHECK("fallback_vertices_kernel");
     return SVP_OK;
@@ -1168,7 +1182,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
         if (rc) return rc;
         double *fb = c->fb, *plo = fb, *phi = fb + 27 * n2, *clo = fb + 2 * 27 * n2, *chi = fb + 3 * 27 * n2,
                *smp = fb + 4 * 27 * n2;
-        { svp::KernelTimer _t("fallback_grid_kernel", s); SVP_LAUNCH(fallback_grid_kernel<<<blocks_for(n2, 64, 16), 64, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
+        { svp::KernelTimer _t("fallback_grid_kernel", s); SVP_LAUNCH(fallback_grid_kernel<<<blocks_for(div_up(n2, kFallbackWarps), 1, 16), 32 * kFallbackWarps, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
                                                                     smp, c->fb_ok)); }
         SVP_LAUNCH_CHECK("fallback_grid_kernel");
         SVP_LAUNCH(job_fail_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, c->fb_ok, n2, tile, c->tile_fail));
