@@ -124,6 +124,12 @@ Q1Const make_const(const svp_grid *g, const svp_weights *w) {
         q.sqmu[p] = std::sqrt(q.mu * q.gw[p]);
         q.sqnu[p] = std::sqrt(q.nu * q.gw[p]);
     }
+    for (int k = 0; k < 3; k++) {
+        q.gnf[k] = (float)q.gn[k];
+        q.gmf[k] = (float)q.gm[k];
+        q.ihf[k] = (float)q.ih[k];
+    }
+    for (int p = 0; p < 27; p++) q.gwf[p] = (float)q.gw[p];
     q.bw = w->kappa * q.omega / 27;
     q.act = w->activation;
     q.delta = w->delta;

@@ -219,7 +219,7 @@ __device__ __forceinline__ void add_flux(R *sl, int T, int ix, int iy, int iz, c
 }
 // adjoint of the edge interpolation (scatter_edges) reading S from the slice
 template <class R, class C>
-__device__ __forceinline__ void scatter_slice(const R *sl, int T, const C n[3], const C m[3], const double ih[3],
+__device__ __forceinline__ void scatter_slice(const R *sl, int T, const C n[3], const C m[3], const C ih[3],
                                               R L[8][3]) {
 #pragma unroll
     for (int j = 0; j < 3; j++)
@@ -624,7 +624,7 @@ __device__ __forceinline__ void load_edges_f32(const double *__restrict__ u, lon
 #pragma unroll
             for (int r = 0; r < 3; r++) E[j][e][r] = (float)E64[j][e][r];
 }
-__global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
+__global__ void __launch_bounds__(CS) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
                                                          const double *__restrict__ uref, double mu_scale,
                                                          double nu_scale, bool barrier, bool split,
                                                          float *__restrict__ L1, float *__restrict__ L2,
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const dou
                 float Jr = det_only(Vr);
                 curl_of(V, C);
                 curl_of(Vr, Cr);
-                const float gw = (float)q.gw[p];
+                const float gw = q.gwf[p];
                 float jd = mu * gw * (J - Jr);
                 float k0 = nu * gw * (C[0] - Cr[0]), k1 = nu * gw * (C[1] - Cr[1]), k2 = nu * gw * (C[2] - Cr[2]);
                 float f[3][3];
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const dou
                 f[1][0] += k2; f[0][1] -= k2;
                 add_flux(sl, T, ix, iy, iz, f);
             });
-            scatter_slice(sl, T, q.gn, q.gm, q.ih, L);
+            scatter_slice(sl, T, q.gnf, q.gmf, q.ihf, L);
         }
         bool any = false;
         // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term
@@ -696,7 +696,7 @@ __global__ void __launch_bounds__(CS, 6) cell_grad32_kernel(Q1Const q, const dou
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) Lb[a][r] = 0.f;
-        if (any) scatter_slice(sl, T, cn, cm, q.ih, Lb);
+        if (any) scatter_slice(sl, T, cn, cm, q.ihf, Lb);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
@@ -725,17 +725,17 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
         sweep<false, float>(E, q, [&](int p, int ix, int iy, int iz, const float (&V)[3][3]) {
             float A[3][3], J;
             cofactor_det(V, A, J);
-            const float gw = (float)q.gw[p];
+            const float gw = q.gwf[p];
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 const int bx = a & 1, by = (a >> 1) & 1, bz = (a >> 2) & 1;
-                const float fx = (float)(bx ? rule_n<false>(q, ix) : rule_m<false>(q, ix));
-                const float fy = (float)(by ? rule_n<false>(q, iy) : rule_m<false>(q, iy));
-                const float fz = (float)(bz ? rule_n<false>(q, iz) : rule_m<false>(q, iz));
+                const float fx = bx ? q.gnf[ix] : q.gmf[ix];
+                const float fy = by ? q.gnf[iy] : q.gmf[iy];
+                const float fz = bz ? q.gnf[iz] : q.gmf[iz];
                 float D[3];
-                D[0] = (float)(bx ? q.ih[0] : -q.ih[0]) * fy * fz;
-                D[1] = (float)(by ? q.ih[1] : -q.ih[1]) * fx * fz;
-                D[2] = (float)(bz ? q.ih[2] : -q.ih[2]) * fx * fy;
+                D[0] = (bx ? q.ihf[0] : -q.ihf[0]) * fy * fz;
+                D[1] = (by ? q.ihf[1] : -q.ihf[1]) * fx * fz;
+                D[2] = (bz ? q.ihf[2] : -q.ihf[2]) * fx * fy;
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     float lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];

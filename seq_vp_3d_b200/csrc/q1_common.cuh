@@ -17,6 +17,7 @@ struct Q1Const {
     double lam, mu, nu, bw;        // weights; bw = kappa omega / 27 (problem.py:310)
     double act, delta;             // localized barrier activation a and delta
     double x0[3];                  // node axis origins (x, y, z)
+    float gnf[3], gmf[3], gwf[27], ihf[3];   // the same rule constants rounded to float (the mixed form's kernels)
 };
 
 // ------------------------------------------------------------------------------------------- double-double
@@ -149,6 +150,22 @@ template <bool CLOSED>
 __device__ __forceinline__ double rule_n(const Q1Const &q, int i) { return CLOSED ? .5 * i : q.gn[i]; }
 template <bool CLOSED>
 __device__ __forceinline__ double rule_m(const Q1Const &q, int i) { return CLOSED ? 1. - .5 * i : q.gm[i]; }
+// the rule's nodes and 1/h in the arithmetic type R (float: the rounded constants, no conversion in the sweeps)
+template <bool CLOSED, class R>
+__device__ __forceinline__ R node_n(const Q1Const &q, int i) {
+    if constexpr (sizeof(R) == 4) return CLOSED ? .5f * (float)i : q.gnf[i];
+    else return rule_n<CLOSED>(q, i);
+}
+template <bool CLOSED, class R>
+__device__ __forceinline__ R node_m(const Q1Const &q, int i) {
+    if constexpr (sizeof(R) == 4) return CLOSED ? 1.f - .5f * (float)i : q.gmf[i];
+    else return rule_m<CLOSED>(q, i);
+}
+template <class R>
+__device__ __forceinline__ R inv_h(const Q1Const &q, int k) {
+    if constexpr (sizeof(R) == 4) return q.ihf[k];
+    else return q.ih[k];
+}
 
 // Visit the 27 points p = 9 iz + 3 iy + ix of a rule with grad u at each, V[r][j].  Column x depends only on
 // (iy, iz) and column y only on (ix, iz), so x is evaluated once per (iy, iz) and y once per (ix, iz): 45 column
@@ -156,23 +173,23 @@ __device__ __forceinline__ double rule_m(const Q1Const &q, int i) { return CLOSE
 // (sweep2, same points); body(p, ix, iy, iz, V[, V2]).
 template <bool CLOSED, class R = double, class Body>
 __device__ __forceinline__ void sweep(const R E[3][4][3], const Q1Const &q, Body &&body) {
-    const R ih0 = (R)q.ih[0], ih1 = (R)q.ih[1], ih2 = (R)q.ih[2];
+    const R ih0 = inv_h<R>(q, 0), ih1 = inv_h<R>(q, 1), ih2 = inv_h<R>(q, 2);
 #pragma unroll 1
     for (int iz = 0; iz < 3; iz++) {
-        const R nz = (R)rule_n<CLOSED>(q, iz), mz = (R)rule_m<CLOSED>(q, iz);
+        const R nz = node_n<CLOSED, R>(q, iz), mz = node_m<CLOSED, R>(q, iz);
         R Y[3][3];
 #pragma unroll
         for (int ix = 0; ix < 3; ix++)
-            column<1>(E, (R)rule_m<CLOSED>(q, ix), (R)rule_n<CLOSED>(q, ix), mz, nz, ih1, Y[ix]);
+            column<1>(E, node_m<CLOSED, R>(q, ix), node_n<CLOSED, R>(q, ix), mz, nz, ih1, Y[ix]);
 #pragma unroll 1
         for (int iy = 0; iy < 3; iy++) {
-            const R ny = (R)rule_n<CLOSED>(q, iy), my = (R)rule_m<CLOSED>(q, iy);
+            const R ny = node_n<CLOSED, R>(q, iy), my = node_m<CLOSED, R>(q, iy);
             R X[3];
             column<0>(E, my, ny, mz, nz, ih0, X);
 #pragma unroll
             for (int ix = 0; ix < 3; ix++) {
                 R Z[3];
-                column<2>(E, (R)rule_m<CLOSED>(q, ix), (R)rule_n<CLOSED>(q, ix), my, ny, ih2, Z);
+                column<2>(E, node_m<CLOSED, R>(q, ix), node_n<CLOSED, R>(q, ix), my, ny, ih2, Z);
                 R V[3][3] = {{X[0], Y[ix][0], Z[0]}, {X[1], Y[ix][1], Z[1]}, {X[2], Y[ix][2], Z[2]}};
                 body(9 * iz + 3 * iy + ix, ix, iy, iz, V);
             }
@@ -181,19 +198,19 @@ __device__ __forceinline__ void sweep(const R E[3][4][3], const Q1Const &q, Body
 }
 template <bool CLOSED, class R = double, class Body>
 __device__ __forceinline__ void sweep2(const R E[3][4][3], const R E2[3][4][3], const Q1Const &q, Body &&body) {
-    const R ih0 = (R)q.ih[0], ih1 = (R)q.ih[1], ih2 = (R)q.ih[2];
+    const R ih0 = inv_h<R>(q, 0), ih1 = inv_h<R>(q, 1), ih2 = inv_h<R>(q, 2);
 #pragma unroll 1
     for (int iz = 0; iz < 3; iz++) {
-        const R nz = (R)rule_n<CLOSED>(q, iz), mz = (R)rule_m<CLOSED>(q, iz);
+        const R nz = node_n<CLOSED, R>(q, iz), mz = node_m<CLOSED, R>(q, iz);
 #pragma unroll 1
         for (int iy = 0; iy < 3; iy++) {
-            const R ny = (R)rule_n<CLOSED>(q, iy), my = (R)rule_m<CLOSED>(q, iy);
+            const R ny = node_n<CLOSED, R>(q, iy), my = node_m<CLOSED, R>(q, iy);
             R X[3], X2[3];
             column<0>(E, my, ny, mz, nz, ih0, X);
             column<0>(E2, my, ny, mz, nz, ih0, X2);
 #pragma unroll 1
             for (int ix = 0; ix < 3; ix++) {
-                const R nx = (R)rule_n<CLOSED>(q, ix), mx = (R)rule_m<CLOSED>(q, ix);
+                const R nx = node_n<CLOSED, R>(q, ix), mx = node_m<CLOSED, R>(q, ix);
                 R Y[3], Z[3], Y2[3], Z2[3];
                 column<1>(E, mx, nx, mz, nz, ih1, Y);
                 column<2>(E, mx, nx, my, ny, ih2, Z);
