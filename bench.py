@@ -118,8 +118,9 @@ def peaks():
 # = 35; curl = 3; sq_change = 20; compensated add = 8.  Barrier-active points add a few hundred more (not counted).
 FLOP_PER_CELL = {
     # edges 108 + reference sweep (45 columns + 27 x (det + curl)) 1890 + Gauss sweep2 (126 columns) 3780
-    # + 27 x (2 det + 2 curl + 4 stable changes + trial energy) 4833 + closed sweep2 3780 + 27 x 2 det 918
-    "cell_trial_kernel": 15309,
+    # + 27 x (2 det + 2 curl + 4 stable changes + trial energy) 4833 + the trial's closed sweep (45 columns) 1350
+    # + 27 x det 459 (the base's closed sweep runs only in cells near the activation: not counted)
+    "cell_trial_kernel": 12420,
     "cell_diff_kernel": 15006,
     # edges 72 + ref sweep 1890 + Gauss sweep (45 columns) 1350 + 27 x 31 + closed sweep 1350 + 27 x det 459
     "cell_energy_kernel": 5958,

@@ -202,6 +202,14 @@ int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *bas
 int svp_energy_difference_masked(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
                                  const double *trial_warped, const uint8_t *base_active, const uint8_t *trial_active,
                                  double *diff2, void *stream);
+/* svp_trial_energy_masked given also the base's mask (base_active: the mask its own evaluation returned, or NULL):
+ * the base's closed27 sweep then runs only in cells where some point of the base or of the trial is below the
+ * activation, the only cells whose barrier difference is not zero.  Values bitwise those of
+ * svp_trial_energy_masked. */
+int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                            double *trial_warped, double *trial_image_grad, const uint8_t *base_active,
+                            uint8_t *trial_active, double *terms5, double *diff2, int64_t *barrier_violations,
+                            void *stream);
 
 /* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
 #define SVP_TERM_IMAGE 1

@@ -912,10 +912,17 @@ __global__ void __launch_bounds__(256) warp_trial_kernel(Q1Const q, SplineRef S,
 
 // Barrier activity mask: act[c] = 1 when some closed27 J of cell c is below the activation; trial_act (optional)
 // receives the trial's mask, which later calls on that state use to skip barrier sweeps that contribute nothing.
+//
+// The closed27 part runs the trial's sweep alone first (its J values parked in the thread's slice, whose reference
+// values are dead after the Gauss sweep); the base's sweep and the barrier differences follow only where some point
+// of either state is below the activation: the trial's (just found) or the base's (base_act, its mask from its own
+// evaluation; NULL: unknown, always sweep).  Elsewhere every difference term is zero.  Same values in the same
+// order per accumulator as one two-field sweep.
 __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double *__restrict__ ua,
                                                         const double *__restrict__ ub,
                                                         const double *__restrict__ uref, dd *pe, dd *pd,
-                                                        unsigned long long *bad, uint8_t *__restrict__ trial_act) {
+                                                        unsigned long long *bad, uint8_t *__restrict__ trial_act,
+                                                        const uint8_t *__restrict__ base_act) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -949,9 +956,9 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
             sc += w * (cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
         });
         bool active = false;
-        sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
-            double ja = det_only(Va), jb = det_only(Vb);
-            if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+        sweep<true>(Eb, q, [&](int p, int, int, int, const double (&Vb)[3][3]) {
+            const double jb = det_only(Vb);
+            sl[p * T] = jb;
             active |= jb < q.act;
             if (!(jb > q.delta)) { nbad++; return; }
             if (jb < q.act) {
@@ -960,6 +967,13 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
                 sb += b;
             }
         });
+        if (active || !base_act || base_act[c]) {
+            load_edges(ua, n0, q, Ea);
+            sweep<true>(Ea, q, [&](int p, int, int, int, const double (&Va)[3][3]) {
+                const double ja = det_only(Va), jb = sl[p * T];
+                if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+            });
+        }
         if (trial_act) trial_act[c] = active ? 1 : 0;
         acc[0] = dd_add_d(acc[0], sj);
         acc[1] = dd_add_d(acc[1], sc);
@@ -1616,10 +1630,10 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
                                         stream);
 }
 
-extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *base_warped,
+extern "C" int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *base_warped,
                                        const double *trial_u, double *trial_warped, double *trial_image_grad,
-                                       uint8_t *trial_active, double *terms5, double *diff2,
-                                       int64_t *barrier_violations, void *stream) {
+                                       const uint8_t *base_active, uint8_t *trial_active, double *terms5,
+                                       double *diff2, int64_t *barrier_violations, void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && terms5 && diff2,
                 "svp_trial_energy: null argument");
     cudaStream_t s = (cudaStream_t)stream;
@@ -1640,7 +1654,7 @@ extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const 
                                                                  p->u_ref, trial_warped, nullptr, pne, pnd));
     }
     SVP_LAUNCH_CHECK("warp_trial_kernel");
-    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter, trial_active)); }
+    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter, trial_active, base_active)); }
     SVP_LAUNCH_CHECK("cell_trial_kernel");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
@@ -1668,6 +1682,14 @@ extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const 
     diff2[0] = (((img + prox) + jd) + curl) + bar;
     diff2[1] = img + bar;
     return SVP_OK;
+}
+
+extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *base_warped,
+                                       const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                       uint8_t *trial_active, double *terms5, double *diff2,
+                                       int64_t *barrier_violations, void *stream) {
+    return svp_trial_energy_active(p, base_u, base_warped, trial_u, trial_warped, trial_image_grad, nullptr,
+                                   trial_active, terms5, diff2, barrier_violations, stream);
 }
 
 extern "C" int svp_trial_energy(svp_pair *p, const double *base_u, const double *base_warped,

@@ -99,17 +99,19 @@ class DevicePair:
     def cell_mask(self):
         return torch.empty(self.grid.n_cells, dtype=torch.uint8, device=self.device)
 
-    def trial_energy(self, base_u, base_w, trial_u, with_gradient=True, stream=None):
+    def trial_energy(self, base_u, base_w, trial_u, with_gradient=True, base_active=None, stream=None):
         """Warp and evaluate a trial against its base in one pass: (warped, image_grad or None, terms[5],
-        barrier violations, (E(trial) - E(base), F(trial) - F(base)), the trial's barrier activity mask)."""
+        barrier violations, (E(trial) - E(base), F(trial) - F(base)), the trial's barrier activity mask).
+        base_active (the base's own mask) limits the base's barrier sweep to the cells where it can contribute;
+        the values are the same bits."""
         w = self.node()
         g = self.node(3) if with_gradient else None
         act = self.cell_mask()
         t = (ctypes.c_double * 5)()
         d = (ctypes.c_double * 2)()
         bad = ctypes.c_int64()
-        _lib.call("svp_trial_energy_masked", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g),
-                  ptr(act), t, d, ctypes.byref(bad), stream_ptr(stream))
+        _lib.call("svp_trial_energy_active", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g),
+                  ptr(base_active), ptr(act), t, d, ctypes.byref(bad), stream_ptr(stream))
         return w, g, np.array(t[:]), int(bad.value), (d[0], d[1]), act
 
     def gradient(self, u, warped, image_grad, term="total", out=None, active=None, stream=None):

@@ -166,7 +166,8 @@ class Registration:
             warped, _ = self.pair.warp(u)
             terms, bad = self.pair.energy(u, warped)
         else:
-            warped, grad, terms, bad, diff, active = self.pair.trial_energy(base.u, base.warped, u)
+            warped, grad, terms, bad, diff, active = self.pair.trial_energy(base.u, base.warped, u,
+                                                                            base_active=base.active)
         if bad or not np.all(np.isfinite(terms)):
             return InvalidTrial("NONFINITE_STATE", "floating barrier-point evaluation contradicts feasible certificate", 1)
         self._eval += 1

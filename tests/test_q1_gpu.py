@@ -103,6 +103,12 @@ def test_one_pass_trial_matches_separate_passes(gold):
     act1 = P.trial_energy(u2, w2, u1)[5]
     assert 0 < int(act1.sum()) < act1.numel()
     assert same_bits(np.array(P.energy_difference(u1, w1, u2, w2, act1, act2)), np.array(diff))
+    # with the base's own mask the trial evaluation sweeps the base only where it can contribute: same bits
+    hw, hg, hterms, hbad, hdiff, hact = P.trial_energy(u1, w1, u2, base_active=act1)
+    assert torch.equal(hw, w2) and torch.equal(hg, g2) and torch.equal(hact, act2)
+    assert same_bits(hterms, terms) and hbad == bad and same_bits(np.array(hdiff), np.array(diff))
+    rw, rg, rterms, rbad, rdiff, ract = P.trial_energy(u2, w2, u1, base_active=act2)
+    assert torch.equal(ract, act1) and same_bits(np.array(rdiff), np.array(P.energy_difference(u2, w2, u1, w1)))
     # the gradient, the outer triple and the GGN diagonal with u1's mask: bitwise the unmasked values
     for term in ("total", "barrier"):
         assert torch.equal(P.gradient(u1, w1, g1, term, active=act1), P.gradient(u1, w1, g1, term))
