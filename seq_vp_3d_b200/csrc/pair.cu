@@ -26,6 +26,30 @@ std::vector<double> not_a_knot(const std::vector<double> &x) {
     return t;
 }
 
+// The reciprocals cubic_basis multiplies by, per span s in [3, n-1] (row s of 14): the Cox-de Boor denominators
+// t[s+r+1] - t[s+1-d+r] for d = 1..3, r < d (6), then for each basis function k = 0..3 of the span the two derivative
+// denominators a = t[i+3] - t[i], b = t[i+4] - t[i+1] with i = s - 3 + k (1 where a difference is zero, the
+// reference's guard).  Rows below 3 are unused (zero).
+std::vector<double> spline_reciprocals(const std::vector<double> &t, long long n) {
+    std::vector<double> R((size_t)n * 14, 0.);
+    for (long long s = 3; s <= n - 1; s++) {
+        double *row = R.data() + 14 * s;
+        int k = 0;
+        for (int d = 1; d <= 3; d++)
+            for (int r = 0; r < d; r++) {
+                double len = t[(size_t)(s + r + 1)] - t[(size_t)(s + 1 - d + r)];
+                row[k++] = len != 0. ? 1. / len : 0.;
+            }
+        for (int b = 0; b < 4; b++) {
+            long long i = s - 3 + b;
+            double a = t[(size_t)(i + 3)] - t[(size_t)i], bb = t[(size_t)(i + 4)] - t[(size_t)(i + 1)];
+            row[6 + 2 * b] = 1. / (a != 0. ? a : 1.);
+            row[7 + 2 * b] = 1. / (bb != 0. ? bb : 1.);
+        }
+    }
+    return R;
+}
+
 // Cox-de Boor values of the 4 cubic B-splines on span s at x (backends/spline.py:12 cubic_basis)
 void basis4(const std::vector<double> &t, int s, double x, double B[4]) {
     double b[4] = {1., 0., 0., 0.};
@@ -144,7 +168,9 @@ using namespace svp;
 extern "C" int svp_pair_destroy(svp_pair *p) {
     if (!p) return SVP_OK;
     cudaFree(p->fixed); cudaFree(p->coeff); cudaFree(p->u_ref);
-    for (int k = 0; k < 3; k++) { cudaFree(p->knots[k]); cudaFree(p->dst_half[k]); cudaFree(p->dst_half32[k]); }
+    for (int k = 0; k < 3; k++) {
+        cudaFree(p->knots[k]); cudaFree(p->spline_rcp[k]); cudaFree(p->dst_half[k]); cudaFree(p->dst_half32[k]);
+    }
     cudaFree(p->loc1); cudaFree(p->loc2); cudaFree(p->cellbuf); cudaFree(p->partial); cudaFree(p->result);
     cudaFree(p->counter); cudaFree(p->cand); cudaFree(p->dst_tmp); cudaFree(p->den);
     delete p;
@@ -196,6 +222,12 @@ extern "C" int svp_pair_create(const svp_grid *g, const svp_weights *w, const do
             return bail(cuda_fail(e, "knots"));
         if ((e = cudaMemcpy(p->knots[k], t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(cuda_fail(e, "knots copy"));
+        std::vector<double> rcp = spline_reciprocals(t, len[k]);
+        if ((e = cudaMalloc((void **)&p->spline_rcp[k], sizeof(double) * rcp.size())) != cudaSuccess)
+            return bail(cuda_fail(e, "spline reciprocals"));
+        if ((e = cudaMemcpy(p->spline_rcp[k], rcp.data(), sizeof(double) * rcp.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return bail(cuda_fail(e, "spline reciprocals copy"));
         inv[k] = cached_inverse_collocation(x);
     }
     // the prefilter's matrices and intermediate live in the stream-ordered scratch pool: freeing them does not

@@ -11,6 +11,7 @@ struct svp_pair {
     double *fixed = nullptr;      // (nz, ny, nx)
     double *coeff = nullptr;      // (nz, ny, nx) not-a-knot cubic coefficients
     double *knots[3] = {nullptr, nullptr, nullptr};  // x, y, z knot vectors (n + 4)
+    double *spline_rcp[3] = {nullptr, nullptr, nullptr};  // per span, 14 reciprocal knot differences (n x 14)
     double *u_ref = nullptr;      // (nz, ny, nx, 3) frozen reference displacement
     // workspace
     double *loc1 = nullptr, *loc2 = nullptr;  // (24, ncell) per-cell vertex values (SoA)

@@ -22,13 +22,16 @@ constexpr int CELL_PER_SM = 8;
 // ============================================================================================== spline sampler
 struct SplineRef {
     const double *c;
-    const double *t[3];  // x, y, z knots
-    long long n[3];      // nx, ny, nz coefficients per axis
-    double x0[3], h[3];
+    const double *t[3];    // x, y, z knots
+    const double *rcp[3];  // per span, the reciprocals of the knot differences cubic_basis divides by (14 per span)
+    long long n[3];        // nx, ny, nz coefficients per axis
+    double x0[3], ih[3];
 };
 
-__device__ __forceinline__ int find_span(const double *__restrict__ t, long long n, double x, double x0, double h) {
-    long long i = (long long)floor((x - x0) / h);
+// The span s with t[s] <= x < t[s+1] (clamped to [3, n-1]): a first guess from the uniform node spacing, then the
+// knot comparisons decide (so the guess's rounding never matters).
+__device__ __forceinline__ int find_span(const double *__restrict__ t, long long n, double x, double x0, double ih) {
+    long long i = (long long)floor((x - x0) * ih);
     long long s = i + 2;
     s = s < 3 ? 3 : (s > n - 1 ? n - 1 : s);
     while (s < n - 1 && __ldg(t + s + 1) <= x) s++;
@@ -36,8 +39,13 @@ __device__ __forceinline__ int find_span(const double *__restrict__ t, long long
     return (int)s;
 }
 
-// backends/spline.py:12 cubic_basis: Cox-de Boor values and derivatives of the 4 B-splines on the span
-__device__ __forceinline__ void cubic_basis(const double *__restrict__ t, int s, double x, double B[4], double dB[4]) {
+// backends/spline.py:12 cubic_basis: Cox-de Boor values and derivatives of the 4 B-splines on the span.  The
+// denominators are knot differences (right + left = t[s+r+1] - t[s+1-d+r] up to rounding), so their reciprocals are
+// tabled per span and the 14 divisions per axis become multiplies (a relative change of one rounding, inside the
+// float64 contract's 1e-12).
+__device__ __forceinline__ void cubic_basis(const double *__restrict__ t, const double *__restrict__ rcp, int s,
+                                            double x, double B[4], double dB[4]) {
+    const double *R = rcp + 14 * (long long)s;
     double b[4] = {1., 0., 0., 0.}, q[3];
 #pragma unroll
     for (int degree = 1; degree <= 3; degree++) {
@@ -47,7 +55,7 @@ __device__ __forceinline__ void cubic_basis(const double *__restrict__ t, int s,
         for (int r = 0; r < degree; r++) {
             double right = __ldg(t + s + r + 1) - x;
             double left = x - __ldg(t + s + 1 - degree + r);
-            double temp = b[r] / (right + left);
+            double temp = b[r] * __ldg(R + (degree - 1) * degree / 2 + r);
             nb[r] = saved + right * temp;
             saved = left * temp;
         }
@@ -58,10 +66,8 @@ __device__ __forceinline__ void cubic_basis(const double *__restrict__ t, int s,
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        int idx = s - 3 + k;
-        double a = __ldg(t + idx + 3) - __ldg(t + idx), bb = __ldg(t + idx + 4) - __ldg(t + idx + 1);
         double left = k == 0 ? 0. : q[k - 1], right = k == 3 ? 0. : q[k];
-        dB[k] = 3. * left / (a != 0. ? a : 1.) - 3. * right / (bb != 0. ? bb : 1.);
+        dB[k] = 3. * left * __ldg(R + 6 + 2 * k) - 3. * right * __ldg(R + 7 + 2 * k);
         B[k] = b[k];
     }
 }
@@ -69,13 +75,13 @@ __device__ __forceinline__ void cubic_basis(const double *__restrict__ t, int s,
 // value and (optionally) xyz gradient at physical point (x, y, z)
 template <bool GRAD>
 __device__ __forceinline__ double spline_eval(const SplineRef &S, double px, double py, double pz, double g[3]) {
-    int sx = find_span(S.t[0], S.n[0], px, S.x0[0], S.h[0]);
-    int sy = find_span(S.t[1], S.n[1], py, S.x0[1], S.h[1]);
-    int sz = find_span(S.t[2], S.n[2], pz, S.x0[2], S.h[2]);
+    int sx = find_span(S.t[0], S.n[0], px, S.x0[0], S.ih[0]);
+    int sy = find_span(S.t[1], S.n[1], py, S.x0[1], S.ih[1]);
+    int sz = find_span(S.t[2], S.n[2], pz, S.x0[2], S.ih[2]);
     double bx[4], dx[4], by[4], dy[4], bz[4], dz[4];
-    cubic_basis(S.t[0], sx, px, bx, dx);
-    cubic_basis(S.t[1], sy, py, by, dy);
-    cubic_basis(S.t[2], sz, pz, bz, dz);
+    cubic_basis(S.t[0], S.rcp[0], sx, px, bx, dx);
+    cubic_basis(S.t[1], S.rcp[1], sy, py, by, dy);
+    cubic_basis(S.t[2], S.rcp[2], sz, pz, bz, dz);
     const long long nx = S.n[0], ny = S.n[1];
     const double *c = S.c + ((long long)(sz - 3) * ny + (sy - 3)) * nx + (sx - 3);
     double val = 0., gx = 0., gy = 0., gz = 0.;
@@ -1471,8 +1477,9 @@ SplineRef spline_ref(const svp_pair *p) {
     S.c = p->coeff;
     for (int k = 0; k < 3; k++) {
         S.t[k] = p->knots[k];
+        S.rcp[k] = p->spline_rcp[k];
         S.x0[k] = p->q.x0[k];
-        S.h[k] = p->q.h[k];
+        S.ih[k] = 1. / p->q.h[k];
     }
     S.n[0] = p->q.nx; S.n[1] = p->q.ny; S.n[2] = p->q.nz;
     return S;
