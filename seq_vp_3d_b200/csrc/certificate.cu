@@ -61,7 +61,8 @@ CellGrid cell_grid(const svp_grid *g) {
 }
 
 __device__ __forceinline__ long long cell_base(long long c, const CellGrid &g) {
-    long long x0 = c % g.cx, y0 = (c / g.cx) % g.cy, z0 = c / (g.cx * g.cy);
+    long long x0, y0, z0;
+    unflatten3(c, g.cx, g.cy, x0, y0, z0);
     return (z0 * g.ny + y0) * g.nx + x0;
 }
 __device__ __forceinline__ long long vnode(long long base, int a, long long ny, long long nx) {

@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(256) warp_kernel(Q1Const q, SplineRef S, const
     dd acc[2] = {{0., 0.}, {0., 0.}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        long long x, y, z;
+        unflatten3(i, q.nx, q.ny, x, y, z);
         double ux = u[3 * i], uy = u[3 * i + 1], uz = u[3 * i + 2];
         double px = (q.x0[0] + q.h[0] * (double)x) + ux;
         double py = (q.x0[1] + q.h[1] * (double)y) + uy;
@@ -158,7 +159,8 @@ __global__ void __launch_bounds__(256) node_energy_kernel(Q1Const q, const doubl
     dd acc[2] = {{0., 0.}, {0., 0.}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        long long x, y, z;
+        unflatten3(i, q.nx, q.ny, x, y, z);
         double qw = node_weight(x, y, z, q);
         double d = warped[i] - fixed[i];
         double e0 = u[3 * i] - uref[3 * i], e1 = u[3 * i + 1] - uref[3 * i + 1], e2 = u[3 * i + 2] - uref[3 * i + 2];
@@ -421,7 +423,9 @@ __global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, co
                                                      const double *__restrict__ image_grad) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long x, y, z;
+        unflatten3(i, q.fx, q.fy, x, y, z);
+        x++; y++; z++;
         long long node = (z * q.ny + y) * q.nx + x;
         double qw = node_weight(x, y, z, q);
         double dimg = warped ? qw * (warped[node] - fixed[node]) : 0.;
@@ -586,7 +590,9 @@ __global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const LT *__re
                                                        const double *__restrict__ vv, double *__restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long x, y, z;
+        unflatten3(i, q.fx, q.fy, x, y, z);
+        x++; y++; z++;
         long long node = (z * q.ny + y) * q.nx + x;
         double qw = node_weight(x, y, z, q);
         double s[3] = {0., 0., 0.};
@@ -807,7 +813,8 @@ __global__ void __launch_bounds__(256) node_diff_kernel(Q1Const q, const double 
     dd acc[2] = {{0., 0.}, {0., 0.}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        long long x, y, z;
+        unflatten3(i, q.nx, q.ny, x, y, z);
         double qw = node_weight(x, y, z, q);
         double sq = sqrt(qw), sl = sqrt(q.lam * qw);
         acc[0] = dd_add(acc[0], sq_change(sq * (wa[i] - fixed[i]), sq * (wb[i] - fixed[i])));
@@ -885,7 +892,8 @@ __global__ void __launch_bounds__(256) warp_trial_kernel(Q1Const q, SplineRef S,
     dd acc[2] = {{0., 0.}, {0., 0.}}, dif[2] = {{0., 0.}, {0., 0.}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        long long x, y, z;
+        unflatten3(i, q.nx, q.ny, x, y, z);
         double ux = ub[3 * i], uy = ub[3 * i + 1], uz = ub[3 * i + 2];
         double px = (q.x0[0] + q.h[0] * (double)x) + ux;
         double py = (q.x0[1] + q.h[1] * (double)y) + uy;
@@ -1321,7 +1329,8 @@ __global__ void __launch_bounds__(256) node_min_kernel(Q1Const q, const double *
                                                        double *__restrict__ node) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nnode;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.nx, y = (i / q.nx) % q.ny, z = i / (q.nx * q.ny);
+        long long x, y, z;
+        unflatten3(i, q.nx, q.ny, x, y, z);
         double mn = __longlong_as_double(0x7FF0000000000000LL);
 #pragma unroll
         for (int a = 0; a < 8; a++) {
@@ -1423,7 +1432,9 @@ __global__ void __launch_bounds__(256) shift_kernel(Q1Const q, const double *__r
     dd acc[1] = {{0., 0.}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long x, y, z;
+        unflatten3(i, q.fx, q.fy, x, y, z);
+        x++; y++; z++;
         const double *b = image_grad + 3 * ((z * q.ny + y) * q.nx + x);
         double qo = node_weight(x, y, z, q) / q.omega;
         acc[0] = dd_add_d(acc[0], qo * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2]));
@@ -1438,7 +1449,9 @@ __global__ void __launch_bounds__(256) pg_scale_kernel(Q1Const q, const double *
     unsigned long long nb = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < q.nfree;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % q.fx + 1, y = (i / q.fx) % q.fy + 1, z = i / (q.fx * q.fy) + 1;
+        long long x, y, z;
+        unflatten3(i, q.fx, q.fy, x, y, z);
+        x++; y++; z++;
         double ja = node[(z * q.ny + y) * q.nx + x];
         double r = fmin(1., fmax(ja, floor_) / act);
         if (!(ja == ja) || !(ja < INFINITY) || !(ja > -INFINITY)) nb++;

@@ -79,7 +79,8 @@ __device__ void block_reduce_dd(dd (&acc)[K], dd *partial) {
 
 // ------------------------------------------------------------------------------------------- cell geometry
 __device__ __forceinline__ long long cell_node0(long long c, const Q1Const &q) {
-    long long x0 = c % q.cx, y0 = (c / q.cx) % q.cy, z0 = c / (q.cx * q.cy);
+    long long x0, y0, z0;
+    unflatten3(c, q.cx, q.cy, x0, y0, z0);
     return (z0 * q.ny + y0) * q.nx + x0;
 }
 __device__ __forceinline__ long long vertex_node(long long n0, int a, const Q1Const &q) {

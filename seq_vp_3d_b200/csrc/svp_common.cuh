@@ -60,6 +60,24 @@ namespace svp {
 
 constexpr int kSMs = 148;  // B200: grid sizes are multiples of the SM count
 
+// Flat index -> (x, y, z) over rows of nx entries and planes of ny rows.  In 32-bit unsigned arithmetic when the
+// index and the plane size fit (a 64-bit integer division is a long instruction sequence on the GPU; every grid below
+// 2^32 entries takes this path), in 64 bits otherwise.
+__device__ __forceinline__ void unflatten3(long long i, long long nx, long long ny, long long &x, long long &y,
+                                           long long &z) {
+    if ((unsigned long long)i <= 0xFFFFFFFFull && (unsigned long long)(nx * ny) <= 0xFFFFFFFFull) {
+        const unsigned u = (unsigned)i, a = (unsigned)nx, b = (unsigned)ny;
+        const unsigned r = u / a;
+        x = (long long)(u - r * a);
+        y = (long long)(r % b);
+        z = (long long)(r / b);
+    } else {
+        x = i % nx;
+        y = (i / nx) % ny;
+        z = i / (nx * ny);
+    }
+}
+
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Grid launch helper: enough blocks to cover n items, capped at a multiple of the SM count (grid-stride kernels).

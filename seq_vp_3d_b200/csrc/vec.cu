@@ -43,7 +43,8 @@ __global__ void inject_kernel(long long nx, long long ny, long long nz, const do
     const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz, nn = nx * ny * nz;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        long long x, y, z;
+        unflatten3(i, nx, ny, x, y, z);
         bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
         long long f = ((z - 1) * fy + (y - 1)) * fx + (x - 1);
 #pragma unroll
@@ -56,7 +57,9 @@ __global__ void restrict_kernel(long long nx, long long ny, long long nz, const 
     const long long fx = nx - 2, fy = ny - 2, fz = nz - 2, nf = fx * fy * fz;
     for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
          f += (long long)gridDim.x * blockDim.x) {
-        long long x = f % fx + 1, y = (f / fx) % fy + 1, z = f / (fx * fy) + 1;
+        long long x, y, z;
+        unflatten3(f, fx, fy, x, y, z);
+        x++; y++; z++;
         long long i = (z * ny + y) * nx + x;
 #pragma unroll
         for (int r = 0; r < 3; r++) theta[r * nf + f] = u[3 * i + r];
@@ -74,7 +77,9 @@ __global__ void step_bound_kernel(long long nx, long long ny, long long nz, doub
     long long key = kKeyPosInf;
     for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
          f += (long long)gridDim.x * blockDim.x) {
-        long long x = f % fx + 1, y = (f / fx) % fy + 1, z = f / (fx * fy) + 1;
+        long long x, y, z;
+        unflatten3(f, fx, fy, x, y, z);
+        x++; y++; z++;
         long long idx[3] = {x, y, z};
         long long i = (z * ny + y) * nx + x;
 #pragma unroll
@@ -162,7 +167,8 @@ __global__ void trial_point_kernel(long long nx, long long ny, long long nz, con
     long long k0 = 0, k1 = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
          i += (long long)gridDim.x * blockDim.x) {
-        long long x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        long long x, y, z;
+        unflatten3(i, nx, ny, x, y, z);
         bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
         long long f = ((z - 1) * fy + (y - 1)) * fx + (x - 1);
 #pragma unroll
