@@ -127,8 +127,9 @@ FLOP_PER_CELL = {
     # edges 72 + soft sweep2 3780 + 27 x 94 (cofactor, det, curls, fluxes) + adjoint scatter 693
     # + barrier sweep 1350 + 27 x det 459
     "cell_grad_kernel": 8892,
-    # edges 36 + Gauss sweep 1350 + 27 x (cofactor 35 + 8 vertices x 48) + closed sweep 1350 + 27 x det 459
-    "cell_ggn_diag_kernel": 14508,
+    # edges 36 + Gauss sweep 1350 + 27 x (cofactor 35 + 8 vertices x 30) + closed sweep 1350 + 27 x det 459
+    # + the state-independent curl term 24
+    "cell_ggn_diag_kernel": 10644,
     "cell_min_jd_kernel": 2009,
 }
 FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12     # nominal: 148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz

@@ -154,6 +154,27 @@ Q1Const make_const(const svp_grid *g, const svp_weights *w) {
         q.ihf[k] = (float)q.ih[k];
     }
     for (int p = 0; p < 27; p++) q.gwf[p] = (float)q.gw[p];
+    for (int a = 0; a < 8; a++) {
+        const int b[3] = {a & 1, (a >> 1) & 1, (a >> 2) & 1};
+        for (int r = 0; r < 3; r++) {
+            double sum = 0.;
+            for (int p = 0; p < 27; p++) {
+                const int idx[3] = {p % 3, (p / 3) % 3, p / 9};
+                double f[3], D[3];
+                for (int k = 0; k < 3; k++) f[k] = b[k] ? q.gn[idx[k]] : q.gm[idx[k]];
+                for (int k = 0; k < 3; k++) {
+                    const int k1 = k == 0 ? 1 : 0, k2 = k == 2 ? 1 : 2;
+                    D[k] = (b[k] ? q.ih[k] : -q.ih[k]) * f[k1] * f[k2];
+                }
+                double cs = 0.;
+                for (int j = 0; j < 3; j++)
+                    if (j != r) cs += D[j] * D[j];
+                sum += q.gw[p] * (w->nu * cs);
+            }
+            q.ggn_curl[3 * a + r] = sum;
+            q.ggn_curlf[3 * a + r] = (float)sum;
+        }
+    }
     q.bw = w->kappa * q.omega / 27;
     q.act = w->activation;
     q.delta = w->delta;

@@ -475,10 +475,11 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] = 0.;
+        // JD part per Gauss point; the curl part is the state-independent q.ggn_curl
         sweep<false>(E, q, [&](int p, int ix, int iy, int iz, const double (&V)[3][3]) {
             double A[3][3], J;
             cofactor_det(V, A, J);
-            const double gw = q.gw[p];
+            const double gmu = q.gw[p] * q.mu;
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 double D[3];
@@ -486,14 +487,14 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
-                    double cs = 0.;
-#pragma unroll
-                    for (int j = 0; j < 3; j++)
-                        if (j != r) cs += D[j] * D[j];
-                    out[a][r] += gw * (q.mu * lj * lj + q.nu * cs);
+                    out[a][r] += gmu * (lj * lj);
                 }
             }
         });
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] += q.ggn_curl[3 * a + r];
         if (!active || active[c])
         sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
             if (!(det_only(V) < q.act)) return;
@@ -724,7 +725,7 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
                                                              float *__restrict__ L,
                                                            const uint8_t *__restrict__ active) {
     const float guard = (float)q.act + kBarrierGuard;
-    const float mu = (float)q.mu, nu = (float)q.nu;
+    const float mu = (float)q.mu;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         const long long n0 = cell_node0(c, q);
@@ -737,7 +738,7 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
         sweep<false, float>(E, q, [&](int p, int ix, int iy, int iz, const float (&V)[3][3]) {
             float A[3][3], J;
             cofactor_det(V, A, J);
-            const float gw = q.gwf[p];
+            const float gmu = q.gwf[p] * mu;
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 const int bx = a & 1, by = (a >> 1) & 1, bz = (a >> 2) & 1;
@@ -751,14 +752,14 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     float lj = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
-                    float cs = 0.f;
-#pragma unroll
-                    for (int j = 0; j < 3; j++)
-                        if (j != r) cs += D[j] * D[j];
-                    out[a][r] += gw * (mu * lj * lj + nu * cs);
+                    out[a][r] += gmu * (lj * lj);
                 }
             }
         });
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] += q.ggn_curlf[3 * a + r];
         if (!active || active[c])
         sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
             if (!(det_only(V) < guard)) return;

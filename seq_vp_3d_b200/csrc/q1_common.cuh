@@ -18,6 +18,10 @@ struct Q1Const {
     double act, delta;             // localized barrier activation a and delta
     double x0[3];                  // node axis origins (x, y, z)
     float gnf[3], gmf[3], gwf[27], ihf[3];   // the same rule constants rounded to float (the mixed form's kernels)
+    // the curl term of the GGN diagonal does not depend on the state: per vertex a and component r,
+    // nu sum_p gw[p] sum_(j != r) D_j(p, a)^2 over the Gauss points (index 3 a + r), float copy for the mixed form
+    double ggn_curl[24];
+    float ggn_curlf[24];
 };
 
 // ------------------------------------------------------------------------------------------- double-double
