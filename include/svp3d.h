@@ -295,6 +295,12 @@ int svp_bb2_dots_dev(const double *theta, const double *theta_old, const double 
                      const double *p_old, const double *pvec, int64_t n, double *out4_dev, void *stream);
 int svp_max_abs_diff_dev(const double *a, const double *b, int64_t n, double *out2_dev, void *stream);
 int svp_step_bound_dev(const svp_grid *g, const double *u, const double *pvec, double *bound_dev, void *stream);
+/* The scalars of one PG step in one pass over the free vectors: out_dev[0] = g.g, out_dev[1] = g.pvec and, when the
+ * previous step is given (theta, theta_old, g_old, p_old all non-NULL), out_dev[2..5] = the BB2 products of
+ * svp_bb2_dots_dev (poisson_gradient.py:785 _step_proposal_fast).  Each value is bitwise the one svp_dot_dev /
+ * svp_bb2_dots_dev returns. */
+int svp_step_dots_dev(const double *g, const double *pvec, const double *theta, const double *theta_old,
+                      const double *g_old, const double *p_old, int64_t n, double *out_dev, void *stream);
 /* One line-search trial point in one pass: candidate = fl(theta + fl(tau pvec)) exactly as svp_axpy, u = inject
  * (candidate) exactly as svp_inject, and out2_dev (device) = (max |candidate - theta|, max |theta|) exactly as
  * svp_max_abs_diff_dev(candidate, theta) (poisson_gradient.py:1245 trial theta; fast_checks.py:120 step ratio). */

@@ -89,6 +89,7 @@ SIGNATURES = {
     "svp_max_abs_diff_dev": [P, P, I64, P, P],
     "svp_step_bound_dev": [P, P, P, P, P],
     "svp_trial_point": [P, P, D, P, P, P, P, P],
+    "svp_step_dots_dev": [P, P, P, P, P, P, I64, P, P],
     "svp_pre_energy_grad": [P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, D, D, D, P, D, D, D, D, P, P, P],
     "svp_pre_level": [P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, D, D, D, P, ctypes.c_int32, ctypes.c_int32,
                       P, P, P, P, P, P, P],

@@ -118,6 +118,32 @@ __global__ void __launch_bounds__(256) bb2_kernel(const double *__restrict__ th,
     block_reduce_dd<4>(acc, partial);
 }
 
+// The scalars of one PG step in one pass: g.g, g.p and, with the previous step, the four BB2 products of bb2_kernel.
+// Same grid, per-thread order and reductions as dot_kernel and bb2_kernel, so each value is bitwise theirs.
+template <int K>
+__global__ void __launch_bounds__(256) step_dots_kernel(const double *__restrict__ g, const double *__restrict__ p,
+                                                        const double *__restrict__ th, const double *__restrict__ th0,
+                                                        const double *__restrict__ g0, const double *__restrict__ p0,
+                                                        long long n, dd *partial) {
+    dd acc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = {0., 0.};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double gi = g[i], pi = p[i];
+        acc[0] = dd_add(acc[0], two_prod(gi, gi));
+        acc[1] = dd_add(acc[1], two_prod(gi, pi));
+        if constexpr (K == 6) {
+            double s = th[i] - th0[i], y = gi - g0[i], iy = p0[i] - pi;
+            acc[2] = dd_add(acc[2], two_prod(s, y));
+            acc[3] = dd_add(acc[3], two_prod(s, s));
+            acc[4] = dd_add(acc[4], two_prod(y, y));
+            acc[5] = dd_add(acc[5], two_prod(y, iy));
+        }
+    }
+    block_reduce_dd<K>(acc, partial);
+}
+
 __global__ void multi_final_kernel(const dd *__restrict__ partial, long long blocks, int K, double *out) {
     __shared__ dd sh[256];
     for (int k = 0; k < K; k++) {
@@ -239,6 +265,28 @@ extern "C" int svp_bb2_dots_dev(const double *theta, const double *theta_old, co
     cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "bb2 kernels");
     if (fe != cudaSuccess) return cuda_fail(fe, "bb2 free");
+    return SVP_OK;
+}
+
+extern "C" int svp_step_dots_dev(const double *g, const double *pvec, const double *theta, const double *theta_old,
+                                 const double *g_old, const double *p_old, int64_t n, double *out_dev, void *stream) {
+    SVP_REQUIRE(g && pvec && out_dev && n >= 0, "svp_step_dots_dev: invalid argument");
+    const bool bb2 = theta && theta_old && g_old && p_old;
+    SVP_REQUIRE(bb2 || !(theta || theta_old || g_old || p_old), "svp_step_dots_dev: previous step given in part");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = blocks_for(n, 256, 4);
+    const int K = bb2 ? 6 : 2;
+    dd *part = nullptr;
+    SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * K * nb, s));
+    if (bb2)
+        SVP_LAUNCH(step_dots_kernel<6><<<nb, 256, 0, s>>>(g, pvec, theta, theta_old, g_old, p_old, n, part));
+    else
+        SVP_LAUNCH(step_dots_kernel<2><<<nb, 256, 0, s>>>(g, pvec, nullptr, nullptr, nullptr, nullptr, n, part));
+    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, K, out_dev));
+    cudaError_t le = cudaGetLastError();
+    cudaError_t fe = scratch_free(part, s);
+    if (le != cudaSuccess) return cuda_fail(le, "step dots kernels");
+    if (fe != cudaSuccess) return cuda_fail(fe, "step dots free");
     return SVP_OK;
 }
 

@@ -223,6 +223,13 @@ class Scalars:
         _lib.call("svp_bb2_dots_dev", ptr(theta), ptr(theta_old), ptr(g), ptr(g_old), ptr(p_old), ptr(p),
                   theta.numel(), self.slot(k), stream_ptr(stream))
 
+    def step_dots(self, k, g, p, previous=None, stream=None):
+        """Slots k, k+1 = g.g, g.p and, with previous = (theta, theta_old, g_old, p_old), k+2..k+5 = the BB2
+        products, in one pass (the values of dot() and bb2())."""
+        th, th0, g0, p0 = (None,) * 4 if previous is None else previous
+        _lib.call("svp_step_dots_dev", ptr(g), ptr(p), ptr(th), ptr(th0), ptr(g0), ptr(p0), g.numel(), self.slot(k),
+                  stream_ptr(stream))
+
     def max_abs_diff(self, k, a, b, stream=None):
         _lib.call("svp_max_abs_diff_dev", ptr(a), ptr(b), a.numel(), self.slot(k), stream_ptr(stream))
 

@@ -454,7 +454,6 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         g = pending if pending is not None else reg.pair.gradient(base.u, base.warped, base.image_grad,
                                                                   active=base.active)
         pending = None
-        S.dot(0, g, g)
         metric_error = None
         if metric is None:
             try:
@@ -464,10 +463,11 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
         if metric_error is None:
             a, b, scale = metric
             p = reg.pair.poisson_apply(a, b, g, scale=scale, sign=-1.)
-            S.dot(1, g, p)
-            if previous is not None:
-                S.bb2(2, base.theta, previous[0], g, previous[1], previous[2], p)
+            # |g|^2, the slope g.p and the BB2 products in one pass
+            S.step_dots(0, g, p, None if previous is None else (base.theta, previous[0], previous[1], previous[2]))
             S.step_bound(6, reg.pair, base.u, p)
+        else:
+            S.dot(0, g, g)
         v = S.fetch()
         G = reg.norm_of(v[0])
         if G <= target:

@@ -243,6 +243,16 @@ def test_vector_kernels_bitwise(big):
         assert torch.equal(uc, P.inject(cand))
         assert same_bits(v[:2], v[2:4]) and v[0] == np.max(np.abs((theta + tau * p) - theta))
     assert abs(pm.dot(dev(theta), dev(p)) - float(np.dot(theta, p))) <= 1e-13 * np.abs(theta * p).sum()
+    # the fused step scalars: bitwise the separate dot and BB2 reductions, with and without the previous step
+    g, pp, th0, g0, p0 = (dev(rng.normal(size=theta.shape)) for _ in range(5))
+    T = pm.Scalars(16)
+    T.step_dots(0, g, pp)
+    T.step_dots(2, g, pp, (dev(theta), th0, g0, p0))
+    T.dot(8, g, g)
+    T.dot(9, g, pp)
+    T.bb2(10, dev(theta), th0, g, g0, p0, pp)
+    v = T.fetch()
+    assert same_bits(v[0:2], v[8:10]) and same_bits(v[2:4], v[8:10]) and same_bits(v[4:8], v[10:14])
     # step bound: exact min of the reference quotients
     v = p.reshape((3,) + OP.grid.interior_shape)
     pts = (OP.grid.identity() + u)[1:-1, 1:-1, 1:-1]
