@@ -1,0 +1,42 @@
+"""Host-side pieces that need no GPU: the per-grid weight total, the boundary taper's host form, and the bench's
+phase split."""
+import numpy as np
+
+from seq_vp_3d_b200.grid import make_grid_3d
+from seq_vp_3d_b200.preopt import boundary_taper
+
+
+def test_node_weight_total_cached_and_exact():
+    grid = make_grid_3d(nx=23, ny=19, nz=17, hx=1.0, hy=1.1, hz=0.9, unit="mm")
+    direct = float(np.sum(grid.node_weights(), dtype=np.longdouble))
+    assert grid.node_weight_total() == direct
+    assert grid.node_weight_total() == direct          # second call: the cached value
+    # the total of the trapezoid weights is the box volume
+    extent = np.prod([a[-1] - a[0] for a in grid.axes])
+    assert abs(direct - extent) <= 1e-12 * extent
+
+
+def test_boundary_taper_host_form():
+    """preopt.py:617: weights min(min(k, n-1-k) / L, 1) per axis, multiplied; faces go to zero, the interior beyond L
+    keeps the field."""
+    grid = make_grid_3d(nx=14, ny=12, nz=11, hx=1., hy=1., hz=1., unit="mm")
+    rng = np.random.default_rng(3)
+    u = rng.normal(size=grid.shape + (3,))
+    out, w = boundary_taper(u, grid, L=4)
+    assert w.shape == grid.shape and np.all(w[[0, -1]] == 0) and np.all(w[:, [0, -1]] == 0)
+    assert np.all(w[:, :, [0, -1]] == 0) and w[5, 5, 6] == 1.
+    k = np.arange(grid.shape[2])
+    assert np.array_equal(w[5, 5], np.minimum(np.minimum(k, grid.shape[2] - 1 - k) / 4., 1.))
+    assert np.array_equal(out, w[..., None] * u)
+
+
+def test_bench_phase_split():
+    import bench
+    phases = [dict(preopt_s=.2, transfer_s=.01, certified_loop_s=10.), dict(preopt_s=.4, transfer_s=.03,
+                                                                              certified_loop_s=12.)]
+    timers = {"cell_trial_kernel": (10, 4000.), "prescreen_kernel": (5, 1000.), "pre_data_kernel": (3, 500.)}
+    out = bench.phase_summary(phases, timers, steps=1)
+    assert abs(out["preopt_s"] - .3) < 1e-12 and abs(out["certified_loop_s"] - 11.) < 1e-12
+    assert abs(out["fp64_kernels_s"] - 5.) < 1e-12          # the pre-optimizer's kernels are not the loop's
+    assert abs(out["loop_host_gap_s"] - 6.) < 1e-12
+    assert bench.phase_summary([], timers, 1) is None
