@@ -59,13 +59,24 @@ int svp_timer_read(const char *name, int64_t *count, double *total_ms);
  * Arithmetic: binary64 round-to-nearest with one outward ulp step (bit steps) after every interval operation, no
  * FMA contraction, IEEE division -- the reference's exact operation sequence, so margins, verdicts and records are
  * bit-identical to jd_curl's CPU certifier. */
+/* Execution flags of svp_cert_config.execution, one per member of the reference's config family
+ * (feasibility.py:22-121):
+ *   0                                          EnclosureCertificateConfig and its compiled/parallel/prescreen
+ *                                              subclasses: edge-hull preproof, lowest-bound-first subdivision
+ *   SVP_CERT_NO_HULL                           AdaptiveCertificateConfig: every cell to the interval fallback,
+ *                                              lowest-bound-first subdivision
+ *   SVP_CERT_NO_HULL | SVP_CERT_DEPTH_FIRST    CertificateConfig (the bare class): every cell to the fallback,
+ *                                              depth-first subdivision (feasibility.py:353, left child first) */
+#define SVP_CERT_NO_HULL 1
+#define SVP_CERT_DEPTH_FIRST 2
 typedef struct svp_cert_config {
     double delta;       /* J > delta is proven; 0 <= delta < 1 */
-    int64_t max_depth;  /* subdivision depth budget (reference default 48) */
-    int64_t max_boxes;  /* boxes per cell budget (reference default 255) */
-    int64_t tile_size;  /* cells per tile of the edge-hull flag rule (reference default 65536) */
-    int32_t prescreen;  /* 1: float Bernstein prescreen between hull and interval fallback (PrescreenCertificateConfig) */
-    int32_t reserved;
+    int64_t max_depth;  /* subdivision depth budget */
+    int64_t max_boxes;  /* boxes per cell budget */
+    int64_t tile_size;  /* cells per tile (edge-hull flag rule, arithmetic-failure rule) */
+    int32_t prescreen;  /* 1: float Bernstein prescreen between hull and interval fallback (PrescreenCertificateConfig);
+                           requires the edge-hull execution */
+    int32_t execution;  /* SVP_CERT_* flags above (0 = edge-hull execution) */
 } svp_cert_config;
 
 /* Mirrors feasibility.py:148-179 FeasibilityResult / PrescreenFeasibilityResult (state_hash and ids excluded). */
@@ -109,6 +120,16 @@ int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing
 int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi, int64_t n,
                        double delta, int64_t max_depth, int64_t max_boxes, svp_cell_verdict *out, void *stream);
 
+/* svp_classify_cells with the subdivision order chosen as the reference's _classify chooses it from the config class
+ * (feasibility.py:309-312, :351-357): SVP_SUBDIVIDE_LOWEST_FIRST (AdaptiveCertificateConfig and subclasses; the
+ * order of svp_classify_cells) or SVP_SUBDIVIDE_DEPTH_FIRST (the bare CertificateConfig: pending boxes as a stack,
+ * the left child first). */
+#define SVP_SUBDIVIDE_LOWEST_FIRST 0
+#define SVP_SUBDIVIDE_DEPTH_FIRST 1
+int svp_classify_cells_policy(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
+                              int64_t n, double delta, int64_t max_depth, int64_t max_boxes, int32_t policy,
+                              svp_cell_verdict *out, void *stream);
+
 /* svp_classify_cells without any device allocation.  No counterpart in the reference (whose subdivision runs in
  * Python on the host): it is for callers that cannot allocate device memory once they are running -- a host whose
  * device memory is owned by another allocator (a framework's caching pool, a fixed budget set at start-up) or a
@@ -116,7 +137,9 @@ int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_l
  * heaps live in one file-scope device array of 4,317,184 bytes (32 cells in flight x 257 heap slots), which every
  * device that loads the library keeps until process exit.  Limit: max_boxes <= 255 (larger is rejected with
  * SVP_EINVAL); n is unbounded (cells are processed 32 at a time).  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls share the array:
+ * address up (cudaGetSymbolAddress), so make that first call before any stream capture; the address is cached per
+ * device together with the id of the context it belongs to, and looked up again when that context was replaced
+ * (e.g. after cudaDeviceReset).  All calls share the array:
  * calls that overlap on the GPU (concurrent streams) race and must be serialised by the caller.  Results equal
  * svp_classify_cells' bit for bit. */
 int svp_classify_cells_noalloc(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,

@@ -45,8 +45,9 @@ def lib():
             L.oc_prescreen.argtypes = [P, I, I, I, P, P, I, I, D, D, D, D, D, P]
             L.oc_fallback_cell.argtypes = [P, P, D, P, P, P, P, P]
             L.oc_fallback_cell.restype = ctypes.c_int
-            L.oc_classify.argtypes = [P, P, P, P, D, I, I, P]
-            L.oc_certify_map.argtypes = [P, I, I, I, P, P, P, P, D, I, I, I, P, ctypes.c_int, D, D, D, D, D, P, P]
+            L.oc_classify.argtypes = [P, P, P, P, D, I, I, ctypes.c_int, P]
+            L.oc_certify_map.argtypes = [P, I, I, I, P, P, P, P, D, I, I, I, P, ctypes.c_int, D, D, D, D, D,
+                                         ctypes.c_int, ctypes.c_int, P, P]
             _lib = L
     return _lib
 
@@ -130,17 +131,21 @@ class _Cls(ctypes.Structure):
                 ("margin", ctypes.c_double), ("witness", ctypes.c_double * 3)]
 
 
-def classify(clo, chi, plo, phi, delta, max_depth=48, max_boxes=255):
+def classify(clo, chi, plo, phi, delta, max_depth=48, max_boxes=255, depth_first=False):
     r = _Cls()
     arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (clo, chi, plo, phi)]
-    lib().oc_classify(*[_ptr(a) for a in arrs], float(delta), int(max_depth), int(max_boxes), ctypes.byref(r))
+    lib().oc_classify(*[_ptr(a) for a in arrs], float(delta), int(max_depth), int(max_boxes), int(depth_first),
+                      ctypes.byref(r))
     return dict(status=r.status, reason=r.reason, boxes=r.boxes, depth=r.depth,
                 margin=r.margin if r.has_margin else None,
                 witness=tuple(r.witness) if r.has_witness else None)
 
 
-def certify_map(u, spacing, delta, *, max_depth=48, max_boxes=255, tile_size=65536, origin=(0., 0., 0.)):
-    """(rec_i int64[13], rec_f float64[6]) of feasibility.certify_map with PrescreenCertificateConfig."""
+def certify_map(u, spacing, delta, *, max_depth=48, max_boxes=255, tile_size=65536, origin=(0., 0., 0.),
+                hull=True, prescreen=True, depth_first=False):
+    """(rec_i int64[13], rec_f float64[6]) of feasibility.certify_map: PrescreenCertificateConfig by default;
+    prescreen=False the CompiledFallback execution, hull=False the whole-cell Bernstein execution of the bare /
+    Adaptive configs (depth_first=True for the bare CertificateConfig)."""
     u = np.ascontiguousarray(u, dtype=np.float64)
     nz, ny, nx = u.shape[:3]
     h = np.ascontiguousarray(spacing, dtype=np.float64)
@@ -150,6 +155,6 @@ def certify_map(u, spacing, delta, *, max_depth=48, max_boxes=255, tile_size=655
     use = int(np.all(np.isfinite(D)) and not (nonzero.size and nonzero.min() < np.finfo(np.float64).tiny))
     rec_i, rec_f = np.zeros(13, np.int64), np.zeros(6)
     lib().oc_certify_map(_ptr(u), nz, ny, nx, _ptr(h), *[_ptr(a) for a in axes], float(delta), int(max_depth),
-                         int(max_boxes), int(tile_size), _ptr(D), use, G12, G6, G3, SQRT27_UP, ETA, _ptr(rec_i),
-                         _ptr(rec_f))
+                         int(max_boxes), int(tile_size), _ptr(D), use and prescreen, G12, G6, G3, SQRT27_UP, ETA,
+                         int(hull), int(depth_first), _ptr(rec_i), _ptr(rec_f))
     return rec_i, rec_f

@@ -368,8 +368,11 @@ static int split_(const box_t *cur, int axis, box_t *left, box_t *right) {
     return ok;
 }
 
+/* depth_first = 0: lowest-bound-first heap of (key, serial) (AdaptiveCertificateConfig, feasibility.py:319);
+ * depth_first = 1: the bare CertificateConfig's pending list used as a stack (feasibility.py:326, :353-354): pop the
+ * last box, push the right child and then the left one. */
 void oc_classify(const double *clo, const double *chi, const double *plo, const double *phi, double delta,
-                 int64_t max_depth, int64_t max_boxes, cls_t *res) {
+                 int64_t max_depth, int64_t max_boxes, int depth_first, cls_t *res) {
     (void)plo;
     memset(res, 0, sizeof *res);
     double root_lower = min27(clo);
@@ -396,15 +399,20 @@ void oc_classify(const double *clo, const double *chi, const double *plo, const 
             cls_result(res, ST_UNCERTAIN, root_lower, boxes, depth_used, NULL, R_BOX_BUDGET, delta);
             free(heap); return;
         }
-        /* pop the minimum (key, serial) */
-        box_t cur = heap[0];
-        heap[0] = heap[--nheap];
-        for (int64_t i = 0;;) {
-            int64_t l = 2 * i + 1, r = l + 1, m = i;
-            if (l < nheap && heap_less(&heap[l], &heap[m])) m = l;
-            if (r < nheap && heap_less(&heap[r], &heap[m])) m = r;
-            if (m == i) break;
-            box_t t = heap[i]; heap[i] = heap[m]; heap[m] = t; i = m;
+        box_t cur;
+        if (depth_first) {
+            cur = heap[--nheap];             /* stack pop */
+        } else {
+            /* pop the minimum (key, serial) */
+            cur = heap[0];
+            heap[0] = heap[--nheap];
+            for (int64_t i = 0;;) {
+                int64_t l = 2 * i + 1, r = l + 1, m = i;
+                if (l < nheap && heap_less(&heap[l], &heap[m])) m = l;
+                if (r < nheap && heap_less(&heap[r], &heap[m])) m = r;
+                if (m == i) break;
+                box_t t = heap[i]; heap[i] = heap[m]; heap[m] = t; i = m;
+            }
         }
         boxes += 1;
         if (cur.depth > depth_used) depth_used = cur.depth;
@@ -444,6 +452,11 @@ void oc_classify(const double *clo, const double *chi, const double *plo, const 
         memcpy(right.low, cur.low, sizeof right.low); memcpy(right.high, cur.high, sizeof right.high);
         left.high[axis] = mid; right.low[axis] = mid;
         left.depth = right.depth = cur.depth + 1;
+        if (depth_first) {                   /* stack push: right, then left (popped first) */
+            heap[nheap++] = right;
+            heap[nheap++] = left;
+            continue;
+        }
         box_t *kids[2] = {&left, &right};
         for (int k = 0; k < 2; k++) {
             serial += 1;
@@ -470,7 +483,7 @@ void oc_classify(const double *clo, const double *chi, const double *plo, const 
 void oc_certify_map(const double *u, int64_t nz, int64_t ny, int64_t nx, const double *spacing, const double *axx,
                     const double *axy, const double *axz, double delta, int64_t max_depth, int64_t max_boxes,
                     int64_t tile_size, const double *D, int use_prescreen, double g12, double g6, double g3,
-                    double sq27, double eta, int64_t *rec_i, double *rec_f) {
+                    double sq27, double eta, int use_hull, int depth_first, int64_t *rec_i, double *rec_f) {
     int64_t n = (nz - 1) * (ny - 1) * (nx - 1), nn = nz * ny * nx;
     for (int k = 0; k < 13; k++) rec_i[k] = 0;
     for (int k = 0; k < 6; k++) rec_f[k] = NAN;
@@ -506,7 +519,12 @@ void oc_certify_map(const double *u, int64_t nz, int64_t ny, int64_t nx, const d
     double *margin = (double *)malloc(sizeof(double) * (size_t)n);
     uint8_t *flag = (uint8_t *)malloc((size_t)n);
     uint8_t *stage = (uint8_t *)calloc((size_t)n, 1);        /* 1 hull-proven, 2 prescreen-proven, 3 fallback */
-    oc_edge_hull(u, nz, ny, nx, spacing, delta, 0, n, margin, flag);
+    if (use_hull) {
+        oc_edge_hull(u, nz, ny, nx, spacing, delta, 0, n, margin, flag);
+    } else {                                 /* whole-cell Bernstein execution: no preproof (feasibility.py:447) */
+        for (int64_t c = 0; c < n; c++) { margin[c] = NAN; flag[c] = 1; }
+        use_prescreen = 0;
+    }
     int64_t unknown = 0, bad = 0, boxes = 0, maxd = 0, fast = 0, fallback = 0, prescreened = 0;
     int64_t witness_cell = -1;
     double wpt[3] = {NAN, NAN, NAN};
@@ -575,7 +593,7 @@ void oc_certify_map(const double *u, int64_t nz, int64_t ny, int64_t nx, const d
             double mn = min27(clo);
             if (mn > 0) { any_safe = 1; if (mn < safe_min) safe_min = mn; continue; }
             cls_t r;
-            oc_classify(clo, chi, plo, phi, delta, max_depth, max_boxes, &r);
+            oc_classify(clo, chi, plo, phi, delta, max_depth, max_boxes, depth_first, &r);
             if (r.has_margin) { if (r.margin < lowest) lowest = r.margin; any_margin = 1; }
             if (r.reason == R_ARITH) arith = 1;
             boxes += r.boxes - 1;
@@ -594,6 +612,7 @@ void oc_certify_map(const double *u, int64_t nz, int64_t ny, int64_t nx, const d
     if ((fast || prescreened) && status == ST_FEASIBLE) reason = R_ENCLOSURE;
     rec_i[0] = status; rec_i[1] = reason; rec_i[2] = n; rec_i[3] = unknown; rec_i[4] = bad; rec_i[5] = boxes;
     rec_i[6] = maxd; rec_i[7] = witness_cell; rec_i[8] = fast; rec_i[9] = fallback; rec_i[10] = prescreened;
+    if (!use_hull) rec_i[9] = 0;   /* the plain FeasibilityResult has no stage counts */
     if (any_margin && !arith) {
         rec_f[1] = lowest;
         rec_f[0] = delta == 0. ? lowest : nextafter(lowest + delta, -INFINITY);

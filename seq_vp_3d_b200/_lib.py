@@ -28,7 +28,7 @@ class Grid(ctypes.Structure):
 
 class CertConfig(ctypes.Structure):
     _fields_ = [("delta", D), ("max_depth", I64), ("max_boxes", I64), ("tile_size", I64),
-                ("prescreen", I32), ("reserved", I32)]
+                ("prescreen", I32), ("execution", I32)]
 
 
 class CertResult(ctypes.Structure):
@@ -65,6 +65,7 @@ SIGNATURES = {
     "svp_fallback_arrays": [P, I64, P, D, P, P, P, P, P, P, P],
     "svp_classify_cells": [P, P, P, P, I64, D, I64, I64, P, P],
     "svp_classify_cells_noalloc": [P, P, P, P, I64, D, I64, I64, P, P],
+    "svp_classify_cells_policy": [P, P, P, P, I64, D, I64, I64, I32, P, P],
     "svp_certifier_create": [P, P, P],
     "svp_certifier_destroy": [P],
     "svp_certify_map": [P, P, P, P],

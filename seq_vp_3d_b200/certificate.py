@@ -26,44 +26,159 @@ REASONS = ("positive_enclosure_cover", "positive_bernstein_cover", "JACOBIAN_VIO
            "subdivision_budget", "NONFINITE_STATE", "NONZERO_BOUNDARY", "INVALID_DOMAIN", "unsupported_arithmetic",
            "sample_witness", "subdivision_witness", "box_budget", "depth_budget", "positive_edge_hull",
            "not_checked")
+BASE_VERSION = "q1-3d-interval-bernstein-v1"
 CERTIFICATE_VERSION = "q1-3d-parallel-hoisted-edge-hull-float-bernstein-prescreen-compiled-bernstein-v1"
 
 
+def _integer(value, name, minimum):
+    if isinstance(value, bool) or not isinstance(value, (int, np.integer)) or value < minimum:
+        raise InputValidationError(f"{name}: expected an integer >= {minimum}")
+    return int(value)
+
+
+def _require(ok, message):
+    if not ok:
+        raise InputValidationError(message)
+
+
+# The certificate configuration family of the reference (feasibility.py:22-121), with its defaults, validation and
+# isinstance structure: code that picks an execution with isinstance(config, ...) reads these classes the same way.
+# Each class selects a GPU execution: the bare class and AdaptiveCertificateConfig prove every cell by interval
+# Bernstein subdivision (depth-first for the bare class, lowest bound first for the adaptive one); the Enclosure family
+# runs the edge-hull preproof first; PrescreenCertificateConfig adds the float Bernstein prescreen.  The compiled,
+# parallel and worker-count fields name the reference's CPU executions, whose results are the same; on the GPU they
+# select nothing.
 @dataclass(frozen=True)
 class CertificateConfig:
-    """Subdivision budgets and the delta of J > delta (feasibility.py:22-117 config family).
-
-    prescreen=True is the reference's PrescreenCertificateConfig execution (hull, float prescreen, interval
-    fallback); prescreen=False its CompiledFallback/ParallelEnclosure execution (hull, interval fallback)."""
-    delta: float = 0.
-    max_depth: int = 48
+    delta: float = .01
+    max_depth: int = 12
     max_boxes: int = 255
-    tile_size: int = 65536
-    prescreen: bool = True
+    tile_size: int = 8192
 
     def __post_init__(self):
-        d = float(self.delta)
-        if not np.isfinite(d) or d < 0 or d >= 1:
-            raise InputValidationError("delta: require 0 <= delta < 1")
-        object.__setattr__(self, "delta", 0.0 if d == 0 else d)
+        try:
+            d = float(self.delta)
+        except (TypeError, ValueError):
+            raise InputValidationError("delta: finite real required") from None
+        _require(np.isfinite(d), "delta: finite real required")
+        _require(0 <= d < 1, "delta: require 0 <= delta < 1")
+        object.__setattr__(self, "delta", 0.0 if d == 0 else d)     # one spelling of zero (-0.0 -> +0.0)
         for key, minimum in (("max_depth", 0), ("max_boxes", 1), ("tile_size", 1)):
-            v = getattr(self, key)
-            if isinstance(v, bool) or not isinstance(v, (int, np.integer)) or v < minimum:
-                raise InputValidationError(f"{key}: expected an integer >= {minimum}")
-            object.__setattr__(self, key, int(v))
-        if self.max_depth > 120:
-            raise InputValidationError("adaptive max_depth must be <= 120")
+            object.__setattr__(self, key, _integer(getattr(self, key), key, minimum))
+
+    # GPU execution selected by the class (svp_cert_config.prescreen / .execution)
+    @property
+    def hull(self):
+        return isinstance(self, EnclosureCertificateConfig)
+
+    @property
+    def prescreen(self):
+        return isinstance(self, PrescreenCertificateConfig)
+
+    @property
+    def depth_first(self):
+        return not isinstance(self, AdaptiveCertificateConfig)
 
 
-def PrescreenCertificateConfig(delta=.01, max_depth=48, max_boxes=255, tile_size=8192, fallback_workers=8, **_):
-    """The reference's default production certificate (feasibility.py:107); fallback_workers has no GPU meaning."""
-    return CertificateConfig(delta=delta, max_depth=max_depth, max_boxes=max_boxes, tile_size=tile_size,
-                             prescreen=True)
+@dataclass(frozen=True)
+class AdaptiveCertificateConfig(CertificateConfig):
+    """Lowest-lower-bound-first subdivision with a deeper budget."""
+    max_depth: int = 48
+    policy: str = "lowest_bound_first_v1"
+
+    def __post_init__(self):
+        super().__post_init__()
+        _require(self.policy == "lowest_bound_first_v1", "unsupported adaptive certificate policy")
+        _require(self.max_depth <= 120, "adaptive max_depth must be <= 120")
+
+
+@dataclass(frozen=True)
+class EnclosureCertificateConfig(AdaptiveCertificateConfig):
+    """Edge-hull whole-cell preproof, then the adaptive subdivision of the cells it leaves."""
+    prepass: str = "edge_hull_v1"
+
+    def __post_init__(self):
+        super().__post_init__()
+        _require(self.prepass == "edge_hull_v1", "unsupported enclosure prepass")
+
+
+@dataclass(frozen=True)
+class CompiledEnclosureCertificateConfig(EnclosureCertificateConfig):
+    kernel: str = "numba-directed-edge-hull-v1"
+
+    def __post_init__(self):
+        super().__post_init__()
+        _require(self.kernel in ("numba-directed-edge-hull-v1", "numba-hoisted-edge-hull-v1"),
+                 "unsupported compiled enclosure kernel")
+
+
+@dataclass(frozen=True)
+class ParallelEnclosureCertificateConfig(CompiledEnclosureCertificateConfig):
+    kernel: str = "numba-parallel-hoisted-edge-hull-v1"
+    fallback_workers: int = 8
+
+    def __post_init__(self):
+        EnclosureCertificateConfig.__post_init__(self)
+        _require(self.kernel == "numba-parallel-hoisted-edge-hull-v1",
+                 "parallel certificate requires the parallel hoisted kernel")
+        object.__setattr__(self, "fallback_workers", _integer(self.fallback_workers, "fallback_workers", 1))
+
+
+@dataclass(frozen=True)
+class CompiledFallbackCertificateConfig(ParallelEnclosureCertificateConfig):
+    fallback_kernel: str = "numba-bernstein-fallback-v1"
+
+    def __post_init__(self):
+        super().__post_init__()
+        _require(self.fallback_kernel == "numba-bernstein-fallback-v1", "unsupported compiled fallback kernel")
+
+
+@dataclass(frozen=True)
+class PrescreenCertificateConfig(CompiledFallbackCertificateConfig):
+    """Hull preproof, the rigorous float Bernstein prescreen of the cells it leaves, then the interval fallback."""
+    prescreen_kernel: str = "numba-float-bernstein-apriori-v1"
+
+    def __post_init__(self):
+        super().__post_init__()
+        _require(self.prescreen_kernel == "numba-float-bernstein-apriori-v1", "unsupported prescreen kernel")
+
+
+def certificate_version(config):
+    """The record's certificate_version for a config (feasibility.py:123-137)."""
+    if isinstance(config, PrescreenCertificateConfig):
+        return CERTIFICATE_VERSION
+    if isinstance(config, CompiledFallbackCertificateConfig):
+        return "q1-3d-parallel-hoisted-edge-hull-compiled-bernstein-v1"
+    if isinstance(config, ParallelEnclosureCertificateConfig):
+        return "q1-3d-parallel-hoisted-edge-hull-bernstein-v1"
+    if isinstance(config, CompiledEnclosureCertificateConfig):
+        if config.kernel == "numba-hoisted-edge-hull-v1":
+            return "q1-3d-hoisted-edge-hull-bernstein-v1"
+        return "q1-3d-compiled-edge-hull-bernstein-v1"
+    if isinstance(config, EnclosureCertificateConfig):
+        return "q1-3d-edge-hull-bernstein-v1"
+    return BASE_VERSION
+
+
+def execution_of(config):
+    """(prescreen, execution flags) of svp_cert_config for a config object -- ours or the reference's own classes,
+    read by the fields that distinguish them (prepass: edge hull; prescreen_kernel: prescreen; policy: adaptive)."""
+    hull = hasattr(config, "prepass")
+    prescreen = hasattr(config, "prescreen_kernel")
+    adaptive = hasattr(config, "policy")
+    flags = (0 if hull else 1) | (0 if adaptive else 2)
+    return (1 if prescreen else 0), flags
+
+
+# The GPU production configuration of the native loop: the prescreen execution with the budgets the reference's
+# native route passes (delta 0, depth 48, 255 boxes, tiles of 65536 cells).
+NATIVE_CERTIFICATE = PrescreenCertificateConfig(delta=0., max_depth=48, max_boxes=255, tile_size=65536)
 
 
 @dataclass(frozen=True)
 class FeasibilityResult:
-    """feasibility.py:148-179 PrescreenFeasibilityResult fields."""
+    """feasibility.py:148-179 FeasibilityResult fields plus the Enclosure/Prescreen counts (0 where the config's
+    execution has no such stage)."""
     status: str
     min_jd_lower_bound: float | None
     min_margin_lower_bound: float | None
@@ -80,7 +195,7 @@ class FeasibilityResult:
     grid_id: str
     delta_hex: str
     config: CertificateConfig
-    certificate_version: str = CERTIFICATE_VERSION
+    certificate_version: str = BASE_VERSION
     n_fast_cells: int = 0
     n_fallback_cells: int = 0
     n_prescreen_cells: int = 0
@@ -99,8 +214,8 @@ class Certifier:
         require_cuda()
         self.grid, self.config = grid, config
         self._g = grid_struct(grid)
-        cfg = _lib.CertConfig(config.delta, config.max_depth, config.max_boxes, config.tile_size,
-                              1 if config.prescreen else 0, 0)
+        prescreen, execution = execution_of(config)
+        cfg = _lib.CertConfig(config.delta, config.max_depth, config.max_boxes, config.tile_size, prescreen, execution)
         handle = ctypes.c_void_p()
         _lib.call("svp_certifier_create", ctypes.byref(self._g), ctypes.byref(cfg), ctypes.byref(handle))
         self._h = handle
@@ -147,7 +262,8 @@ def result_from_record(r, grid, config, state_hash):
         n_uncertain=int(r.n_uncertain), n_infeasible=int(r.n_infeasible), n_boxes=int(r.n_boxes),
         max_depth=int(r.max_depth), witness_cell=None if r.witness_cell < 0 else int(r.witness_cell),
         witness_reference_point=point, reason=REASONS[r.reason], state_hash=state_hash, grid_id=grid.grid_id,
-        delta_hex=float(config.delta).hex(), config=config, n_fast_cells=int(r.n_fast_cells),
+        delta_hex=float(config.delta).hex(), config=config, certificate_version=certificate_version(config),
+        n_fast_cells=int(r.n_fast_cells),
         n_fallback_cells=int(r.n_fallback_cells), n_prescreen_cells=int(r.n_prescreen_cells))
 
 
@@ -252,15 +368,16 @@ def fallback_arrays(vertices, spacing, delta, errors=None):
             smp.reshape(shape))
 
 
-def classify_cells(c_lo, c_hi, p_lo, p_hi, delta, max_depth=48, max_boxes=255, stream=None):
-    """Subdivision verdicts (feasibility.py:295 _classify) of n cells: list of dicts."""
+def classify_cells(c_lo, c_hi, p_lo, p_hi, delta, max_depth=48, max_boxes=255, depth_first=False, stream=None):
+    """Subdivision verdicts (feasibility.py:295 _classify) of n cells: list of dicts.  depth_first selects the bare
+    CertificateConfig's order (a stack, left child first); the default is the adaptive lowest-bound-first order."""
     arrs = [to_device(np.asarray(a).reshape(-1, 27) if not isinstance(a, torch.Tensor) else a.reshape(-1, 27))
             for a in (c_lo, c_hi, p_lo, p_hi)]
     n = arrs[0].shape[0]
     out = torch.empty((n, ctypes.sizeof(_lib.CellVerdict)), dtype=torch.uint8, device=arrs[0].device)
     if n:
-        _lib.call("svp_classify_cells", *[ptr(a) for a in arrs], n, float(delta), int(max_depth), int(max_boxes),
-                  ptr(out), stream_ptr(stream))
+        _lib.call("svp_classify_cells_policy", *[ptr(a) for a in arrs], n, float(delta), int(max_depth),
+                  int(max_boxes), 1 if depth_first else 0, ptr(out), stream_ptr(stream))
     raw = out.cpu().numpy()
     res = []
     for k in range(n):

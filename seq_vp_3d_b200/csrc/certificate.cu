@@ -9,6 +9,7 @@
 //   4. the record: status, reason, counts, bounds and the first witness (feasibility.py:755-771).
 // This file is compiled with -fmad=false and uses explicit round-to-nearest intrinsics for every certificate
 // operation, so no product can be contracted into an FMA.
+#include <cuda.h>
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
@@ -504,12 +505,18 @@ __device__ __forceinline__ double warp_min27(double x) {
     return x;
 }
 
+// Priority queue of the pending boxes of one cell.  Lowest-bound-first (AdaptiveCertificateConfig family): key = the
+// box's lowest Bernstein coefficient, ties by creation serial (feasibility.py:319 heap of (lower, serial, box)).
+// Depth-first (the bare CertificateConfig's list used as a stack, feasibility.py:353-354): the most recently pushed
+// box pops first, i.e. the largest serial, with the left child pushed after the right one.
 struct WarpHeap {
     double *coef, *meta;
     long long *serial;
     int *depth, *heap, *freel;
     int size, nfree;
+    int depth_first;
     __device__ bool less(int a, int b) const {
+        if (depth_first) return serial[a] > serial[b];
         double ka = meta[8 * a + 6], kb = meta[8 * b + 6];
         return ka < kb || (ka == kb && serial[a] < serial[b]);
     }
@@ -561,7 +568,7 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
                                                        const double *__restrict__ phi, const long long *rows,
                                                        long long n, double delta, long long max_depth,
                                                        long long max_boxes, svp_cell_verdict *out, char *scratch,
-                                                       long long slots) {
+                                                       long long slots, int depth_first) {
     const int lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -575,6 +582,7 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
     H.depth = (int *)(H.serial + slots);
     H.heap = H.depth + slots;
     H.freel = H.heap + slots;
+    H.depth_first = depth_first;
     for (long long i = gw; i < n; i += nw) {
         long long row = rows ? rows[i] : i;
         double lo = act ? clo[27 * row + lane] : INF;
@@ -694,7 +702,8 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
                 }
                 H.meta[8 * slot + 6] = kl; H.meta[8 * rslot + 6] = kr;
                 H.depth[slot] = depth + 1; H.depth[rslot] = depth + 1;
-                H.serial[slot] = serial + 1; H.serial[rslot] = serial + 2;
+                // the heap pushes left then right; the depth-first stack pushes right then left
+                H.serial[slot] = serial + (depth_first ? 2 : 1); H.serial[rslot] = serial + (depth_first ? 1 : 2);
             }
             serial += 2;
             __syncwarp();
@@ -988,17 +997,17 @@ extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const doub
 static int classify_launch(const double *c_lo, const double *c_hi, const double *p_hi, const long long *rows,
                            long long n, double delta, long long max_depth, long long max_boxes,
                            svp_cell_verdict *out, char *scratch, long long warps, long long slots,
-                           cudaStream_t stream) {
+                           int depth_first, cudaStream_t stream) {
     long long threads = 128, blocks = div_up(warps * 32, threads);
     { svp::KernelTimer _t("classify_kernel", stream); SVP_LAUNCH(classify_kernel<<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(c_lo, c_hi, p_hi, rows, n, delta, max_depth,
-                                                                        max_boxes, out, scratch, slots)); }
+                                                                        max_boxes, out, scratch, slots, depth_first)); }
     SVP_LAUNCH_CHECK("classify_kernel");
     return SVP_OK;
 }
 
-extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
-                                  int64_t n, double delta, int64_t max_depth, int64_t max_boxes,
-                                  svp_cell_verdict *out, void *stream) {
+static int classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi, int64_t n,
+                          double delta, int64_t max_depth, int64_t max_boxes, int depth_first,
+                          svp_cell_verdict *out, void *stream) {
     SVP_REQUIRE(n >= 0 && max_depth >= 0 && max_boxes >= 1, "svp_classify_cells: invalid arguments");
     if (n == 0) return SVP_OK;
     SVP_REQUIRE(c_lo && c_hi && p_lo && p_hi && out, "svp_classify_cells: null pointer");
@@ -1009,7 +1018,8 @@ extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const 
     warps = (warps + 3) / 4 * 4;  // whole blocks of 4 warps
     char *scratch = nullptr;
     SVP_CUDA(scratch_alloc((void **)&scratch, warp_scratch_bytes(slots) * warps, s));
-    int rc = classify_launch(c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, warps, slots, s);
+    int rc = classify_launch(c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, warps, slots,
+                             depth_first, s);
     cudaError_t e = scratch_free(scratch, s);
     if (rc != SVP_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
@@ -1017,6 +1027,21 @@ extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const 
 }
 
 }  // namespace svp
+
+extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
+                                  int64_t n, double delta, int64_t max_depth, int64_t max_boxes,
+                                  svp_cell_verdict *out, void *stream) {
+    return svp::classify_cells(c_lo, c_hi, p_lo, p_hi, n, delta, max_depth, max_boxes, 0, out, stream);
+}
+
+extern "C" int svp_classify_cells_policy(const double *c_lo, const double *c_hi, const double *p_lo,
+                                         const double *p_hi, int64_t n, double delta, int64_t max_depth,
+                                         int64_t max_boxes, int32_t policy, svp_cell_verdict *out, void *stream) {
+    SVP_REQUIRE(policy == SVP_SUBDIVIDE_LOWEST_FIRST || policy == SVP_SUBDIVIDE_DEPTH_FIRST,
+                "svp_classify_cells_policy: unknown subdivision policy");
+    return svp::classify_cells(c_lo, c_hi, p_lo, p_hi, n, delta, max_depth, max_boxes,
+                               policy == SVP_SUBDIVIDE_DEPTH_FIRST, out, stream);
+}
 
 // ---------------------------------------------------------------------------------------------- certifier handle
 struct svp_certifier {
@@ -1084,6 +1109,10 @@ extern "C" int svp_certifier_create(const svp_grid *g, const svp_cert_config *cf
     SVP_REQUIRE(cfg->max_depth >= 0 && cfg->max_boxes >= 1 && cfg->tile_size >= 1,
                 "svp_certifier_create: invalid budgets/tile size");
     SVP_REQUIRE(cfg->max_boxes <= (1LL << 24), "svp_certifier_create: max_boxes above 2^24");
+    SVP_REQUIRE((cfg->execution & ~(SVP_CERT_NO_HULL | SVP_CERT_DEPTH_FIRST)) == 0,
+                "svp_certifier_create: unknown execution flags");
+    SVP_REQUIRE(!(cfg->prescreen && (cfg->execution & SVP_CERT_NO_HULL)),
+                "svp_certifier_create: the prescreen runs only after the edge-hull preproof");
     svp_certifier *c = new svp_certifier();
     c->grid = *g;
     c->cfg = *cfg;
@@ -1132,6 +1161,8 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = c->ncell, tile = c->cfg.tile_size;
     const double delta = c->cfg.delta;
+    const bool hull = !(c->cfg.execution & SVP_CERT_NO_HULL);
+    const int depth_first = (c->cfg.execution & SVP_CERT_DEPTH_FIRST) ? 1 : 0;
     const double nan = std::nan("");
     memset(out, 0, sizeof *out);
     out->status = ST_UNCERTAIN;
@@ -1145,11 +1176,16 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     { svp::KernelTimer _t("precheck_kernel", s); SVP_LAUNCH(precheck_kernel<<<blocks_for(n_nodes(&c->grid), 256, 8), 256, 0, s>>>(u, c->cg, c->grid.x0, c->grid.y0,
                                                                             c->grid.z0, c->acc)); }
     SVP_LAUNCH_CHECK("precheck_kernel");
-    { svp::KernelTimer _t("edge_hull_kernel", s); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag)); }
-    SVP_LAUNCH_CHECK("edge_hull_kernel");
-    SVP_CUDA(cudaMemsetAsync(c->tile_bad, 0, sizeof(int) * c->ntiles, s));
     SVP_CUDA(cudaMemsetAsync(c->tile_fail, 0, sizeof(int) * c->ntiles, s));
-    SVP_LAUNCH(tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad));
+    if (hull) {
+        { svp::KernelTimer _t("edge_hull_kernel", s); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag)); }
+        SVP_LAUNCH_CHECK("edge_hull_kernel");
+        SVP_CUDA(cudaMemsetAsync(c->tile_bad, 0, sizeof(int) * c->ntiles, s));
+        SVP_LAUNCH(tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad));
+    } else {
+        // the whole-cell Bernstein execution (feasibility.py:447-491): no preproof, every cell to the fallback
+        SVP_CUDA(cudaMemsetAsync(c->tile_bad, 1, sizeof(int) * c->ntiles, s));
+    }
     SVP_LAUNCH(hull_stage_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->margin, c->tile_bad, n, tile, c->sel, c->acc));
     SVP_LAUNCH_CHECK("hull stage");
     int rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list1, c->counts, n, s);
@@ -1199,7 +1235,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
             warps = (warps + 3) / 4 * 4;
             if (warps > c->heap_warps) warps = c->heap_warps;
             rc = classify_launch(clo, chi, phi, c->list3, n3, delta, c->cfg.max_depth, c->cfg.max_boxes,
-                                 c->verdicts, c->heap, warps, c->heap_slots, s);
+                                 c->verdicts, c->heap, warps, c->heap_slots, depth_first, s);
             if (rc) return rc;
             SVP_LAUNCH(verdict_stage_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
             SVP_LAUNCH(witness_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
@@ -1226,7 +1262,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     out->max_depth = acc.max_depth;
     out->witness_cell = bad ? acc.witness_cell : -1;
     out->n_fast_cells = fast;
-    out->n_fallback_cells = fallback;
+    out->n_fallback_cells = hull ? fallback : 0;   // the plain FeasibilityResult has no stage counts
     out->n_prescreen_cells = pre;
     if (acc.any_margin && !acc.arith) {
         double lowest = key_value(acc.lowest_key);
@@ -1259,18 +1295,49 @@ static __device__ __align__(256) char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[256] = {};
+unsigned long long g_noalloc_ctx[256] = {};   // unique id of the context the cached address belongs to
 
-// Device address of the scratch array on the current device; the first call on a device looks it up.
+// Unique id of the calling thread's current context (0 when there is none yet), through the driver entry points so
+// that the library keeps linking against the runtime alone.  A context created after a cudaDeviceReset gets a new
+// id, so an address cached for the old context is never reused.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+int current_context_id(unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        SVP_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void **)&get_current, 12000, cudaEnableDefault,
+                                                  &q1));
+        SVP_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", (void **)&get_id, 12000, cudaEnableDefault, &q2));
+        SVP_REQUIRE(q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess && get_current && get_id,
+                    "svp_classify_cells_noalloc: driver context queries unavailable");
+    }
+    CUcontext ctx = nullptr;
+    *id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS) return cuda_fail(cudaErrorUnknown, "cuCtxGetCurrent");
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return cuda_fail(cudaErrorUnknown, "cuCtxGetId");
+    return SVP_OK;
+}
+
+// Device address of the scratch array in the current device's context.  The first call on a device (and the first
+// call after that device's context was replaced) looks it up with cudaGetSymbolAddress; later calls reuse it.
 int noalloc_scratch(char **out) {
     int dev = -1;
     SVP_CUDA(cudaGetDevice(&dev));
     SVP_REQUIRE(dev >= 0 && dev < 256, "svp_classify_cells_noalloc: device ordinal out of range");
+    unsigned long long ctx = 0;
+    int rc = current_context_id(&ctx);
+    if (rc) return rc;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || ctx == 0 || g_noalloc_ctx[dev] != ctx) {
         void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);   // creates the primary context if needed
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(svp classify scratch)");
+        rc = current_context_id(&ctx);
+        if (rc) return rc;
         g_noalloc_ptr[dev] = p;
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = (char *)g_noalloc_ptr[dev];
     return SVP_OK;
@@ -1296,6 +1363,6 @@ extern "C" int svp_classify_cells_noalloc(const double *c_lo, const double *c_hi
     SVP_REQUIRE(warp_scratch_bytes(slots) * (size_t)warps <= kNoAllocBytes,
                 "svp_classify_cells_noalloc: scratch capacity exceeded");
     SVP_LAUNCH(classify_kernel<<<(unsigned)(warps * 32 / 128), 128, 0, (cudaStream_t)stream>>>(
-        c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, slots));
+        c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, slots, 0));
     return SVP_OK;
 }

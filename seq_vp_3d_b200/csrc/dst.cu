@@ -508,12 +508,16 @@ static int set_denominator(svp_pair *p, double a, double b, int metric, cudaStre
     }
     double *dev = nullptr;
     SVP_CUDA(scratch_alloc((void **)&dev, sizeof(double) * host.size(), s));
-    SVP_CUDA(cudaMemcpyAsync(dev, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice, s));
-    SVP_LAUNCH(den_kernel<<<blocks_for(p->q.nfree, 256, 8), 256, 0, s>>>(p->den, p->q.fx, p->q.fy, p->q.fz, dev + off[0],
-                                                              dev + off[1], dev + off[2], dev + off[3], dev + off[4],
-                                                              dev + off[5], p->q.omega, a, b, metric));
-    SVP_LAUNCH_CHECK("den_kernel");
-    SVP_CUDA(scratch_free(dev, s));
+    cudaError_t ce = cudaMemcpyAsync(dev, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess)
+        SVP_LAUNCH_KEEP(den_kernel<<<blocks_for(p->q.nfree, 256, 8), 256, 0, s>>>(
+            p->den, p->q.fx, p->q.fy, p->q.fz, dev + off[0], dev + off[1], dev + off[2], dev + off[3], dev + off[4],
+            dev + off[5], p->q.omega, a, b, metric));
+    cudaError_t le = cudaGetLastError();
+    cudaError_t fe = scratch_free(dev, s);
+    if (ce != cudaSuccess) return cuda_fail(ce, "den copy");
+    if (le != cudaSuccess) return cuda_fail(le, "den_kernel");
+    if (fe != cudaSuccess) return cuda_fail(fe, "den free");
     p->den_a = a;
     p->den_b = b;
     p->den_metric = metric;

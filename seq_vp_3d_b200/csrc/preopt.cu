@@ -522,9 +522,9 @@ extern "C" int svp_pre_level(const float *fixed, const float *moving, int32_t D,
     const int dz = D - 2, dy = H - 2, dx = W - 2;
     auto smooth = [&](float *x, const float *k, int r) -> int {
         // z, then y, then x; x -> tmp -> x -> tmp -> ... ending in x
-        SVP_LAUNCH(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(x, tmp, dz, dy, dx, 0, k, r));
-        SVP_LAUNCH(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(tmp, step, dz, dy, dx, 1, k, r));
-        SVP_LAUNCH(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(step, x, dz, dy, dx, 2, k, r));
+        SVP_LAUNCH_KEEP(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(x, tmp, dz, dy, dx, 0, k, r));
+        SVP_LAUNCH_KEEP(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(tmp, step, dz, dy, dx, 1, k, r));
+        SVP_LAUNCH_KEEP(gauss_axis_kernel<<<grid_for(ni), PT, 0, s>>>(step, x, dz, dy, dx, 2, k, r));
         return SVP_OK;
     };
     for (int it = 0; it < iterations; it++) {
@@ -537,11 +537,12 @@ extern "C" int svp_pre_level(const float *fixed, const float *moving, int32_t D,
         // PyTorch divides by the float bias corrections as a multiplication by their float32 reciprocals
         const float rc1 = 1.f / (float)(1. - std::pow(prm->beta1, t));
         const float rc2 = 1.f / (float)(1. - std::pow(prm->beta2, t));
-        { svp::KernelTimer _t("adam_kernel", s); SVP_LAUNCH(adam_kernel<<<ab, PT, 0, s>>>(ni, grad, m, v, (float)prm->beta1, (float)(1. - prm->beta1), (float)prm->beta2, (float)(1. - prm->beta2), (float)prm->lr, rc1, rc2, (float)prm->eps, step, apart)); }
-        SVP_LAUNCH(cap_kernel<<<1, PT, 0, s>>>(apart, (int)ab, prm->cap, scale, hits));
-        SVP_LAUNCH(update_kernel<<<ab, PT, 0, s>>>(ni, step, scale, u_int));
+        { svp::KernelTimer _t("adam_kernel", s); SVP_LAUNCH_KEEP(adam_kernel<<<ab, PT, 0, s>>>(ni, grad, m, v, (float)prm->beta1, (float)(1. - prm->beta1), (float)prm->beta2, (float)(1. - prm->beta2), (float)prm->lr, rc1, rc2, (float)prm->eps, step, apart)); }
+        SVP_LAUNCH_KEEP(cap_kernel<<<1, PT, 0, s>>>(apart, (int)ab, prm->cap, scale, hits));
+        SVP_LAUNCH_KEEP(update_kernel<<<ab, PT, 0, s>>>(ni, step, scale, u_int));
         if (prm->sigma_field > 0) smooth(u_int, taps + kg.size(), rf);
-        SVP_LAUNCH_CHECK("pre-optimizer iteration");
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) return bail(cuda_fail(le, "pre-optimizer iteration"));
     }
     unsigned long long h_hits = 0;
     float th[12];
@@ -607,13 +608,14 @@ extern "C" int svp_image_downsample(const double *src, int32_t nz, int32_t ny, i
         cudaMemcpyAsync(ldev, left.data(), sizeof(int) * left.size(), cudaMemcpyHostToDevice, s))
         return bail(fail(SVP_ECUDA, "svp_image_downsample: copies"));
     // scipy's gaussian_filter goes axis 0, 1, 2 (z, y, x)
-    SVP_LAUNCH(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(src, a, nz, ny, nx, 0, kdev + offs[0], radius[0]));
-    SVP_LAUNCH(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(a, b, nz, ny, nx, 1, kdev + offs[1], radius[1]));
-    SVP_LAUNCH(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(b, a, nz, ny, nx, 2, kdev + offs[2], radius[2]));
-    SVP_LAUNCH(resample_kernel<<<grid_for((long long)mz * my * mx), PT, 0, s>>>(a, nz, ny, nx, 1, dst, mz, my, mx, ldev,
-                                                                     wdev, ldev + mz, wdev + mz, ldev + mz + my,
-                                                                     wdev + mz + my));
-    SVP_LAUNCH_CHECK("svp_image_downsample");
+    SVP_LAUNCH_KEEP(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(src, a, nz, ny, nx, 0, kdev + offs[0], radius[0]));
+    SVP_LAUNCH_KEEP(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(a, b, nz, ny, nx, 1, kdev + offs[1], radius[1]));
+    SVP_LAUNCH_KEEP(image_gauss_kernel<<<grid_for(n), PT, 0, s>>>(b, a, nz, ny, nx, 2, kdev + offs[2], radius[2]));
+    SVP_LAUNCH_KEEP(resample_kernel<<<grid_for((long long)mz * my * mx), PT, 0, s>>>(a, nz, ny, nx, 1, dst, mz, my, mx,
+                                                                          ldev, wdev, ldev + mz, wdev + mz,
+                                                                          ldev + mz + my, wdev + mz + my));
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return bail(cuda_fail(le, "svp_image_downsample"));
     return bail(SVP_OK);
 }
 

@@ -51,6 +51,14 @@ class KernelTimer {
         if (_e != cudaSuccess) return svp::cuda_fail(_e, #__VA_ARGS__);                      \
     } while (0)
 
+// SVP_LAUNCH without the early return, for launches between a scratch allocation and its release: the caller reads
+// cudaGetLastError() after releasing the scratch, so no error path leaks it.
+#define SVP_LAUNCH_KEEP(...)                                                                 \
+    do {                                                                                     \
+        __VA_ARGS__;                                                                         \
+        svp::count_launch();                                                                 \
+    } while (0)
+
 #define SVP_REQUIRE(cond, msg)                                                               \
     do {                                                                                     \
         if (!(cond)) return svp::fail(SVP_EINVAL, msg);                                      \

@@ -243,8 +243,8 @@ extern "C" int svp_dot_dev(const double *a, const double *b, int64_t n, double *
     unsigned nb = blocks_for(n, 256, 4);
     dd *part = nullptr;
     SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * nb, s));
-    SVP_LAUNCH(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
-    SVP_LAUNCH(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, out_dev));
+    SVP_LAUNCH_KEEP(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
+    SVP_LAUNCH_KEEP(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, out_dev));
     cudaError_t le = cudaGetLastError();
     cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "dot kernels");
@@ -259,8 +259,8 @@ extern "C" int svp_bb2_dots_dev(const double *theta, const double *theta_old, co
     unsigned nb = blocks_for(n, 256, 4);
     dd *part = nullptr;
     SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * 4 * nb, s));
-    SVP_LAUNCH(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
-    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, out4_dev));
+    SVP_LAUNCH_KEEP(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
+    SVP_LAUNCH_KEEP(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, out4_dev));
     cudaError_t le = cudaGetLastError();
     cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "bb2 kernels");
@@ -279,10 +279,10 @@ extern "C" int svp_step_dots_dev(const double *g, const double *pvec, const doub
     dd *part = nullptr;
     SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * K * nb, s));
     if (bb2)
-        SVP_LAUNCH(step_dots_kernel<6><<<nb, 256, 0, s>>>(g, pvec, theta, theta_old, g_old, p_old, n, part));
+        SVP_LAUNCH_KEEP(step_dots_kernel<6><<<nb, 256, 0, s>>>(g, pvec, theta, theta_old, g_old, p_old, n, part));
     else
-        SVP_LAUNCH(step_dots_kernel<2><<<nb, 256, 0, s>>>(g, pvec, nullptr, nullptr, nullptr, nullptr, n, part));
-    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, K, out_dev));
+        SVP_LAUNCH_KEEP(step_dots_kernel<2><<<nb, 256, 0, s>>>(g, pvec, nullptr, nullptr, nullptr, nullptr, n, part));
+    SVP_LAUNCH_KEEP(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, K, out_dev));
     cudaError_t le = cudaGetLastError();
     cudaError_t fe = scratch_free(part, s);
     if (le != cudaSuccess) return cuda_fail(le, "step dots kernels");
@@ -334,8 +334,8 @@ extern "C" int svp_bb2_dots(const double *theta, const double *theta_old, const 
     dd *part = nullptr;
     SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * 4 * nb + 4 * sizeof(double), s));
     double *res = (double *)(part + 4 * nb);
-    SVP_LAUNCH(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
-    SVP_LAUNCH(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res));
+    SVP_LAUNCH_KEEP(bb2_kernel<<<nb, 256, 0, s>>>(theta, theta_old, g, g_old, p_old, pvec, n, part));
+    SVP_LAUNCH_KEEP(multi_final_kernel<<<1, 256, 0, s>>>(part, nb, 4, res));
     cudaError_t le = cudaGetLastError();
     double host[4];
     cudaError_t ce = cudaMemcpyAsync(host, res, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -354,7 +354,7 @@ extern "C" int svp_max_abs_diff(const double *a, const double *b, int64_t n, dou
     long long *keys = nullptr;
     SVP_CUDA(scratch_alloc((void **)&keys, 2 * sizeof(long long), s));
     cudaError_t e0 = cudaMemsetAsync(keys, 0, 2 * sizeof(long long), s);
-    SVP_LAUNCH(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
+    SVP_LAUNCH_KEEP(max_abs_diff_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(a, b, n, keys));
     cudaError_t le = cudaGetLastError();
     long long host[2] = {0, 0};
     cudaError_t ce = cudaMemcpyAsync(host, keys, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -375,8 +375,8 @@ extern "C" int svp_dot(const double *a, const double *b, int64_t n, double *out,
     dd *part = nullptr;
     SVP_CUDA(scratch_alloc((void **)&part, sizeof(dd) * nb + sizeof(double), s));
     double *res = (double *)(part + nb);
-    SVP_LAUNCH(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
-    SVP_LAUNCH(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res));
+    SVP_LAUNCH_KEEP(dot_kernel<<<nb, 256, 0, s>>>(a, b, n, part));
+    SVP_LAUNCH_KEEP(dot_final_kernel<<<1, 256, 0, s>>>(part, nb, res));
     cudaError_t le = cudaGetLastError();
     double host = 0.;
     cudaError_t ce = cudaMemcpyAsync(&host, res, sizeof host, cudaMemcpyDeviceToHost, s);
@@ -419,7 +419,7 @@ extern "C" int svp_step_bound(const svp_grid *g, const double *u, const double *
     SVP_CUDA(scratch_alloc((void **)&best, sizeof(long long), s));
     long long init = kKeyPosInf, host = 0;
     cudaError_t e1 = cudaMemcpyAsync(best, &init, sizeof init, cudaMemcpyHostToDevice, s);
-    SVP_LAUNCH(step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
+    SVP_LAUNCH_KEEP(step_bound_kernel<<<blocks_for(n_free(g), 256, 8), 256, 0, s>>>(g->nx, g->ny, g->nz, g->hx, g->hy, g->hz, g->x0,
                                                                     g->y0, g->z0, u, pvec, best));
     cudaError_t le = cudaGetLastError();
     cudaError_t e2 = cudaMemcpyAsync(&host, best, sizeof host, cudaMemcpyDeviceToHost, s);

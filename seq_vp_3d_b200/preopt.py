@@ -204,8 +204,9 @@ def boundary_taper(u, grid, L=4):
 def transfer(seed, grid, certificate_config=None):
     """multiresolution.py:111 prepare_transfer_problem: the first scale alpha in 0.9^k (k = 0..6) whose
     alpha * seed the whole-cell certificate proves (J > 0 on every closed cell).  Returns (field or None, report)."""
-    config = cert_mod.CertificateConfig(delta=0., prescreen=False) if certificate_config is None else certificate_config
-    if config.delta != 0.:
+    # the reference's transfer default (multiresolution.py:127): the edge-hull execution with strict J > 0
+    config = cert_mod.EnclosureCertificateConfig(delta=0.) if certificate_config is None else certificate_config
+    if not isinstance(config, cert_mod.EnclosureCertificateConfig) or config.delta != 0.:
         raise InputValidationError("transfer recovery requires whole-cell strict JD>0 certification")
     certifier = cert_mod.certifier(grid, config)
     attempts = []

@@ -125,7 +125,7 @@ class Registration:
     def __init__(self, grid, fixed, moving, *, lam, mu, nu, kappa, activation=.05, u_ref=None,
                  certificate_config=None, precision="plain"):
         self.grid = grid
-        self.config = cert_mod.CertificateConfig(delta=0.) if certificate_config is None else certificate_config
+        self.config = cert_mod.NATIVE_CERTIFICATE if certificate_config is None else certificate_config
         self.delta = self.config.delta
         self.weights = dict(lam=lam, mu=mu, nu=nu, kappa=kappa)
         self.activation = activation

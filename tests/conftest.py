@@ -52,3 +52,18 @@ def all_vertices(u):
     cx, cy = nx - 1, ny - 1
     x0, y0, z0 = c % cx, (c // cx) % cy, c // (cx * cy)
     return np.stack([u[z0 + (a >> 2), y0 + ((a >> 1) & 1), x0 + (a & 1)] for a in range(8)], axis=1)
+
+
+@pytest.fixture(scope="session")
+def configs_golden():
+    return np.load(os.path.join(GOLDEN, "certificate_configs.npz"))
+
+
+# (hull, prescreen, depth_first, max_depth, tile_size) of each certificate config class at its own defaults
+CONFIG_EXECUTIONS = {
+    "CertificateConfig": (False, False, True, 12, 8192),
+    "AdaptiveCertificateConfig": (False, False, False, 48, 8192),
+    "EnclosureCertificateConfig": (True, False, False, 48, 8192),
+    "CompiledFallbackCertificateConfig": (True, False, False, 48, 8192),
+    "PrescreenCertificateConfig": (True, True, False, 48, 8192),
+}

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of the certified-registration hot path by running the reference CPU code.
 
 This script is the only place that imports the reference (Zhaobh0620/seq_vp_3d, package ``jd_curl``).  It runs in a
-container where the reference tree is mounted (default ``/root/reference``; override with ``--reference``), writes
+container where the reference tree is mounted (its path is the required ``--reference`` argument), writes
 small ``.npz`` files beside itself and records the library versions used.  Nothing at test or bench time reads the
 reference: the fixtures are the frozen evidence.
 
@@ -18,7 +18,12 @@ q1.npz            spline coefficients/samples, energy terms, gradients, GGN diag
                   stable energy reductions of a small problem (residuals.py, linearization.py, poisson.py,
                   energy_comparison.py).
 
-Run:  python tests/golden/make_golden.py [--reference PATH] [--only certificate,cells,q1,seq,t73,preopt]
+certificate_configs.npz  certify_map records of each certificate config class (bare, Adaptive, Enclosure,
+                  CompiledFallback, Prescreen; the reference's defaults) and depth-first subdivision verdicts.
+seq_config1.npz   the reference's solve_sequential on the 32^3 blob pair (seed 0) with the native T73 metric, 40
+                  outer steps of 5 PG steps (the reference CPU route of the 32^3 float64 workload).
+
+Run:  python tests/golden/make_golden.py --reference PATH [--only certificate,cells,q1,seq,t73,preopt,configs,config1]
 """
 import argparse
 import os
@@ -259,6 +264,59 @@ def make_certificate(out):
     print("certificate.npz:", len(names), "fields")
 
 
+def make_configs(out):
+    """certify_map records of the reference's certificate config family (bare, Adaptive, Enclosure, CompiledFallback,
+    Prescreen, each with its own defaults) on every certificate field, plus the bare config's depth-first _classify
+    verdicts on the standalone cells of cells.npz."""
+    from jd_curl.three_d.grid import make_grid_3d
+    from jd_curl.three_d import feasibility as F
+    from jd_curl.three_d.compiled_fallback import fallback_arrays
+    data = {}
+    classes = ("CertificateConfig", "AdaptiveCertificateConfig", "EnclosureCertificateConfig",
+               "CompiledFallbackCertificateConfig", "PrescreenCertificateConfig")
+    names = []
+    for name, kw, u in certificate_fields():
+        g = make_grid_3d(**kw, unit="mm")
+        names.append(name)
+        for cls in classes:
+            for delta in (0.0, 0.01):
+                cfg = getattr(F, cls)(delta=delta)
+                res = F.certify_map(u, g, config=cfg)
+                ints, flts = record_array(res)
+                tag = f"{name}/{cls}/d{delta}"
+                data[f"{tag}/record_i"] = ints
+                data[f"{tag}/record_f"] = flts
+                data[f"{tag}/version"] = np.array(res.certificate_version)
+    data["names"] = np.array(names)
+    data["classes"] = np.array(classes)
+    cells = np.load(os.path.join(out, "cells.npz"))
+    verts, h = cells["vertices"], cells["spacing"]
+    for delta in (0.0, 0.01):
+        for depth, boxes in ((12, 255), (6, 40)):
+            cfg = F.CertificateConfig(delta=delta, max_depth=depth, max_boxes=boxes)
+            n = len(verts)
+            cls_i = np.full((n, 5), -1, np.int64)
+            cls_f = np.full((n, 4), np.nan)
+            for c in range(n):
+                res = fallback_arrays(verts[c:c + 1], h, delta, np.geterr())
+                if res is None:
+                    continue
+                p, coeff, samples = res
+                r = F._classify(coeff[0], p[0], delta, float(samples[0].min()), cfg)
+                cls_i[c] = (STATUS[r.status], REASONS.index(r.reason), r.n_boxes, r.max_depth,
+                            r.min_margin_lower_bound is not None)
+                cls_f[c, 0] = np.nan if r.min_margin_lower_bound is None else r.min_margin_lower_bound
+                if r.witness_reference_point is not None:
+                    cls_f[c, 1:] = r.witness_reference_point
+            tag = f"dfs/d{delta}/m{depth}_{boxes}"
+            data[f"{tag}/classify_i"] = cls_i
+            data[f"{tag}/classify_f"] = cls_f
+            hist = np.bincount(cls_i[:, 1][cls_i[:, 1] >= 0], minlength=len(REASONS))
+            print(tag, {REASONS[i]: int(c) for i, c in enumerate(hist) if c})
+    np.savez_compressed(os.path.join(out, "certificate_configs.npz"), **data, versions=np.array(repr(versions())))
+    print("certificate_configs.npz:", len(names), "fields x", len(classes), "config classes")
+
+
 def make_cells(out):
     """Standalone cells with tiny/negative interior JD, exercising every subdivision outcome."""
     from jd_curl.three_d.feasibility import PrescreenCertificateConfig, _classify
@@ -333,7 +391,7 @@ def make_cells(out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference tree (the directory holding jd_curl)")
     ap.add_argument("--only", default="certificate,cells,q1,seq,t73,preopt")
     args = ap.parse_args()
     import_reference(args.reference)
@@ -354,6 +412,12 @@ def main():
     if "preopt" in only:
         from preopt_golden import make_preopt   # the float32 pyramid pre-optimizer and its pieces
         make_preopt(HERE)
+    if "configs" in only:
+        make_configs(HERE)
+    if "config1" in only:
+        from q1_golden import make_seq     # the 32^3 blob pair, native T73 metric, 40 outer steps
+        make_seq(HERE, policy="image_shift_ggn_equilibrated_jd_affine_v3", name="seq_config1.npz", seed=0,
+                 outer_steps=40, shape=(32, 32, 32))
 
 
 if __name__ == "__main__":

@@ -114,7 +114,7 @@ def test_certify_map_records(svp, cert_golden):
         u, grid = g[f"{name}/u"], grid_of(g, name)
         for d in (0.0, 0.01):
             for tile in (64, 65536):
-                cfg = svp.CertificateConfig(delta=d, max_depth=48, max_boxes=255, tile_size=tile)
+                cfg = svp.PrescreenCertificateConfig(delta=d, max_depth=48, max_boxes=255, tile_size=tile)
                 ri, rf = record_of(svp.certify_map(u, grid, config=cfg))
                 if ri[0] == 0 or ri[2] == 0:      # early returns report n_uncertain = n_cells as the reference does
                     pass
@@ -145,7 +145,7 @@ def test_certify_map_matches_oracle_larger(svp, amp, seed):
     u = seeded_field(shape, h, amp, seed)
     for d in (0.0, 0.01):
         for tile in (4096, 65536):
-            cfg = svp.CertificateConfig(delta=d, tile_size=tile)
+            cfg = svp.PrescreenCertificateConfig(delta=d, max_depth=48, tile_size=tile)
             ri, rf = record_of(svp.certify_map(u, grid, config=cfg))
             oi, of = oc.certify_map(u, h, d, tile_size=tile)
             assert np.array_equal(ri, oi), (amp, d, tile, ri, oi)
@@ -166,3 +166,44 @@ def test_margins_full_size_tile_rule(svp):
     om, of_ = oc.edge_hull(u, h, 0.0, threads=8)
     assert np.array_equal(f, of_) and f.sum() == 8
     assert same_bits(m[~f], om[~f])
+
+
+def test_config_family_records(svp, cert_golden, configs_golden):
+    """certify_map under each certificate config class at the reference's own defaults: the bare class (whole-cell
+    Bernstein, depth-first subdivision), Adaptive (lowest bound first), Enclosure, CompiledFallback and Prescreen;
+    every record field and the certificate version equal the reference's."""
+    from conftest import CONFIG_EXECUTIONS
+    from seq_vp_3d_b200.grid import make_grid_3d
+    from test_oracle_certificate import expected_record
+    c = configs_golden
+    for name in names(c):
+        u = cert_golden[f"{name}/u"]
+        grid = grid_of(cert_golden, name)
+        for cls in c["classes"]:
+            hull, pre, _, _, _ = CONFIG_EXECUTIONS[str(cls)]
+            for d in (0.0, 0.01):
+                tag = f"{name}/{cls}/d{d}"
+                res = svp.certify_map(u, grid, config=getattr(svp, str(cls))(delta=d))
+                ri, rf = record_of(res)
+                assert np.array_equal(ri, expected_record(c[f"{tag}/record_i"], hull, pre)), (tag, ri)
+                assert same_bits_nan(rf, c[f"{tag}/record_f"]), (tag, rf)
+                assert res.certificate_version == str(c[f"{tag}/version"]), tag
+
+
+def test_depth_first_classify(svp, cells_golden, configs_golden):
+    """The bare CertificateConfig's depth-first subdivision (svp_classify_cells_policy) on the standalone cells."""
+    verts, h = cells_golden["vertices"], cells_golden["spacing"]
+    for d in (0.0, 0.01):
+        ok, plo, phi, clo, chi, _ = (t.cpu().numpy() for t in svp.fallback_arrays_device(verts, h, d))
+        sel = np.flatnonzero(ok)
+        for depth, boxes in ((12, 255), (6, 40)):
+            tag = f"dfs/d{d}/m{depth}_{boxes}"
+            ci, cf = configs_golden[f"{tag}/classify_i"], configs_golden[f"{tag}/classify_f"]
+            got = svp.classify_cells(clo[sel], chi[sel], plo[sel], phi[sel], d, depth, boxes, depth_first=True)
+            for k, r in zip(sel, got):
+                assert (r["status"], r["reason"], r["boxes"], r["depth"], r["margin"] is not None) == tuple(ci[k]), \
+                    (tag, k)
+                if r["margin"] is not None:
+                    assert same_bits(r["margin"], cf[k, 0])
+                if r["witness"] is not None:
+                    assert same_bits(r["witness"], cf[k, 1:])

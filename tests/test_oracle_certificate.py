@@ -92,3 +92,51 @@ def test_oracle_standalone_cells(cells_golden, delta, budget):
             assert same_bits(r["margin"], g[f"{tag}/classify_f"][k, 0])
         if r["witness"] is not None:
             assert same_bits(r["witness"], g[f"{tag}/classify_f"][k, 1:])
+
+
+def expected_record(ints, hull, prescreen):
+    """The reference's plain FeasibilityResult (bare and Adaptive configs) has no stage counts and its
+    EnclosureFeasibilityResult no prescreen count; the golden writes -1 there, the record structure here 0."""
+    ints = np.array(ints)
+    absent = slice(8, 11) if not hull else slice(10, 11) if not prescreen else slice(0, 0)
+    assert np.all(ints[absent] == -1)
+    ints[absent] = 0
+    return ints
+
+
+def test_oracle_config_family_records(cert_golden, configs_golden):
+    """The C oracle reproduces certify_map's record for every config class of the reference (bare: whole-cell
+    Bernstein with depth-first subdivision; Adaptive: lowest bound first; the Enclosure family with the hull)."""
+    from conftest import CONFIG_EXECUTIONS
+    g, c = cert_golden, configs_golden
+    for name in _names(c):
+        u, h = g[f"{name}/u"], g[f"{name}/spacing"]
+        for cls in c["classes"]:
+            hull, pre, dfs, depth, tile = CONFIG_EXECUTIONS[str(cls)]
+            for d in (0.0, 0.01):
+                tag = f"{name}/{cls}/d{d}"
+                ri, rf = cert.certify_map(u, h, d, max_depth=depth, tile_size=tile, hull=hull, prescreen=pre,
+                                          depth_first=dfs)
+                assert np.array_equal(ri, expected_record(c[f"{tag}/record_i"], hull, pre)), (tag, ri)
+                assert same_bits_nan(rf, c[f"{tag}/record_f"]), (tag, rf)
+
+
+def test_oracle_depth_first_classify(cells_golden, configs_golden):
+    """Depth-first subdivision verdicts of the bare CertificateConfig on the standalone cells."""
+    verts, h = cells_golden["vertices"], cells_golden["spacing"]
+    for d in (0.0, 0.01):
+        for depth, boxes in ((12, 255), (6, 40)):
+            tag = f"dfs/d{d}/m{depth}_{boxes}"
+            ci, cf = configs_golden[f"{tag}/classify_i"], configs_golden[f"{tag}/classify_f"]
+            for k, v in enumerate(verts):
+                res = cert.fallback_cell(v, h, d)
+                if not res[0]:
+                    assert ci[k, 0] < 0
+                    continue
+                r = cert.classify(res[3], res[4], res[1], res[2], d, depth, boxes, depth_first=True)
+                assert (r["status"], r["reason"], r["boxes"], r["depth"], r["margin"] is not None) == tuple(ci[k]), \
+                    (tag, k)
+                if r["margin"] is not None:
+                    assert same_bits(r["margin"], cf[k, 0])
+                if r["witness"] is not None:
+                    assert same_bits(r["witness"], cf[k, 1:])
