@@ -173,6 +173,10 @@ int svp_pair_create(const svp_grid *g, const svp_weights *w, const double *fixed
 /* New proximal reference (problem.py:381 with_controls / :397 make_self_reference), copied from u_ref. */
 int svp_pair_set_reference(svp_pair *p, const double *u_ref, void *stream);
 int svp_pair_destroy(svp_pair *p);
+/* Replace the pair's spline coefficients (nz, ny, nx) by coeff (device): for a host that already holds the moving
+ * image's not-a-knot coefficients on the pair's own knots (the reference's ImageSampler3D, interpolation.py:29-40,
+ * whose NdBSpline keeps the coefficients and not the image). */
+int svp_pair_set_spline_coefficients(svp_pair *p, const double *coeff, void *stream);
 /* Copy of the spline coefficients (nz, ny, nx) into out (device). */
 int svp_pair_spline_coefficients(const svp_pair *p, double *out, void *stream);
 

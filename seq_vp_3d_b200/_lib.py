@@ -73,6 +73,7 @@ SIGNATURES = {
     "svp_pair_set_reference": [P, P, P],
     "svp_pair_destroy": [P],
     "svp_pair_spline_coefficients": [P, P, P],
+    "svp_pair_set_spline_coefficients": [P, P, P],
     "svp_warp": [P, P, P, P, P],
     "svp_sample_points": [P, P, I64, P, P, P],
     "svp_energy": [P, P, P, P, P, P],

@@ -288,6 +288,13 @@ extern "C" int svp_pair_set_reference(svp_pair *p, const double *u_ref, void *st
     return SVP_OK;
 }
 
+extern "C" int svp_pair_set_spline_coefficients(svp_pair *p, const double *coeff, void *stream) {
+    SVP_REQUIRE(p && coeff, "svp_pair_set_spline_coefficients: null argument");
+    SVP_CUDA(cudaMemcpyAsync(p->coeff, coeff, sizeof(double) * p->q.nnode, cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream));
+    return SVP_OK;
+}
+
 extern "C" int svp_pair_spline_coefficients(const svp_pair *p, double *out, void *stream) {
     SVP_REQUIRE(p && out, "svp_pair_spline_coefficients: null argument");
     SVP_CUDA(cudaMemcpyAsync(out, p->coeff, sizeof(double) * p->q.nnode, cudaMemcpyDeviceToDevice,

@@ -62,6 +62,13 @@ class DevicePair:
         r = to_device(u_ref)
         _lib.call("svp_pair_set_reference", self._h, ptr(r), stream_ptr(stream))
 
+    def set_spline_coefficients(self, coefficients, stream=None):
+        """Use given not-a-knot coefficients (nz, ny, nx) of the moving image on this grid's knots."""
+        c = to_device(coefficients)
+        if tuple(c.shape) != self.grid.shape:
+            raise ValueError("spline coefficients: (nz, ny, nx) required")
+        _lib.call("svp_pair_set_spline_coefficients", self._h, ptr(c), stream_ptr(stream))
+
     def spline_coefficients(self, stream=None):
         out = self.node()
         _lib.call("svp_pair_spline_coefficients", self._h, ptr(out), stream_ptr(stream))

@@ -67,3 +67,18 @@ CONFIG_EXECUTIONS = {
     "CompiledFallbackCertificateConfig": (True, False, False, 48, 8192),
     "PrescreenCertificateConfig": (True, True, False, 48, 8192),
 }
+
+
+def installed_reference():
+    """The reference package (jd_curl) installed under baseline/_ref, or None.  Only the backend= adapter's GPU test
+    uses it: the reference's own solve_sequential then drives this library through the adapter.  The package needs
+    nibabel only for NIfTI I/O, so a stub module stands in for it."""
+    import types
+    path = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(path, "jd_curl")):
+        return None
+    sys.modules.setdefault("nibabel", types.ModuleType("nibabel"))
+    if path not in sys.path:
+        sys.path.append(path)
+    import jd_curl
+    return jd_curl

@@ -20,10 +20,12 @@ q1.npz            spline coefficients/samples, energy terms, gradients, GGN diag
 
 certificate_configs.npz  certify_map records of each certificate config class (bare, Adaptive, Enclosure,
                   CompiledFallback, Prescreen; the reference's defaults) and depth-first subdivision verdicts.
+backend_signatures.json  parameter lists of the reference plug-in methods (backends/accelerated.py,
+                  backends/hybrid.py) that the backend= adapter provides.
 seq_config1.npz   the reference's solve_sequential on the 32^3 blob pair (seed 0) with the native T73 metric, 40
                   outer steps of 5 PG steps (the reference CPU route of the 32^3 float64 workload).
 
-Run:  python tests/golden/make_golden.py --reference PATH [--only certificate,cells,q1,seq,t73,preopt,configs,config1]
+Run:  python tests/golden/make_golden.py --reference PATH [--only certificate,cells,q1,seq,t73,preopt,configs,signatures,config1]
 """
 import argparse
 import os
@@ -317,6 +319,40 @@ def make_configs(out):
     print("certificate_configs.npz:", len(names), "fields x", len(classes), "config classes")
 
 
+# the adapter methods of seq_vp_3d_b200.backend.B200Backend and the reference plug-in class each one mirrors
+BACKEND_METHODS = {
+    "evaluate_trial": "AcceleratedHybridBackend", "promote_trial": "AcceleratedHybridBackend",
+    "gradient": "AcceleratedHybridBackend", "poisson": "AcceleratedHybridBackend",
+    "diagonal": "HybridBackend", "diagonal_launch": "AcceleratedHybridBackend",
+    "node_min_jd": "HybridBackend", "global_jd_root": "HybridBackend", "linearize": "AcceleratedHybridBackend",
+    "stable_energy_reduction": "AcceleratedHybridBackend", "stable_energy_reductions": "AcceleratedHybridBackend",
+    "outer_gradient_vectors": "AcceleratedHybridBackend", "outer_norms": "AcceleratedHybridBackend",
+    "cpu_state": "AcceleratedHybridBackend",
+}
+POISSON_METHODS = ("apply", "prepare_equilibrated", "apply_equilibrated")
+
+
+def make_signatures(out):
+    """backend_signatures.json: the parameter lists (name, kind, default) of the reference plug-in's methods that
+    the B200 backend adapter provides, read with inspect from the reference classes."""
+    import inspect
+    import json
+    from jd_curl.three_d.backends import accelerated, hybrid
+
+    def params(fn):
+        fn = inspect.unwrap(fn)
+        return [[p.name, str(p.kind), None if p.default is inspect.Parameter.empty else repr(p.default)]
+                for p in inspect.signature(fn).parameters.values()]
+
+    classes = dict(AcceleratedHybridBackend=accelerated.AcceleratedHybridBackend, HybridBackend=hybrid.HybridBackend)
+    data = dict(backend={name: params(getattr(classes[cls], name)) for name, cls in BACKEND_METHODS.items()},
+                poisson={name: params(getattr(hybrid._HostPoisson, name)) for name in POISSON_METHODS},
+                source={name: cls for name, cls in BACKEND_METHODS.items()})
+    with open(os.path.join(out, "backend_signatures.json"), "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    print("backend_signatures.json:", len(data["backend"]), "backend methods,", len(data["poisson"]), "Poisson methods")
+
+
 def make_cells(out):
     """Standalone cells with tiny/negative interior JD, exercising every subdivision outcome."""
     from jd_curl.three_d.feasibility import PrescreenCertificateConfig, _classify
@@ -412,6 +448,8 @@ def main():
     if "preopt" in only:
         from preopt_golden import make_preopt   # the float32 pyramid pre-optimizer and its pieces
         make_preopt(HERE)
+    if "signatures" in only:
+        make_signatures(HERE)
     if "configs" in only:
         make_configs(HERE)
     if "config1" in only:

@@ -18,10 +18,13 @@ pytestmark = pytest.mark.gpu
 # (fixture, metric policy, outer steps): the T62 metric from u = 0, and the native T73 metric from a certified start
 # with a strong local compression
 CASES = [("seq.npz", "image_shift_ggn_equilibrated_jd_affine_v1", 6),
-         ("seq_t73.npz", "image_shift_ggn_equilibrated_jd_affine_v3", 8)]
+         ("seq_t73.npz", "image_shift_ggn_equilibrated_jd_affine_v3", 8),
+         # the 32^3 blob pair (seed 0) with the native T73 metric and 40 outer steps: the reference's CPU route of
+         # the 32^3 float64 workload
+         ("seq_config1.npz", "image_shift_ggn_equilibrated_jd_affine_v3", 40)]
 
 
-@pytest.fixture(scope="module", params=CASES, ids=["t62", "t73"])
+@pytest.fixture(scope="module", params=CASES, ids=["t62", "t73", "blob32_40outer"])
 def run(request):
     from seq_vp_3d_b200.grid import make_grid_3d
     from seq_vp_3d_b200.solver import PGConfig3D, Registration, SequentialConfig3D, solve_sequential
