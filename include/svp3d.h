@@ -109,7 +109,7 @@ int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, const int64_t
                                void *stream);
 
 /* Interval J - delta at the closed27 points, its interval Bernstein coefficients and float64 samples of standalone
- * cells.  Replaces compiled_fallback.py:330 fallback_arrays (per cell: ok[i] = 0 where the reference returns None).
+ * cells.  Replaces compiled_fallback.py:177 fallback_arrays (per cell: ok[i] = 0 where the reference returns None).
  * vertices: (n, 8, 3) displacements; spacing3: host (3,) hx, hy, hz; the five outputs are (n, 27) float64 in
  * storage order 9 iz + 3 iy + ix; ok: (n,) uint8. */
 int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta, double *p_lo,
@@ -199,12 +199,12 @@ int svp_sample_points(const svp_pair *p, const double *points, int64_t n, double
                       void *stream);
 
 /* Energy terms (image, proximity, jd, curl, barrier) of u with its warped image, summed in double-double.
- * Replaces residuals.py:302 _energy and backends/accelerated.py:1574 _energy.  terms5: host; barrier_violations:
+ * Replaces residuals.py:189 _energy and backends/accelerated.py:1574 _energy.  terms5: host; barrier_violations:
  * host count of closed27 points with J <= delta (the reference raises there).  Synchronizes. */
 int svp_energy(svp_pair *p, const double *u, const double *warped, double *terms5, int64_t *barrier_violations,
                void *stream);
 /* Stable differences trial - base of E and of F = image + barrier, cancellation-free per residual and per
- * barrier point (energy_comparison.py:223 _differences; backends/accelerated.py:3062 _compare).  diff2 host. */
+ * barrier point (energy_comparison.py:92 _differences; backends/accelerated.py:3062 _compare).  diff2 host. */
 int svp_energy_difference(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
                           const double *trial_warped, double *diff2, void *stream);
 

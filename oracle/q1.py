@@ -2,14 +2,14 @@
 
 Covers (reference paths inside jd_curl/three_d/):
   cell_q1.py:101     CellQ1Operators3D tables (gauss27 / closed27_uniform points, weights, derivative tables)
-  geometry.py:254    _compute_cell_geometry (F = I + grad u, cofactor rows, J, curl)
-  barrier.py:290     barrier_terms, localized C2 branch
+  geometry.py:60     _compute_cell_geometry (F = I + grad u, cofactor rows, J, curl)
+  barrier.py:7-36    barrier_terms, localized C2 branch
   interpolation.py:29 build_image_sampler: not-a-knot tensor cubic spline (SciPy make_interp_spline per axis);
                      restated here as the collocation solve on the not-a-knot knot vector
   backends/spline.py:12 cubic_basis (Cox-de Boor basis and derivative on the knot span)
-  residuals.py:302   _energy (longdouble sums), linearization.py:180 energy_gradient, :217 outer_gradient_vectors,
+  residuals.py:189   _energy (longdouble sums), linearization.py:180 energy_gradient, :217 outer_gradient_vectors,
                      :327 barrier_ggn_hvp, :357 barrier_ggn_diagonal
-  energy_comparison.py:145 _barrier_difference, :196 _squared_change, :223 _differences
+  energy_comparison.py:14 _barrier_difference, :65 _squared_change, :92 _differences
   poisson.py:16      poisson_spectrum, :99 PoissonInverse3D.apply (DST-I, orthonormal) -- restated by the DST-I
                      definition as a dense sine matrix per axis
   solvers/poisson_gradient.py:269 image_curvature_shift, :281 metric_diagonal
@@ -132,7 +132,7 @@ def cofactor(F):
 
 def grad_points(loc, op):
     """V[n, p, r, j] = sum_a loc[n, a, r] D[j, p, a]: per component/axis (cells, 8) @ (8, P) products, as
-    geometry.py:268-272 forms them."""
+    geometry.py:11-32 forms them."""
     n, P = loc.shape[0], op.D.shape[1]
     V = np.empty((n, P, 3, 3))
     for r in range(3):
@@ -153,7 +153,7 @@ def geometry(loc, op):
 
 
 def barrier_terms(J, delta, weight, activation):
-    """Localized C2 barrier b = -w r^2 log t, first and second derivative (barrier.py:301-319)."""
+    """Localized C2 barrier b = -w r^2 log t, first and second derivative (barrier.py:18-36)."""
     value, first, second = (np.zeros_like(J) for _ in range(3))
     active = J < activation
     scale = activation - delta
@@ -270,7 +270,7 @@ def warp(problem, u, with_gradient=False):
 
 
 def cell_terms(problem, u):
-    """(jd, curl, barrier) longdouble sums over all cells, tile by tile (residuals.py:279 _cell_energy)."""
+    """(jd, curl, barrier) longdouble sums over all cells, tile by tile (residuals.py:166 _cell_energy)."""
     g = problem.grid
     G, C = ops(g, "gauss27"), ops(g, "closed27_uniform")
     jd = cu = bar = np.longdouble(0)
@@ -288,7 +288,7 @@ def cell_terms(problem, u):
 
 
 def energy(problem, u, warped=None):
-    """(image, proximity, jd, curl, barrier) of residuals.py:302 _energy."""
+    """(image, proximity, jd, curl, barrier) of residuals.py:189 _energy."""
     if warped is None:
         warped, _ = warp(problem, u)
     q = problem.grid.node_weights()
@@ -299,7 +299,7 @@ def energy(problem, u, warped=None):
 
 
 def _scatter(grid, op, flux, out, cells=None):
-    """out (3, nz, ny, nx) += D^T flux (flux (n,P,3,3) [r, j]) (cell_q1.py:186 _transpose_add)."""
+    """out (3, nz, ny, nx) += D^T flux (flux (n,P,3,3) [r, j]) (cell_q1.py:116 _transpose_add)."""
     nodes = cell_nodes(grid, cells)
     size = out[0].size
     for r in range(3):
@@ -400,7 +400,7 @@ def ggn_hvp(problem, u, image_grad, p):
 
 # ----------------------------------------------------------------------------------------------- stable differences
 def barrier_difference(a, b, delta, activation):
-    """energy_comparison.py:145 localized branch, longdouble."""
+    """energy_comparison.py:14-62 localized branch, longdouble."""
     a, b, d = a.astype(np.longdouble), b.astype(np.longdouble), np.longdouble(delta)
     act = np.longdouble(activation)
     a, b = np.minimum(a, act), np.minimum(b, act)
@@ -424,7 +424,7 @@ def _sq(a, b):
 
 
 def differences(problem, base_u, base_w, trial_u, trial_w):
-    """(E difference, F difference) trial - base (energy_comparison.py:223 _differences)."""
+    """(E difference, F difference) trial - base (energy_comparison.py:92 _differences)."""
     g = problem.grid
     q = g.node_weights()
     img = lambda w: np.sqrt(q) * (w - problem.fixed)

@@ -316,7 +316,7 @@ class B200Backend:
     # ------------------------------------------------------------------ evaluation (accelerated.py:1667, :2851)
     def evaluate_trial(self, problem, theta, *, certificate_observer=None, witness_observer=None):
         """Certify, sample and evaluate theta: TrialState3D, or InvalidTrial with the reference's reasons
-        (residuals.py:322-349)."""
+        (residuals.py:209-236)."""
         J = _jd()
         started = perf_counter()
         theta = np.asarray(theta, dtype=np.float64)
@@ -353,7 +353,7 @@ class B200Backend:
         return state
 
     def promote_trial(self, problem, trial):
-        """AcceptedState3D with the physical image gradient at X + u (residuals.py:351)."""
+        """AcceptedState3D with the physical image gradient at X + u (residuals.py:238)."""
         J = _jd()
         J["R"].validate_state(problem, trial)
         started = perf_counter()

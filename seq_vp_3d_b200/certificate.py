@@ -4,7 +4,7 @@ Call surface kept from the reference:
   certify_map(u, grid, *, config)                       feasibility.py:393 (and certify_map_owned :558)
   parallel_margins(u, grid, delta)                      compiled_enclosure.py:303
   prescreen_lower_bounds(u, grid, coefficients, cells)  certificate_prescreen.py:125
-  fallback_arrays(vertices, spacing, delta, errors)     compiled_fallback.py:330
+  fallback_arrays(vertices, spacing, delta, errors)     compiled_fallback.py:177
 Every decision is made by libsvp3d's CUDA kernels, bit-identical to the reference CPU certifier (binary64 round to
 nearest plus one outward ulp per interval operation, no FMA).  Host numpy inputs are uploaded; CUDA tensors are used
 in place.  There is no CPU path.

@@ -793,7 +793,7 @@ __device__ __forceinline__ dd sq_change(double a, double b) {
     return {p.hi * .5, p.lo * .5};
 }
 
-// energy_comparison.py:145 localized branch (double precision), unweighted
+// energy_comparison.py:14-62 localized branch (double precision), unweighted
 __device__ __forceinline__ double barrier_difference(double ja, double jb, double act, double d) {
     double a = ja < act ? ja : act, b = jb < act ? jb : act;
     double scale = act - d;

@@ -240,7 +240,7 @@ __device__ __forceinline__ void grad_at(const T G[3][3][3][3], int ix, int iy, i
     }
 }
 
-// Cofactor rows (cross products of cyclic rows of F = I + V) and J = F0 . A0 (geometry.py:205, :274).
+// Cofactor rows (cross products of cyclic rows of F = I + V) and J = F0 . A0 (geometry.py:11 cofactor, :26 determinant).
 template <class T>
 __device__ __forceinline__ void cofactor_det(const T V[3][3], T A[3][3], T &J) {
     T F[3][3];
@@ -313,7 +313,7 @@ __device__ __forceinline__ void scatter_edges(const T S[3][3][3][3], const T n[3
 }
 
 // ------------------------------------------------------------------------------------------- localized barrier
-// barrier.py:301-319: b = -w r^2 log t, b' and b'' for J < a (zero above); log t via log1p(-r) when r < 1/2.
+// barrier.py:18-36: b = -w r^2 log t, b' and b'' for J < a (zero above); log t via log1p(-r) when r < 1/2.
 __device__ __forceinline__ void barrier_eval(double J, double a, double delta, double w, double &b, double &b1,
                                              double &b2) {
     b = b1 = b2 = 0.;

@@ -68,44 +68,52 @@ class Grid3D:
         return out
 
 
-def _size(n, name):
-    if isinstance(n, bool) or not isinstance(n, (int, np.integer)) or n < 5:
-        raise InputValidationError(f"{name}: expected an integer >= 5")
-    return int(n)
+def _count(value, name):
+    """A node count: a plain integer of at least 5 (the Q1 cell kernels need interior nodes on every axis)."""
+    ok = isinstance(value, (int, np.integer)) and not isinstance(value, bool) and value >= 5
+    if not ok:
+        raise InputValidationError(f"{name} must be an integer node count >= 5, got {value!r}")
+    return int(value)
 
 
-def _real(v, name, positive=False):
-    if isinstance(v, bool) or not isinstance(v, (int, float, np.floating, np.integer)):
-        raise InputValidationError(f"{name}: expected a real scalar")
-    v = float(v)
-    if not np.isfinite(v) or (positive and v <= 0):
-        raise InputValidationError(f"{name}: must be {'positive and ' if positive else ''}finite")
-    return v
+def _scalar(value, name, *, positive=False):
+    ok = isinstance(value, (int, float, np.integer, np.floating)) and not isinstance(value, bool)
+    value = float(value) if ok else float("nan")
+    if not (ok and np.isfinite(value) and (value > 0 or not positive)):
+        kind = "a positive finite" if positive else "a finite"
+        raise InputValidationError(f"{name} must be {kind} real number")
+    return value
+
+
+def _axis(count, step, start):
+    """Node coordinates start + step * k, k = 0 .. count - 1 (read-only), and the trapezoid weights of the axis."""
+    with np.errstate(all="ignore"):
+        coords = start + step * np.arange(count, dtype=np.float64)
+    if not (np.isfinite(coords).all() and (coords[1:] > coords[:-1]).all()):
+        raise InputValidationError("axis coordinates overflow or do not increase strictly")
+    weights = np.full(count, 1.0)
+    weights[0] = weights[-1] = 0.5
+    coords.flags.writeable = weights.flags.writeable = False
+    return coords, weights
 
 
 def make_grid_3d(*, nx, ny, nz, hx, hy, hz, x0=0., y0=0., z0=0., unit="unit"):
-    sizes = tuple(_size(n, name) for n, name in zip((nx, ny, nz), ("nx", "ny", "nz")))
-    spacing = tuple(_real(h, name, positive=True) for h, name in zip((hx, hy, hz), ("hx", "hy", "hz")))
-    origins = tuple(_real(o, name) for o, name in zip((x0, y0, z0), ("x0", "y0", "z0")))
-    if not isinstance(unit, str) or not unit.strip():
-        raise InputValidationError("unit: explicit nonempty length unit required")
-    axes, mass = [], []
-    with np.errstate(over="ignore", under="ignore", invalid="ignore"):
-        omega = float(np.prod(spacing))
-        for n, h, origin in zip(sizes, spacing, origins):
-            axis = origin + h * np.arange(n, dtype=np.float64)
-            if not np.all(np.isfinite(axis)) or not np.all(np.diff(axis) > 0):
-                raise InputValidationError("coordinates must be finite and strictly increasing")
-            axis.flags.writeable = False
-            axes.append(axis)
-            weights = np.ones(n)
-            weights[[0, -1]] = .5
-            weights.flags.writeable = False
-            mass.append(weights)
-    if not np.isfinite(omega) or omega / 8 <= 0:
-        raise InputValidationError("grid mass must be positive finite float64, including corners")
-    digest = hashlib.sha256(repr((sizes, spacing, origins, unit)).encode()).hexdigest()
-    return Grid3D(sizes[::-1], spacing, tuple(axes), tuple(mass), omega, unit, digest)
+    """Grid3D of nx x ny x nz nodes (keyword arguments as the reference's factory, grid.py:49).  The grid id is the
+    SHA-256 of repr((sizes, spacings, origins, unit)) with xyz-ordered tuples, the identity the reference assigns to
+    the same arguments, so states and certificates carry interchangeable grid ids."""
+    counts = tuple(_count(v, k) for k, v in (("nx", nx), ("ny", ny), ("nz", nz)))
+    steps = tuple(_scalar(v, k, positive=True) for k, v in (("hx", hx), ("hy", hy), ("hz", hz)))
+    starts = tuple(_scalar(v, k) for k, v in (("x0", x0), ("y0", y0), ("z0", z0)))
+    if not (isinstance(unit, str) and unit.strip()):
+        raise InputValidationError("unit must name the length unit (a nonempty string)")
+    axes, weights = zip(*(_axis(n, h, o) for n, h, o in zip(counts, steps, starts)))
+    with np.errstate(all="ignore"):
+        cell_volume = float(steps[0] * steps[1] * steps[2])
+    # the smallest node mass, a corner's omega / 8, must stay a positive finite double
+    if not (np.isfinite(cell_volume) and cell_volume * 0.125 > 0):
+        raise InputValidationError("cell volume hx * hy * hz (and its corner eighth) must be positive and finite")
+    grid_id = hashlib.sha256(repr((counts, steps, starts, unit)).encode()).hexdigest()
+    return Grid3D(counts[::-1], steps, tuple(axes), tuple(weights), cell_volume, unit, grid_id)
 
 
 def grid_from_shape(shape_zyx, spacing_xyz, unit="mm"):

@@ -143,7 +143,7 @@ class Registration:
             raise ValueError(f"u_ref: not certified feasible ({ref.reason})")
         self.reference_certificate = ref
 
-    # ------------------------------------------------------------------ evaluation (residuals.py:322, :351)
+    # ------------------------------------------------------------------ evaluation (residuals.py:209, :238)
     def certify(self, u):
         rec = self.certifier.run(u)
         return cert_mod.result_from_record(rec, self.grid, self.config, None)
@@ -212,7 +212,7 @@ class Registration:
         return state.norms
 
     def stable_reductions(self, base, trial):
-        """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:266)."""
+        """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:135)."""
         cached = trial.differences
         if cached is not None and cached[0] == (base.eval_id, self._reference_version):
             dE, dF = cached[1]

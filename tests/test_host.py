@@ -40,3 +40,25 @@ def test_bench_phase_split():
     assert abs(out["fp64_kernels_s"] - 5.) < 1e-12          # the pre-optimizer's kernels are not the loop's
     assert abs(out["loop_host_gap_s"] - 6.) < 1e-12
     assert bench.phase_summary([], timers, 1) is None
+
+
+def test_grid_ids_equal_the_reference():
+    """Grid ids are the reference's (grid.py:49 make_grid_3d) for the same arguments: the ids below were produced by
+    the reference's own factory, so certificates and states carry interchangeable grid ids."""
+    import pytest
+    from seq_vp_3d_b200.grid import InputValidationError, make_grid_3d
+    cases = [(dict(nx=9, ny=8, nz=7, hx=1.0, hy=1.25, hz=0.8, unit="mm"),
+              "620fe16f0e74b7f6179f254a2fc6cd63b404c299d6ab8b81ecbfca3b1ccc1f1d"),
+             (dict(nx=160, ny=192, nz=224, hx=1., hy=1., hz=1., unit="mm"),
+              "51c2d3c616b2f6ffbc725eedf59a1547299d87150f2970fb670369a24d85b675"),
+             (dict(nx=17, ny=13, nz=12, hx=.9, hy=1.1, hz=1.3, x0=-3.5, y0=2, z0=1e-3, unit="um"),
+              "c71764ed3546beb1bd2539b5da42ac304856beefc164a178ee07f16cdb77c3a7")]
+    for kw, gid in cases:
+        g = make_grid_3d(**kw)
+        assert g.grid_id == gid
+        assert g.shape == (kw["nz"], kw["ny"], kw["nx"]) and g.omega == kw["hx"] * kw["hy"] * kw["hz"]
+    for bad in (dict(nx=4), dict(hx=0.), dict(hx=float("inf")), dict(unit=" "), dict(nx=True)):
+        kw = dict(nx=9, ny=8, nz=7, hx=1., hy=1., hz=1., unit="mm")
+        kw.update(bad)
+        with pytest.raises(InputValidationError):
+            make_grid_3d(**kw)
