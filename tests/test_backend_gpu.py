@@ -40,7 +40,8 @@ def run(request):
                            u_ref=np.zeros(grid.shape + (3,)), weights=Weights3D(lam=lam, mu=mu, nu=nu, kappa=kappa),
                            certificate_config=config, barrier_location="closed27_uniform", barrier_activation=.05)
     backend = B200Backend()
-    res = solve_sequential(problem, np.array(d["theta0"]), solver="pg",
+    theta0 = np.array(d["theta0"]) if "theta0" in d.files else np.zeros(3 * grid.n_free_scalar)
+    res = solve_sequential(problem, theta0, solver="pg",
                            inner_config=ConservativePGConfig3D(max_iterations=5, metric_policy=policy,
                                                                resolution_exit=True),
                            config=SequentialReuseConfig3D(max_iterations=outer, eta0=.01), backend=backend)
