@@ -192,6 +192,7 @@ class B200Backend:
         self.timings = {}
         self.cpu_gradient_checks = 0
         self.comparison_counts = dict(gpu=0, cpu=0)
+        self.last_comparison = {}             # read by the reference loops for their attempt rows
         self._max_states = int(max_states)
         self._states = OrderedDict()          # eval_id -> device fields of an evaluated state
         self._pairs = {}                      # (grid id, image ids, weights, activation, delta) -> DevicePair
@@ -465,10 +466,14 @@ class B200Backend:
         if critical:
             # the decision is within a few resolutions of its threshold: the reference's CPU comparison decides
             self.comparison_counts["cpu"] += 1
-            if joint:
-                return J["EC3"].stable_energy_reductions(problem, base, trial)
-            return J["EC3"].stable_energy_reduction(problem, base, trial, outer_only=outer_only)
-        self.comparison_counts["gpu"] += 1
+            out = (J["EC3"].stable_energy_reductions(problem, base, trial) if joint else
+                   (J["EC3"].stable_energy_reduction(problem, base, trial, outer_only=outer_only),))
+            path = "cpu"
+        else:
+            self.comparison_counts["gpu"] += 1
+            path = "gpu"
+        self.last_comparison = dict(path=path, reason="critical_margin" if critical else "resolved",
+                                    required_reduction=required, guard=[r.resolution for r in out])
         return out if joint else out[0]
 
     def stable_energy_reduction(self, problem, base, trial, *, outer_only=False, required_reduction=0.):

@@ -1,5 +1,6 @@
 """Device plumbing: torch owns device memory and streams; the kernels are libsvp3d's."""
 import ctypes
+import warnings
 
 import numpy as np
 import torch
@@ -31,7 +32,10 @@ def to_device(a, dtype=torch.float64, device="cuda"):
     if isinstance(a, torch.Tensor):
         t = a.to(device=device, dtype=dtype)
     else:
-        t = torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype)
+        with warnings.catch_warnings():
+            # read-only host arrays (frozen states) are only read: the tensor view is copied to the device at once
+            warnings.simplefilter("ignore", UserWarning)
+            t = torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype)
     return t.contiguous()
 
 
