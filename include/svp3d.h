@@ -69,6 +69,15 @@ int svp_timer_read(const char *name, int64_t *count, double *total_ms);
  *                                              depth-first subdivision (feasibility.py:353, left child first) */
 #define SVP_CERT_NO_HULL 1
 #define SVP_CERT_DEPTH_FIRST 2
+/* SVP_CERT_DIRECTED (combinable with the above): the mixed form's arithmetic.  Every interval operation of the edge
+ * hull, the interval fallback and the Bernstein subdivision rounds its lower end toward -inf and its upper end toward
+ * +inf (__dadd_rd / __dmul_ru ...), one rounding per end, instead of round-to-nearest plus one outward ulp.  Each
+ * end lies inside the reference's, so every enclosure is valid and at least as tight: cells the reference proves stay
+ * proven, witnesses are true violations in both, and only cells the reference leaves undecided can change (to a
+ * decision).  The prescreen keeps its a-priori bound on nearest rounding; min_jd_lower_bound = lowest + delta is
+ * stepped one ulp down as in the plain form.  No counterpart in the reference (whose intervals step after rounding to
+ * nearest, interval.py:52-54). */
+#define SVP_CERT_DIRECTED 4
 typedef struct svp_cert_config {
     double delta;       /* J > delta is proven; 0 <= delta < 1 */
     int64_t max_depth;  /* subdivision depth budget */
@@ -102,6 +111,10 @@ typedef struct svp_cell_verdict {
  * GpuEdgeHull.margins.  margin: (ncell,) float64, flag: (ncell,) uint8. */
 int svp_edge_hull_margins(const svp_grid *g, const double *u, double delta, double *margin, uint8_t *flag,
                           void *stream);
+/* The same margins in the directed-rounding arithmetic (SVP_CERT_DIRECTED): margin >= svp_edge_hull_margins' margin
+ * wherever neither is flagged. */
+int svp_edge_hull_margins_directed(const svp_grid *g, const double *u, double delta, double *margin, uint8_t *flag,
+                                   void *stream);
 
 /* Rigorous float Bernstein lower bounds of J over the listed cells (NaN where not finite).
  * Replaces certificate_prescreen.py:125 prescreen_lower_bounds.  cells: (n,) int64 cell ids; out: (n,) float64. */
@@ -114,6 +127,10 @@ int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, const int64_t
  * storage order 9 iz + 3 iy + ix; ok: (n,) uint8. */
 int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta, double *p_lo,
                         double *p_hi, double *c_lo, double *c_hi, double *samples, uint8_t *ok, void *stream);
+/* svp_fallback_arrays in the directed-rounding arithmetic (SVP_CERT_DIRECTED); the float64 samples are unchanged. */
+int svp_fallback_arrays_directed(const double *vertices, int64_t n, const double *spacing3, double delta,
+                                 double *p_lo, double *p_hi, double *c_lo, double *c_hi, double *samples, uint8_t *ok,
+                                 void *stream);
 
 /* Lowest-bound-first Bernstein subdivision of n cells (one warp per cell, heap in a stream-ordered scratch
  * allocation).  Replaces feasibility.py:295 _classify.  Inputs (n, 27) from svp_fallback_arrays; out: (n,). */
@@ -126,6 +143,7 @@ int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_l
  * the left child first). */
 #define SVP_SUBDIVIDE_LOWEST_FIRST 0
 #define SVP_SUBDIVIDE_DEPTH_FIRST 1
+#define SVP_SUBDIVIDE_DIRECTED 2      /* or-ed in: Bernstein splits in the directed-rounding arithmetic */
 int svp_classify_cells_policy(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
                               int64_t n, double delta, int64_t max_depth, int64_t max_boxes, int32_t policy,
                               svp_cell_verdict *out, void *stream);

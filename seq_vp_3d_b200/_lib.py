@@ -61,8 +61,10 @@ SIGNATURES = {
     "svp_timers_enable": [ctypes.c_int],
     "svp_timer_read": [ctypes.c_char_p, P, P],
     "svp_edge_hull_margins": [P, P, D, P, P, P],
+    "svp_edge_hull_margins_directed": [P, P, D, P, P, P],
     "svp_prescreen_lower_bounds": [P, P, P, I64, P, P],
     "svp_fallback_arrays": [P, I64, P, D, P, P, P, P, P, P, P],
+    "svp_fallback_arrays_directed": [P, I64, P, D, P, P, P, P, P, P, P],
     "svp_classify_cells": [P, P, P, P, I64, D, I64, I64, P, P],
     "svp_classify_cells_noalloc": [P, P, P, P, I64, D, I64, I64, P, P],
     "svp_classify_cells_policy": [P, P, P, P, I64, D, I64, I64, I32, P, P],

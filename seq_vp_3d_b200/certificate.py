@@ -208,13 +208,15 @@ class Interval:
 
 
 class Certifier:
-    """Owned device workspace for one (grid, config) pair (libsvp3d svp_certifier)."""
+    """Owned device workspace for one (grid, config) pair (libsvp3d svp_certifier).  directed=True selects the
+    directed-rounding arithmetic of the mixed form (valid enclosures at least as tight as the reference's)."""
 
-    def __init__(self, grid, config):
+    def __init__(self, grid, config, directed=False):
         require_cuda()
-        self.grid, self.config = grid, config
+        self.grid, self.config, self.directed = grid, config, bool(directed)
         self._g = grid_struct(grid)
         prescreen, execution = execution_of(config)
+        execution |= 4 if directed else 0          # SVP_CERT_DIRECTED
         cfg = _lib.CertConfig(config.delta, config.max_depth, config.max_boxes, config.tile_size, prescreen, execution)
         handle = ctypes.c_void_p()
         _lib.call("svp_certifier_create", ctypes.byref(self._g), ctypes.byref(cfg), ctypes.byref(handle))
@@ -239,16 +241,16 @@ _CERTIFIERS = {}
 _CERT_LOCK = threading.Lock()
 
 
-def certifier(grid, config):
+def certifier(grid, config, directed=False):
     """The workspace of (grid, config) on the current device for the calling host thread: registrations that run
     concurrently on their own threads and streams never share a certificate workspace."""
-    key = (grid.grid_id, grid.shape, config, torch.cuda.current_device(), threading.get_ident())
+    key = (grid.grid_id, grid.shape, config, bool(directed), torch.cuda.current_device(), threading.get_ident())
     with _CERT_LOCK:
         c = _CERTIFIERS.get(key)
         if c is None:
             if len(_CERTIFIERS) > 16:
                 _CERTIFIERS.clear()
-            c = _CERTIFIERS[key] = Certifier(grid, config)
+            c = _CERTIFIERS[key] = Certifier(grid, config, directed)
     return c
 
 
@@ -278,14 +280,14 @@ def _field(u, grid):
     return to_device(a), a
 
 
-def certify_map(u, grid, *, config=None, with_hash=True, stream=None):
+def certify_map(u, grid, *, config=None, with_hash=True, stream=None, directed=False):
     """All cells plus six faces and sampling domain (feasibility.py:393).  Host input is hashed (SHA-256 of its
     C-order bytes) as the reference does; a device tensor is hashed only with with_hash=True (one download)."""
     config = CertificateConfig() if config is None else config
     if not isinstance(config, CertificateConfig):
         raise InputValidationError("config: CertificateConfig required")
     dev, host = _field(u, grid)
-    record = certifier(grid, config).run(dev, stream)
+    record = certifier(grid, config, directed).run(dev, stream)
     digest = None
     if with_hash:
         if host is None:
@@ -294,7 +296,7 @@ def certify_map(u, grid, *, config=None, with_hash=True, stream=None):
     return result_from_record(record, grid, config, digest)
 
 
-def parallel_margins(u, grid, delta, stream=None):
+def parallel_margins(u, grid, delta, stream=None, directed=False):
     """(margin float64[ncell], flag bool[ncell]) of the edge-hull enclosure; numpy out for numpy in."""
     require_cuda()
     dev, host = _field(u, grid)
@@ -302,8 +304,8 @@ def parallel_margins(u, grid, delta, stream=None):
     margin = torch.empty(n, dtype=torch.float64, device=dev.device)
     flag = torch.empty(n, dtype=torch.uint8, device=dev.device)
     g = grid_struct(grid)
-    _lib.call("svp_edge_hull_margins", ctypes.byref(g), ptr(dev), float(delta), ptr(margin), ptr(flag),
-              stream_ptr(stream))
+    _lib.call("svp_edge_hull_margins_directed" if directed else "svp_edge_hull_margins", ctypes.byref(g), ptr(dev),
+              float(delta), ptr(margin), ptr(flag), stream_ptr(stream))
     if host is not None:
         return margin.cpu().numpy(), flag.cpu().numpy().astype(bool)
     return margin, flag.bool()
@@ -342,7 +344,7 @@ def prescreen_lower_bounds(u, grid, coefficients, cells, *, workers=None, stream
     return out.cpu().numpy() if host is not None else out
 
 
-def fallback_arrays_device(vertices, spacing, delta, stream=None):
+def fallback_arrays_device(vertices, spacing, delta, stream=None, directed=False):
     """(ok uint8[n], p_lo, p_hi, c_lo, c_hi, samples: (n, 27)) as CUDA tensors."""
     require_cuda()
     v = to_device(vertices)
@@ -353,8 +355,8 @@ def fallback_arrays_device(vertices, spacing, delta, stream=None):
     ok = torch.empty(n, dtype=torch.uint8, device=v.device)
     h = (ctypes.c_double * 3)(*[float(x) for x in spacing])
     if n:
-        _lib.call("svp_fallback_arrays", ptr(v), n, h, float(delta), *[ptr(o) for o in outs], ptr(ok),
-                  stream_ptr(stream))
+        _lib.call("svp_fallback_arrays_directed" if directed else "svp_fallback_arrays", ptr(v), n, h, float(delta),
+                  *[ptr(o) for o in outs], ptr(ok), stream_ptr(stream))
     return (ok, *outs)
 
 
@@ -368,7 +370,8 @@ def fallback_arrays(vertices, spacing, delta, errors=None):
             smp.reshape(shape))
 
 
-def classify_cells(c_lo, c_hi, p_lo, p_hi, delta, max_depth=48, max_boxes=255, depth_first=False, stream=None):
+def classify_cells(c_lo, c_hi, p_lo, p_hi, delta, max_depth=48, max_boxes=255, depth_first=False, stream=None,
+                   directed=False):
     """Subdivision verdicts (feasibility.py:295 _classify) of n cells: list of dicts.  depth_first selects the bare
     CertificateConfig's order (a stack, left child first); the default is the adaptive lowest-bound-first order."""
     arrs = [to_device(np.asarray(a).reshape(-1, 27) if not isinstance(a, torch.Tensor) else a.reshape(-1, 27))
@@ -377,7 +380,7 @@ def classify_cells(c_lo, c_hi, p_lo, p_hi, delta, max_depth=48, max_boxes=255, d
     out = torch.empty((n, ctypes.sizeof(_lib.CellVerdict)), dtype=torch.uint8, device=arrs[0].device)
     if n:
         _lib.call("svp_classify_cells_policy", *[ptr(a) for a in arrs], n, float(delta), int(max_depth),
-                  int(max_boxes), 1 if depth_first else 0, ptr(out), stream_ptr(stream))
+                  int(max_boxes), (1 if depth_first else 0) | (2 if directed else 0), ptr(out), stream_ptr(stream))
     raw = out.cpu().numpy()
     res = []
     for k in range(n):

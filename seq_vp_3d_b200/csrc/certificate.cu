@@ -45,6 +45,77 @@ __device__ __forceinline__ double div_axis(double x, const AxisDiv &d, int j) {
     return d.pow2[j] ? rmul(x, d.ih[j]) : rdiv(x, d.h[j]);
 }
 
+// ---------------------------------------------------------------------------------------- directed rounding
+// The directed-rounding arithmetic of the mixed form's certificate: every interval operation rounds its lower end
+// toward -inf and its upper end toward +inf (__d*_rd / __d*_ru), one rounding per end.  Each such end lies inside
+// the nearest-plus-one-ulp end of the reference's arithmetic (RD(x) >= step_down(RN(x)), RU(x) <= step_up(RN(x))),
+// so every enclosure is a valid one at least as tight as the reference's: a cell the reference proves stays proven,
+// and a witness (an upper bound <= 0) is a true violation in both.  Validity: both ends finite and lo <= hi.
+__device__ __forceinline__ bool dvalid(double lo, double hi) { return finite64(lo) && finite64(hi) && lo <= hi; }
+__device__ __forceinline__ bool dadd(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    rl = __dadd_rd(al, bl);
+    rh = __dadd_ru(ah, bh);
+    return dvalid(rl, rh);
+}
+__device__ __forceinline__ bool dsub(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    rl = __dsub_rd(al, bh);
+    rh = __dsub_ru(ah, bl);
+    return dvalid(rl, rh);
+}
+__device__ __forceinline__ bool dmul(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    rl = nmin(nmin(nmin(__dmul_rd(al, bl), __dmul_rd(al, bh)), __dmul_rd(ah, bl)), __dmul_rd(ah, bh));
+    rh = nmax(nmax(nmax(__dmul_ru(al, bl), __dmul_ru(al, bh)), __dmul_ru(ah, bl)), __dmul_ru(ah, bh));
+    return dvalid(rl, rh);
+}
+// interval / h_j with h_j > 0 (a power of two: the exact reciprocal multiply, directed)
+__device__ __forceinline__ double div_axis_rd(double x, const AxisDiv &d, int j) {
+    return d.pow2[j] ? __dmul_rd(x, d.ih[j]) : __ddiv_rd(x, d.h[j]);
+}
+__device__ __forceinline__ double div_axis_ru(double x, const AxisDiv &d, int j) {
+    return d.pow2[j] ? __dmul_ru(x, d.ih[j]) : __ddiv_ru(x, d.h[j]);
+}
+// the left-associated cofactor expansion of idet, directed
+__device__ __forceinline__ bool ddet(const double fl[3][3], const double fh[3][3], double &jl, double &jh) {
+    double p1l, p1h, p2l, p2h, al, ah, bl, bh, cl, ch, t1l, t1h, t2l, t2h, sl, sh, t3l, t3h;
+    bool ok = true;
+    ok &= dmul(fl[1][1], fh[1][1], fl[2][2], fh[2][2], p1l, p1h);
+    ok &= dmul(fl[1][2], fh[1][2], fl[2][1], fh[2][1], p2l, p2h);
+    ok &= dsub(p1l, p1h, p2l, p2h, al, ah);
+    ok &= dmul(fl[1][2], fh[1][2], fl[2][0], fh[2][0], p1l, p1h);
+    ok &= dmul(fl[1][0], fh[1][0], fl[2][2], fh[2][2], p2l, p2h);
+    ok &= dsub(p1l, p1h, p2l, p2h, bl, bh);
+    ok &= dmul(fl[1][0], fh[1][0], fl[2][1], fh[2][1], p1l, p1h);
+    ok &= dmul(fl[1][1], fh[1][1], fl[2][0], fh[2][0], p2l, p2h);
+    ok &= dsub(p1l, p1h, p2l, p2h, cl, ch);
+    ok &= dmul(fl[0][0], fh[0][0], al, ah, t1l, t1h);
+    ok &= dmul(fl[0][1], fh[0][1], bl, bh, t2l, t2h);
+    ok &= dadd(t1l, t1h, t2l, t2h, sl, sh);
+    ok &= dmul(fl[0][2], fh[0][2], cl, ch, t3l, t3h);
+    ok &= dadd(sl, sh, t3l, t3h, jl, jh);
+    return ok;
+}
+// the interval operations of either arithmetic (DIR: directed; else the reference's nearest plus one ulp)
+template <bool DIR>
+__device__ __forceinline__ bool Iadd(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    if constexpr (DIR) return dadd(al, ah, bl, bh, rl, rh);
+    else return iadd(al, ah, bl, bh, rl, rh);
+}
+template <bool DIR>
+__device__ __forceinline__ bool Isub(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    if constexpr (DIR) return dsub(al, ah, bl, bh, rl, rh);
+    else return isub(al, ah, bl, bh, rl, rh);
+}
+template <bool DIR>
+__device__ __forceinline__ bool Imul(double al, double ah, double bl, double bh, double &rl, double &rh) {
+    if constexpr (DIR) return dmul(al, ah, bl, bh, rl, rh);
+    else return imul(al, ah, bl, bh, rl, rh);
+}
+template <bool DIR>
+__device__ __forceinline__ bool Idet(const double fl[3][3], const double fh[3][3], double &jl, double &jh) {
+    if constexpr (DIR) return ddet(fl, fh, jl, jh);
+    else return idet(fl, fh, jl, jh);
+}
+
 struct CellGrid {
     long long nx, ny, nz, cx, cy, cz, ncell;
     double h[3];
@@ -82,26 +153,42 @@ __device__ __forceinline__ int edge_start(int j, int e) {
 
 // ============================================================================================== 1. edge hull
 // F_rj interval: hull of the 4 edge differences (from +inf / -inf in edge order), outward, /h, outward, + identity.
+template <bool DIR>
 __device__ __forceinline__ bool hull_entry_v(const double v[8][3], int j, int r, const AxisDiv &dv, double &lo,
                                              double &hi) {
     bool ok = true;
     double lower = __longlong_as_double(0x7FF0000000000000LL), upper = -lower;
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        int a = edge_start(j, e), b = a | (1 << j);
-        double d = rsub(v[b][r], v[a][r]);
-        ok &= finite64(d);
-        lower = nmin(lower, d);
-        upper = nmax(upper, d);
-    }
     double l, hh;
-    ok &= iout(lower, upper, l, hh);
-    ok &= iout(div_axis(l, dv, j), div_axis(hh, dv, j), l, hh);
+    if constexpr (DIR) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            int a = edge_start(j, e), b = a | (1 << j);
+            double dl = __dsub_rd(v[b][r], v[a][r]), dh = __dsub_ru(v[b][r], v[a][r]);
+            ok &= finite64(dl) && finite64(dh);
+            lower = nmin(lower, dl);
+            upper = nmax(upper, dh);
+        }
+        l = div_axis_rd(lower, dv, j);
+        hh = div_axis_ru(upper, dv, j);
+        ok &= dvalid(l, hh);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            int a = edge_start(j, e), b = a | (1 << j);
+            double d = rsub(v[b][r], v[a][r]);
+            ok &= finite64(d);
+            lower = nmin(lower, d);
+            upper = nmax(upper, d);
+        }
+        ok &= iout(lower, upper, l, hh);
+        ok &= iout(div_axis(l, dv, j), div_axis(hh, dv, j), l, hh);
+    }
     double id = (r == j) ? 1.0 : 0.0;
-    ok &= iadd(l, hh, id, id, lo, hi);
+    ok &= Iadd<DIR>(l, hh, id, id, lo, hi);
     return ok;
 }
 
+template <bool DIR>
 __global__ void __launch_bounds__(256) edge_hull_kernel(const double *__restrict__ u, CellGrid g, double delta,
                                                         double *__restrict__ margin, uint8_t *__restrict__ flag) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncell;
@@ -117,10 +204,11 @@ __global__ void __launch_bounds__(256) edge_hull_kernel(const double *__restrict
 #pragma unroll
         for (int j = 0; j < 3; j++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) ok &= hull_entry_v(v, j, r, g.div, fl[r][j], fh[r][j]);
+            for (int r = 0; r < 3; r++) ok &= hull_entry_v<DIR>(v, j, r, g.div, fl[r][j], fh[r][j]);
         double jl, jh, ml, mh;
-        ok &= idet(fl, fh, jl, jh);
-        ok &= iout(rsub(jl, delta), rsub(jh, delta), ml, mh);
+        ok &= Idet<DIR>(fl, fh, jl, jh);
+        if constexpr (DIR) ok &= dsub(jl, jh, delta, delta, ml, mh);
+        else ok &= iout(rsub(jl, delta), rsub(jh, delta), ml, mh);
         margin[c] = ml;
         flag[c] = ok ? 0 : 1;
     }
@@ -337,6 +425,7 @@ __device__ __forceinline__ double edge_weight(int j, int e, int p) {
 // the middle entries of each line on their own lanes, with a warp barrier between passes.  Bitwise the sequential
 // form: each point's arithmetic is the same, and a pass reads only entries it does not write.  Returns ok for the
 // whole cell (warp-uniform).
+template <bool DIR>
 __device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double delta, double *plo, double *phi,
                                    double *clo, double *chi, double *smp, double *sb) {
     const int p = threadIdx.x & 31;
@@ -350,12 +439,21 @@ __device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double
             int a = edge_start(j, e), b = a | (1 << j);
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                double d = rsub(v[3 * b + r], v[3 * a + r]);
-                double sl, sh;
-                ok &= iout(d, d, sl, sh);
-                double x1 = div_axis(sl, dv, j), x2 = div_axis(sh, dv, j);
-                ok &= iout(nmin(nmin(nmin(x1, x1), x2), x2), nmax(nmax(nmax(x1, x1), x2), x2), elo[j][e][r],
-                           ehi[j][e][r]);
+                if constexpr (DIR) {
+                    // [RD(vb - va), RU(vb - va)] / h_j directed (h_j > 0)
+                    double dl = __dsub_rd(v[3 * b + r], v[3 * a + r]), dh = __dsub_ru(v[3 * b + r], v[3 * a + r]);
+                    ok &= dvalid(dl, dh);
+                    elo[j][e][r] = div_axis_rd(dl, dv, j);
+                    ehi[j][e][r] = div_axis_ru(dh, dv, j);
+                    ok &= dvalid(elo[j][e][r], ehi[j][e][r]);
+                } else {
+                    double d = rsub(v[3 * b + r], v[3 * a + r]);
+                    double sl, sh;
+                    ok &= iout(d, d, sl, sh);
+                    double x1 = div_axis(sl, dv, j), x2 = div_axis(sh, dv, j);
+                    ok &= iout(nmin(nmin(nmin(x1, x1), x2), x2), nmax(nmax(nmax(x1, x1), x2), x2), elo[j][e][r],
+                               ehi[j][e][r]);
+                }
             }
         }
     if (point) {
@@ -368,15 +466,16 @@ __device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     double w = edge_weight(j, e, p), wl, wh;
-                    ok &= iout(rmul(elo[j][e][r], w), rmul(ehi[j][e][r], w), wl, wh);
-                    ok &= iadd(dl, dh, wl, wh, dl, dh);
+                    if constexpr (DIR) ok &= dmul(elo[j][e][r], ehi[j][e][r], w, w, wl, wh);
+                    else ok &= iout(rmul(elo[j][e][r], w), rmul(ehi[j][e][r], w), wl, wh);
+                    ok &= Iadd<DIR>(dl, dh, wl, wh, dl, dh);
                 }
                 double c = (r == j) ? 1. : 0.;
-                ok &= iadd(dl, dh, c, c, fl[r][j], fh[r][j]);
+                ok &= Iadd<DIR>(dl, dh, c, c, fl[r][j], fh[r][j]);
             }
         double jl, jh, ml, mh;
-        ok &= idet(fl, fh, jl, jh);
-        ok &= isub(jl, jh, delta, delta, ml, mh);
+        ok &= Idet<DIR>(fl, fh, jl, jh);
+        ok &= Isub<DIR>(jl, jh, delta, delta, ml, mh);
         plo[p] = ml; phi[p] = mh;
         sb[p] = ml; sb[27 + p] = mh;
     }
@@ -390,10 +489,10 @@ __device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double
         if (mid) {
             int a0 = p - stride, a2 = p + stride;
             double ml1, mh1, sl1, sh1, hl1, hh1;
-            ok &= imul(sb[p], sb[27 + p], 2., 2., ml1, mh1);
-            ok &= iadd(sb[a0], sb[27 + a0], sb[a2], sb[27 + a2], sl1, sh1);
-            ok &= imul(sl1, sh1, .5, .5, hl1, hh1);
-            ok &= isub(ml1, mh1, hl1, hh1, nl, nh);
+            ok &= Imul<DIR>(sb[p], sb[27 + p], 2., 2., ml1, mh1);
+            ok &= Iadd<DIR>(sb[a0], sb[27 + a0], sb[a2], sb[27 + a2], sl1, sh1);
+            ok &= Imul<DIR>(sl1, sh1, .5, .5, hl1, hh1);
+            ok &= Isub<DIR>(ml1, mh1, hl1, hh1, nl, nh);
         }
         __syncwarp();
         if (mid) { sb[p] = nl; sb[27 + p] = nh; }
@@ -445,6 +544,7 @@ __device__ bool fallback_cell_warp(const double v[24], const AxisDiv &dv, double
 constexpr int kFallbackWarps = 4;   // cells per 128-thread block
 
 // Standalone cells: vertices (n, 8, 3), one warp per cell
+template <bool DIR>
 __global__ void __launch_bounds__(32 * kFallbackWarps) fallback_vertices_kernel(
     const double *__restrict__ vertices, long long n, const AxisDiv dv, double delta, double *plo, double *phi,
     double *clo, double *chi, double *smp, uint8_t *ok) {
@@ -454,14 +554,15 @@ __global__ void __launch_bounds__(32 * kFallbackWarps) fallback_vertices_kernel(
         double v[24];
 #pragma unroll
         for (int k = 0; k < 24; k++) v[k] = vertices[24 * i + k];
-        bool good = fallback_cell_warp(v, dv, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i,
-                                       smp + 27 * i, sb[w]);
+        bool good = fallback_cell_warp<DIR>(v, dv, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i,
+                                            smp + 27 * i, sb[w]);
         if ((threadIdx.x & 31) == 0) ok[i] = good;
         __syncwarp();
     }
 }
 
 // Grid cells from a list: vertices gathered from u, one warp per cell
+template <bool DIR>
 __global__ void __launch_bounds__(32 * kFallbackWarps) fallback_grid_kernel(
     const double *__restrict__ u, CellGrid g, const long long *__restrict__ cells, long long n, double delta,
     double *plo, double *phi, double *clo, double *chi, double *smp, uint8_t *ok) {
@@ -474,8 +575,8 @@ __global__ void __launch_bounds__(32 * kFallbackWarps) fallback_grid_kernel(
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) v[3 * a + r] = __ldg(u + 3 * vnode(base, a, g.ny, g.nx) + r);
-        bool good = fallback_cell_warp(v, g.div, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i, chi + 27 * i,
-                                       smp + 27 * i, sb[w]);
+        bool good = fallback_cell_warp<DIR>(v, g.div, delta, plo + 27 * i, phi + 27 * i, clo + 27 * i,
+                                            chi + 27 * i, smp + 27 * i, sb[w]);
         if ((threadIdx.x & 31) == 0) ok[i] = good;
         __syncwarp();
     }
@@ -546,13 +647,14 @@ struct WarpHeap {
     }
 };
 
+template <bool DIR>
 __device__ void verdict_result(svp_cell_verdict &v, int status, double margin, long long boxes, long long depth,
                                const double *w, int reason, double delta) {
     v.boxes = boxes; v.depth = depth;
     v.witness[0] = v.witness[1] = v.witness[2] = __longlong_as_double(0x7FF8000000000000LL);
     if (delta != 0.) {
         double l, h;
-        if (!iout(radd(margin, delta), radd(margin, delta), l, h)) {
+        if (DIR ? !dadd(margin, margin, delta, delta, l, h) : !iout(radd(margin, delta), radd(margin, delta), l, h)) {
             v.status = ST_UNCERTAIN; v.reason = R_ARITH; v.has_margin = 0; v.has_witness = 0;
             v.margin = __longlong_as_double(0x7FF8000000000000LL);
             return;
@@ -564,6 +666,7 @@ __device__ void verdict_result(svp_cell_verdict &v, int status, double margin, l
 }
 
 // One warp per cell; rows[i] selects the input row (nullptr: row i).  Lanes 0..26 hold one coefficient each.
+template <bool DIR>
 __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict__ clo, const double *__restrict__ chi,
                                                        const double *__restrict__ phi, const long long *rows,
                                                        long long n, double delta, long long max_depth,
@@ -594,7 +697,7 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
         if (sw) {
             int q = __ffs(sw) - 1;
             double w[3] = {(q % 3) / 2., ((q / 3) % 3) / 2., (q / 9) / 2.};
-            verdict_result(v, ST_INFEASIBLE, root_lower, 1, 0, w, R_SAMPLE_WITNESS, delta);
+            verdict_result<DIR>(v, ST_INFEASIBLE, root_lower, 1, 0, w, R_SAMPLE_WITNESS, delta);
             if (lane == 0) out[i] = v;
             continue;
         }
@@ -615,7 +718,7 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
         int size = 1;
         while (size > 0) {
             if (boxes >= max_boxes) {
-                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_BOX_BUDGET, delta);
+                verdict_result<DIR>(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_BOX_BUDGET, delta);
                 done = true;
                 break;
             }
@@ -645,7 +748,7 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
                 int bits[3] = {(q % 3) / 2, ((q / 3) % 3) / 2, (q / 9) / 2};
                 double w[3];
                 for (int k = 0; k < 3; k++) w[k] = bits[k] ? high[k] : low[k];
-                verdict_result(v, ST_INFEASIBLE, root_lower, boxes, depth_used, w, R_SUBDIV_WITNESS, delta);
+                verdict_result<DIR>(v, ST_INFEASIBLE, root_lower, boxes, depth_used, w, R_SUBDIV_WITNESS, delta);
                 done = true;
                 break;
             }
@@ -670,14 +773,14 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
             double cl = __shfl_sync(0xFFFFFFFFu, clo_, lc), ch = __shfl_sync(0xFFFFFFFFu, chi_, lc);
             double sl, sh, abl, abh, bcl, bch, ml, mh;
             bool ok = true;
-            ok &= iadd(al, ah, bl, bh, sl, sh);
-            ok &= imul(sl, sh, .5, .5, abl, abh);
-            ok &= iadd(bl, bh, cl, ch, sl, sh);
-            ok &= imul(sl, sh, .5, .5, bcl, bch);
-            ok &= iadd(abl, abh, bcl, bch, sl, sh);
-            ok &= imul(sl, sh, .5, .5, ml, mh);
+            ok &= Iadd<DIR>(al, ah, bl, bh, sl, sh);
+            ok &= Imul<DIR>(sl, sh, .5, .5, abl, abh);
+            ok &= Iadd<DIR>(bl, bh, cl, ch, sl, sh);
+            ok &= Imul<DIR>(sl, sh, .5, .5, bcl, bch);
+            ok &= Iadd<DIR>(abl, abh, bcl, bch, sl, sh);
+            ok &= Imul<DIR>(sl, sh, .5, .5, ml, mh);
             if (__ballot_sync(0xFFFFFFFFu, act && !ok)) {
-                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_ARITH, delta);
+                verdict_result<DIR>(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_ARITH, delta);
                 done = true;
                 break;
             }
@@ -713,9 +816,9 @@ __global__ void __launch_bounds__(128) classify_kernel(const double *__restrict_
         }
         if (!done) {
             if (uncertain)
-                verdict_result(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_DEPTH_BUDGET, delta);
+                verdict_result<DIR>(v, ST_UNCERTAIN, root_lower, boxes, depth_used, nullptr, R_DEPTH_BUDGET, delta);
             else
-                verdict_result(v, ST_FEASIBLE, cert_min, boxes, depth_used, nullptr, R_BERNSTEIN, delta);
+                verdict_result<DIR>(v, ST_FEASIBLE, cert_min, boxes, depth_used, nullptr, R_BERNSTEIN, delta);
         }
         if (lane == 0) out[i] = v;
         __syncwarp();
@@ -962,7 +1065,17 @@ extern "C" int svp_edge_hull_margins(const svp_grid *g, const double *u, double 
     SVP_REQUIRE(grid_ok(g), "svp_edge_hull_margins: invalid grid");
     SVP_REQUIRE(u && margin && flag, "svp_edge_hull_margins: null pointer");
     CellGrid cg = cell_grid(g);
-    { svp::KernelTimer _t("edge_hull_kernel", (cudaStream_t)stream); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag)); }
+    { svp::KernelTimer _t("edge_hull_kernel", (cudaStream_t)stream); SVP_LAUNCH(edge_hull_kernel<false><<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag)); }
+    SVP_LAUNCH_CHECK("edge_hull_kernel");
+    return SVP_OK;
+}
+
+extern "C" int svp_edge_hull_margins_directed(const svp_grid *g, const double *u, double delta, double *margin,
+                                              uint8_t *flag, void *stream) {
+    SVP_REQUIRE(grid_ok(g), "svp_edge_hull_margins_directed: invalid grid");
+    SVP_REQUIRE(u && margin && flag, "svp_edge_hull_margins_directed: null pointer");
+    CellGrid cg = cell_grid(g);
+    { svp::KernelTimer _t("edge_hull_kernel", (cudaStream_t)stream); SVP_LAUNCH(edge_hull_kernel<true><<<blocks_for(cg.ncell, 256, 8), 256, 0, (cudaStream_t)stream>>>(u, cg, delta, margin, flag)); }
     SVP_LAUNCH_CHECK("edge_hull_kernel");
     return SVP_OK;
 }
@@ -980,33 +1093,55 @@ extern "C" int svp_prescreen_lower_bounds(const svp_grid *g, const double *u, co
     return SVP_OK;
 }
 
-extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta,
-                                   double *p_lo, double *p_hi, double *c_lo, double *c_hi, double *samples,
-                                   uint8_t *ok, void *stream) {
+static int fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta, double *p_lo,
+                           double *p_hi, double *c_lo, double *c_hi, double *samples, uint8_t *ok, bool directed,
+                           void *stream) {
     SVP_REQUIRE(n >= 0 && spacing3, "svp_fallback_arrays: invalid arguments");
     if (n == 0) return SVP_OK;
     SVP_REQUIRE(vertices && p_lo && p_hi && c_lo && c_hi && samples && ok, "svp_fallback_arrays: null pointer");
+    SVP_REQUIRE(spacing3[0] > 0 && spacing3[1] > 0 && spacing3[2] > 0, "svp_fallback_arrays: spacing must be > 0");
     const AxisDiv dv = axis_div(spacing3);
-    SVP_LAUNCH(fallback_vertices_kernel<<<blocks_for(div_up(n, kFallbackWarps), 1, 16), 32 * kFallbackWarps, 0,
-                                         (cudaStream_t)stream>>>(
-        vertices, n, dv, delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
+    const unsigned blocks = blocks_for(div_up(n, kFallbackWarps), 1, 16);
+    if (directed)
+        SVP_LAUNCH(fallback_vertices_kernel<true><<<blocks, 32 * kFallbackWarps, 0, (cudaStream_t)stream>>>(
+            vertices, n, dv, delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
+    else
+        SVP_LAUNCH(fallback_vertices_kernel<false><<<blocks, 32 * kFallbackWarps, 0, (cudaStream_t)stream>>>(
+            vertices, n, dv, delta, p_lo, p_hi, c_lo, c_hi, samples, ok));
     SVP_LAUNCH_CHECK("fallback_vertices_kernel");
     return SVP_OK;
+}
+
+extern "C" int svp_fallback_arrays(const double *vertices, int64_t n, const double *spacing3, double delta,
+                                   double *p_lo, double *p_hi, double *c_lo, double *c_hi, double *samples,
+                                   uint8_t *ok, void *stream) {
+    return fallback_arrays(vertices, n, spacing3, delta, p_lo, p_hi, c_lo, c_hi, samples, ok, false, stream);
+}
+
+extern "C" int svp_fallback_arrays_directed(const double *vertices, int64_t n, const double *spacing3, double delta,
+                                            double *p_lo, double *p_hi, double *c_lo, double *c_hi, double *samples,
+                                            uint8_t *ok, void *stream) {
+    return fallback_arrays(vertices, n, spacing3, delta, p_lo, p_hi, c_lo, c_hi, samples, ok, true, stream);
 }
 
 static int classify_launch(const double *c_lo, const double *c_hi, const double *p_hi, const long long *rows,
                            long long n, double delta, long long max_depth, long long max_boxes,
                            svp_cell_verdict *out, char *scratch, long long warps, long long slots,
-                           int depth_first, cudaStream_t stream) {
+                           int depth_first, bool directed, cudaStream_t stream) {
     long long threads = 128, blocks = div_up(warps * 32, threads);
-    { svp::KernelTimer _t("classify_kernel", stream); SVP_LAUNCH(classify_kernel<<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(c_lo, c_hi, p_hi, rows, n, delta, max_depth,
-                                                                        max_boxes, out, scratch, slots, depth_first)); }
+    svp::KernelTimer _t("classify_kernel", stream);
+    if (directed)
+        SVP_LAUNCH(classify_kernel<true><<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(
+            c_lo, c_hi, p_hi, rows, n, delta, max_depth, max_boxes, out, scratch, slots, depth_first));
+    else
+        SVP_LAUNCH(classify_kernel<false><<<(unsigned)blocks, (unsigned)threads, 0, stream>>>(
+            c_lo, c_hi, p_hi, rows, n, delta, max_depth, max_boxes, out, scratch, slots, depth_first));
     SVP_LAUNCH_CHECK("classify_kernel");
     return SVP_OK;
 }
 
 static int classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi, int64_t n,
-                          double delta, int64_t max_depth, int64_t max_boxes, int depth_first,
+                          double delta, int64_t max_depth, int64_t max_boxes, int depth_first, bool directed,
                           svp_cell_verdict *out, void *stream) {
     SVP_REQUIRE(n >= 0 && max_depth >= 0 && max_boxes >= 1, "svp_classify_cells: invalid arguments");
     if (n == 0) return SVP_OK;
@@ -1019,7 +1154,7 @@ static int classify_cells(const double *c_lo, const double *c_hi, const double *
     char *scratch = nullptr;
     SVP_CUDA(scratch_alloc((void **)&scratch, warp_scratch_bytes(slots) * warps, s));
     int rc = classify_launch(c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, warps, slots,
-                             depth_first, s);
+                             depth_first, directed, s);
     cudaError_t e = scratch_free(scratch, s);
     if (rc != SVP_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
@@ -1031,16 +1166,17 @@ static int classify_cells(const double *c_lo, const double *c_hi, const double *
 extern "C" int svp_classify_cells(const double *c_lo, const double *c_hi, const double *p_lo, const double *p_hi,
                                   int64_t n, double delta, int64_t max_depth, int64_t max_boxes,
                                   svp_cell_verdict *out, void *stream) {
-    return svp::classify_cells(c_lo, c_hi, p_lo, p_hi, n, delta, max_depth, max_boxes, 0, out, stream);
+    return svp::classify_cells(c_lo, c_hi, p_lo, p_hi, n, delta, max_depth, max_boxes, 0, false, out, stream);
 }
 
 extern "C" int svp_classify_cells_policy(const double *c_lo, const double *c_hi, const double *p_lo,
                                          const double *p_hi, int64_t n, double delta, int64_t max_depth,
                                          int64_t max_boxes, int32_t policy, svp_cell_verdict *out, void *stream) {
-    SVP_REQUIRE(policy == SVP_SUBDIVIDE_LOWEST_FIRST || policy == SVP_SUBDIVIDE_DEPTH_FIRST,
+    SVP_REQUIRE((policy & ~(SVP_SUBDIVIDE_DEPTH_FIRST | SVP_SUBDIVIDE_DIRECTED)) == 0,
                 "svp_classify_cells_policy: unknown subdivision policy");
     return svp::classify_cells(c_lo, c_hi, p_lo, p_hi, n, delta, max_depth, max_boxes,
-                               policy == SVP_SUBDIVIDE_DEPTH_FIRST, out, stream);
+                               (policy & SVP_SUBDIVIDE_DEPTH_FIRST) ? 1 : 0, (policy & SVP_SUBDIVIDE_DIRECTED) != 0,
+                               out, stream);
 }
 
 // ---------------------------------------------------------------------------------------------- certifier handle
@@ -1109,7 +1245,7 @@ extern "C" int svp_certifier_create(const svp_grid *g, const svp_cert_config *cf
     SVP_REQUIRE(cfg->max_depth >= 0 && cfg->max_boxes >= 1 && cfg->tile_size >= 1,
                 "svp_certifier_create: invalid budgets/tile size");
     SVP_REQUIRE(cfg->max_boxes <= (1LL << 24), "svp_certifier_create: max_boxes above 2^24");
-    SVP_REQUIRE((cfg->execution & ~(SVP_CERT_NO_HULL | SVP_CERT_DEPTH_FIRST)) == 0,
+    SVP_REQUIRE((cfg->execution & ~(SVP_CERT_NO_HULL | SVP_CERT_DEPTH_FIRST | SVP_CERT_DIRECTED)) == 0,
                 "svp_certifier_create: unknown execution flags");
     SVP_REQUIRE(!(cfg->prescreen && (cfg->execution & SVP_CERT_NO_HULL)),
                 "svp_certifier_create: the prescreen runs only after the edge-hull preproof");
@@ -1163,6 +1299,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     const double delta = c->cfg.delta;
     const bool hull = !(c->cfg.execution & SVP_CERT_NO_HULL);
     const int depth_first = (c->cfg.execution & SVP_CERT_DEPTH_FIRST) ? 1 : 0;
+    const bool directed = (c->cfg.execution & SVP_CERT_DIRECTED) != 0;
     const double nan = std::nan("");
     memset(out, 0, sizeof *out);
     out->status = ST_UNCERTAIN;
@@ -1178,7 +1315,15 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     SVP_LAUNCH_CHECK("precheck_kernel");
     SVP_CUDA(cudaMemsetAsync(c->tile_fail, 0, sizeof(int) * c->ntiles, s));
     if (hull) {
-        { svp::KernelTimer _t("edge_hull_kernel", s); SVP_LAUNCH(edge_hull_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin, c->flag)); }
+        {
+            svp::KernelTimer _t("edge_hull_kernel", s);
+            if (directed)
+                SVP_LAUNCH(edge_hull_kernel<true><<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin,
+                                                                                      c->flag));
+            else
+                SVP_LAUNCH(edge_hull_kernel<false><<<blocks_for(n, 256, 8), 256, 0, s>>>(u, c->cg, delta, c->margin,
+                                                                                       c->flag));
+        }
         SVP_LAUNCH_CHECK("edge_hull_kernel");
         SVP_CUDA(cudaMemsetAsync(c->tile_bad, 0, sizeof(int) * c->ntiles, s));
         SVP_LAUNCH(tile_flag_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->flag, n, tile, c->tile_bad));
@@ -1219,8 +1364,16 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
         if (rc) return rc;
         double *fb = c->fb, *plo = fb, *phi = fb + 27 * n2, *clo = fb + 2 * 27 * n2, *chi = fb + 3 * 27 * n2,
                *smp = fb + 4 * 27 * n2;
-        { svp::KernelTimer _t("fallback_grid_kernel", s); SVP_LAUNCH(fallback_grid_kernel<<<blocks_for(div_up(n2, kFallbackWarps), 1, 16), 32 * kFallbackWarps, 0, s>>>(u, c->cg, list2, n2, delta, plo, phi, clo, chi,
-                                                                    smp, c->fb_ok)); }
+        {
+            svp::KernelTimer _t("fallback_grid_kernel", s);
+            const unsigned fb_blocks = blocks_for(div_up(n2, kFallbackWarps), 1, 16);
+            if (directed)
+                SVP_LAUNCH(fallback_grid_kernel<true><<<fb_blocks, 32 * kFallbackWarps, 0, s>>>(
+                    u, c->cg, list2, n2, delta, plo, phi, clo, chi, smp, c->fb_ok));
+            else
+                SVP_LAUNCH(fallback_grid_kernel<false><<<fb_blocks, 32 * kFallbackWarps, 0, s>>>(
+                    u, c->cg, list2, n2, delta, plo, phi, clo, chi, smp, c->fb_ok));
+        }
         SVP_LAUNCH_CHECK("fallback_grid_kernel");
         SVP_LAUNCH(job_fail_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, c->fb_ok, n2, tile, c->tile_fail));
         SVP_LAUNCH(fallback_stage_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, clo, smp, n2, tile, c->tile_fail,
@@ -1235,7 +1388,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
             warps = (warps + 3) / 4 * 4;
             if (warps > c->heap_warps) warps = c->heap_warps;
             rc = classify_launch(clo, chi, phi, c->list3, n3, delta, c->cfg.max_depth, c->cfg.max_boxes,
-                                 c->verdicts, c->heap, warps, c->heap_slots, depth_first, s);
+                                 c->verdicts, c->heap, warps, c->heap_slots, depth_first, directed, s);
             if (rc) return rc;
             SVP_LAUNCH(verdict_stage_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
             SVP_LAUNCH(witness_kernel<<<blocks_for(n3, 256, 8), 256, 0, s>>>(c->verdicts, c->list3, list2, n3, c->acc));
@@ -1362,7 +1515,7 @@ extern "C" int svp_classify_cells_noalloc(const double *c_lo, const double *c_hi
     warps = (warps + 3) / 4 * 4;
     SVP_REQUIRE(warp_scratch_bytes(slots) * (size_t)warps <= kNoAllocBytes,
                 "svp_classify_cells_noalloc: scratch capacity exceeded");
-    SVP_LAUNCH(classify_kernel<<<(unsigned)(warps * 32 / 128), 128, 0, (cudaStream_t)stream>>>(
+    SVP_LAUNCH(classify_kernel<false><<<(unsigned)(warps * 32 / 128), 128, 0, (cudaStream_t)stream>>>(
         c_lo, c_hi, p_hi, nullptr, n, delta, max_depth, max_boxes, out, scratch, slots, 0));
     return SVP_OK;
 }

@@ -132,7 +132,8 @@ class Registration:
         u_ref = torch.zeros(grid.shape + (3,), dtype=torch.float64, device="cuda") if u_ref is None else u_ref
         self.pair = DevicePair(grid, fixed, moving, u_ref, lam=lam, mu=mu, nu=nu, kappa=kappa,
                                activation=activation, delta=self.delta, precision=precision)
-        self.certifier = cert_mod.certifier(grid, self.config)
+        # the mixed form proves J > delta in the directed-rounding arithmetic (enclosures at least as tight)
+        self.certifier = cert_mod.certifier(grid, self.config, directed=precision == "mixed")
         self.q_sum = grid.node_weight_total()
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0

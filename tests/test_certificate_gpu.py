@@ -207,3 +207,67 @@ def test_depth_first_classify(svp, cells_golden, configs_golden):
                     assert same_bits(r["margin"], cf[k, 0])
                 if r["witness"] is not None:
                     assert same_bits(r["witness"], cf[k, 1:])
+
+
+# ---------------------------------------------------------------------------------------------- directed rounding
+def test_directed_margins_are_valid_and_tighter(svp, cert_golden):
+    """The directed-rounding edge hull: wherever neither arithmetic flags a cell, its margin is at least the
+    reference's (every directed end lies inside the nearest-plus-one-ulp end), and it flags no cell the reference
+    does not."""
+    g = cert_golden
+    tighter = 0
+    for name in names(g):
+        u, grid = g[f"{name}/u"], grid_of(g, name)
+        if not np.all(np.isfinite(u)):
+            continue
+        for d in (0.0, 0.01):
+            m, f = svp.parallel_margins(u, grid, d)
+            md, fd = svp.parallel_margins(u, grid, d, directed=True)
+            assert not np.any(fd & ~f), (name, d)
+            both = ~f & ~fd
+            assert np.all(md[both] >= m[both]), (name, d)
+            tighter += int(np.sum(md[both] > m[both]))
+    assert tighter > 0
+
+
+def test_directed_verdicts_cell_by_cell(svp, cells_golden):
+    """Verdict by verdict on the 420 standalone cells (every subdivision outcome of the reference), both deltas, both
+    budgets: every cell the reference decides (certified or infeasible) gets the same verdict in the directed
+    arithmetic; an undecided directed verdict where the reference decided counts as a failure.  Cells the reference
+    leaves uncertain may be decided."""
+    verts, h = cells_golden["vertices"], cells_golden["spacing"]
+    decided_more = 0
+    for d in (0.0, 0.01):
+        ok, plo, phi, clo, chi, _ = (t.cpu().numpy() for t in svp.fallback_arrays_device(verts, h, d, directed=True))
+        for depth, boxes in ((48, 255), (6, 40)):
+            tag = f"d{d}/m{depth}_{boxes}"
+            ref_ok, ci = cells_golden[f"{tag}/ok"].astype(bool), cells_golden[f"{tag}/classify_i"]
+            assert np.all(ok.astype(bool) | ~ref_ok), tag      # finite reference arrays stay finite
+            sel = np.flatnonzero(ok)
+            got = svp.classify_cells(clo[sel], chi[sel], plo[sel], phi[sel], d, depth, boxes, directed=True)
+            for k, r in zip(sel, got):
+                if not ref_ok[k]:
+                    continue
+                ref_status = int(ci[k, 0])
+                if ref_status in (0, 1):
+                    assert r["status"] == ref_status, (tag, k, r, ci[k])
+                elif r["status"] != 2:
+                    decided_more += 1
+    print("directed decisions where the reference was uncertain:", decided_more)
+
+
+def test_directed_certify_map_records(svp, cert_golden):
+    """Whole-map certificates in the directed arithmetic on the golden fields (PrescreenCertificateConfig, both
+    deltas): the reference's decided statuses are reproduced, and a certified map's lower bound is at least the
+    reference's."""
+    g = cert_golden
+    for name in names(g):
+        u, grid = g[f"{name}/u"], grid_of(g, name)
+        for d in (0.0, 0.01):
+            cfg = svp.PrescreenCertificateConfig(delta=d, max_depth=48, max_boxes=255, tile_size=65536)
+            res = svp.certify_map(u, grid, config=cfg, directed=True)
+            ri, rf = g[f"{name}/d{d}/t65536/record_i"], g[f"{name}/d{d}/t65536/record_f"]
+            if ri[0] in (0, 1):
+                assert svp.STATUS.index(res.status) == ri[0], (name, d, res.status)
+            if ri[0] == 0 and np.isfinite(rf[0]):
+                assert res.min_jd_lower_bound >= rf[0], (name, d)

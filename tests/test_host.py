@@ -31,15 +31,27 @@ def test_boundary_taper_host_form():
 
 
 def test_bench_phase_split():
+    """One timed pair's host-clock phases: the loop's remainder after its kernels' device time (the pre-optimizer's
+    kernels are not the loop's)."""
     import bench
-    phases = [dict(preopt_s=.2, transfer_s=.01, certified_loop_s=10.), dict(preopt_s=.4, transfer_s=.03,
-                                                                              certified_loop_s=12.)]
+    phase = dict(preopt_s=.2, transfer_s=.01, certified_loop_s=10.)
     timers = {"cell_trial_kernel": (10, 4000.), "prescreen_kernel": (5, 1000.), "pre_data_kernel": (3, 500.)}
-    out = bench.phase_summary(phases, timers, steps=1)
-    assert abs(out["preopt_s"] - .3) < 1e-12 and abs(out["certified_loop_s"] - 11.) < 1e-12
-    assert abs(out["fp64_kernels_s"] - 5.) < 1e-12          # the pre-optimizer's kernels are not the loop's
-    assert abs(out["loop_host_gap_s"] - 6.) < 1e-12
-    assert bench.phase_summary([], timers, 1) is None
+    out = bench.phase_summary(phase, timers)
+    assert abs(out["preopt_s"] - .2) < 1e-12 and abs(out["certified_loop_s"] - 10.) < 1e-12
+    assert abs(out["loop_kernels_s"] - 5.) < 1e-12
+    assert abs(out["loop_host_gap_s"] - 5.) < 1e-12
+    assert bench.phase_summary(None, timers) is None
+
+
+def test_cpu_extrapolation_formula():
+    """The CPU baseline's seconds per pair: outer x (sum of count x slab seconds x cell-plane scale, the DST-I apply
+    counted at full size)."""
+    import bench
+    t = bench.CpuTable.__new__(bench.CpuTable)
+    t.outer, t.scale = 10, 4.
+    t.t = {k: 1. for k in bench.PER_OUTER}
+    per_outer = sum(bench.PER_OUTER[k] * (1. if k == "direction" else 4.) for k in bench.PER_OUTER)
+    assert abs(t.seconds_per_pair() - 10 * per_outer) < 1e-9
 
 
 def test_grid_ids_equal_the_reference():
