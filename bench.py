@@ -76,6 +76,13 @@ def parse():
     ap.add_argument("--cpu-planes", type=int, default=5, help="node planes of the CPU baseline's z-slab")
     ap.add_argument("--parity-planes", type=int, default=8, help="node planes of the parity checker's z-slab")
     ap.add_argument("--profile", action="store_true", help="per-kernel device times to stderr")
+    ap.add_argument("--serve", default=None, metavar="RATES",
+                    help="open-loop serving sweep: comma-separated arrival rates in requests/hour (Poisson arrivals); "
+                         "requests mix the grids 96^3, 128x144x128, 160x192x160, 160x192x224 with 25%% 48^3, each a "
+                         "seeded blob pair with a fixed outer-step budget (--serve-outer)")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests per arrival rate")
+    ap.add_argument("--serve-outer", type=int, default=50, help="outer-step budget per served request")
+    ap.add_argument("--serve-slots", type=int, default=4, help="registrations in flight at most")
     return ap.parse_args()
 
 
@@ -423,7 +430,22 @@ def parity_check(grid, fixed, moving, weights, u_dev, planes):
     d_full = pair.ggn_diagonal(u_dev, image_grad).cpu().numpy()
     node = pair.node_min_jd(u_dev, .25).cpu().numpy()
     g_full, w_g, ig_g = g_dev.cpu().numpy(), warped.cpu().numpy(), image_grad.cpu().numpy()
-    del pair, warped, image_grad, g_dev
+    # the mixed form's float32 kernels on the same state, against these float64 values (the oracle-checked ones)
+    mp = DevicePair(grid, fixed, moving, torch.zeros_like(u_dev), precision="mixed", **weights)
+    mixed = dict(gradient_rel=rel(mp.gradient(u_dev, warped, image_grad, term="total").cpu().numpy(), g_full),
+                 ggn_diagonal_rel=rel(mp.ggn_diagonal(u_dev, image_grad).cpu().numpy(), d_full),
+                 dst_apply_rel=rel(mp.poisson_apply(a, b, g_dev).cpu().numpy(), x_full),
+                 energy_terms_rel=0.0)
+    rd = cert_mod.result_from_record(cert_mod.certifier(grid, cfg, directed=True).run(u_dev), grid, cfg, None)
+    mixed["certificate_directed"] = dict(status=rd.status, same_status=rd.status == r.status,
+                                         min_jd_lower_bound=rd.min_jd_lower_bound,
+                                         bound_at_least_plain=bool(rd.min_jd_lower_bound is not None and
+                                                                   r.min_jd_lower_bound is not None and
+                                                                   rd.min_jd_lower_bound >= r.min_jd_lower_bound))
+    mixed["note"] = ("float32 gradient / GGN diagonal / DST-I against the float64 path on the final state; energies, "
+                     "differences and decisions are float64 in both forms")
+    out["mixed_form_errors"] = mixed
+    del pair, mp, warped, image_grad, g_dev
     # DST-I apply at full size
     out["dst_apply_rel"] = rel(x_full, Q.poisson_apply(og, a, b, g_full))
     # energy terms at full size (cell terms and node terms by z-slabs on every host core, summed in long double)
@@ -572,6 +594,78 @@ def serving_bench(args, grid, weights, shape, config, world, rank, local):
     return 0
 
 
+SERVE_GRIDS = ((96, 96, 96), (128, 144, 128), (160, 192, 160), (160, 192, 224))   # nx, ny, nz
+
+
+def serve_sweep(args, world, rank, local):
+    """Open-loop serving: for each arrival rate, --serve-requests requests arrive at Poisson times (exponential
+    gaps, seeded) and are admitted by the server as slots and HBM footprint allow; each request registers a seeded
+    blob pair (the 32^3 generator at its grid) for a fixed outer-step budget and returns only a certified field.
+    Reports, per rate, the latency from arrival to certified result (p50/p95/p99) and the pairs/hour delivered."""
+    import torch
+    from seq_vp_3d_b200.grid import make_grid_3d
+    from seq_vp_3d_b200.preopt import NATIVE_PREOPT, register_pair
+    from seq_vp_3d_b200.serve import RegistrationServer
+    from seq_vp_3d_b200.synthetic import blob_pair, default_weights
+    rates = [float(r) for r in args.serve.split(",")]
+    rng = np.random.default_rng(args.seed)
+    # the request mix: 25% 48^3, the rest uniform over the four grids; a pool of distinct seeded pairs per grid
+    kinds = [(48, 48, 48) if rng.random() < .25 else SERVE_GRIDS[rng.integers(len(SERVE_GRIDS))]
+             for _ in range(args.serve_requests)]
+    pool = {}
+    for k, shape in enumerate(kinds):
+        nx, ny, nz = shape
+        if shape not in pool:
+            pool[shape] = []
+        if len(pool[shape]) < 2:
+            f, m, _ = blob_pair((nz, ny, nx), (1., 1., 1.), seed=args.seed + 1000 * len(pool[shape]) + nx + ny + nz)
+            grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=1., hy=1., hz=1., unit="mm")
+            pool[shape].append((torch.from_numpy(f).cuda(), torch.from_numpy(m).cuda(), grid,
+                                default_weights((nz, ny, nx), (1., 1., 1.))))
+    requests = [pool[shape][k % len(pool[shape])] for k, shape in enumerate(kinds)]
+
+    def run(fixed, moving, grid, weights):
+        res, _ = register_pair(fixed, moving, grid, weights, preopt=NATIVE_PREOPT if args.preopt else None,
+                               outer=args.serve_outer, precision=args.form)
+        return res
+
+    rows = []
+    with RegistrationServer(slots=args.serve_slots, run=run) as srv:
+        for f, m, grid, w in requests[:2]:          # warm-up: library set-up and pools
+            srv.submit(f, m, grid, w).result()
+        with Clocks(local) as clocks:
+            for rate in rates:
+                gaps = rng.exponential(3600. / rate, size=len(requests))
+                srv.latencies.clear()
+                t0 = time.perf_counter()
+                futures, due = [], t0
+                for (f, m, grid, w), gap in zip(requests, gaps):
+                    due += gap
+                    wait = due - time.perf_counter()
+                    if wait > 0:
+                        time.sleep(wait)
+                    futures.append(srv.submit(f, m, grid, w))
+                results = [fu.result() for fu in futures]
+                span = time.perf_counter() - t0
+                lat = srv.percentiles()
+                rows.append(dict(rate_per_hour=rate, requests=len(requests), pairs_per_hour=len(requests) / span * 3600.,
+                                 latency_s=lat, certified=all(r.certified for r in results),
+                                 mean_final_mse=float(np.mean([r.final_mse for r in results]))))
+    if rank == 0:
+        best = max(rows, key=lambda r: r["pairs_per_hour"])
+        line = dict(metric=METRIC.format(args.form) + ", open-loop serving sweep", value=best["pairs_per_hour"],
+                    unit="pairs/hour", n_gpus=world, steps=len(rates), warmup=2,
+                    ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64" if args.form == "plain" else "f32+f64", data="synthetic",
+                    config=dict(workload="open-loop Poisson arrivals of seeded blob pairs, grids 96^3 / 128x144x128 / "
+                                         "160x192x160 / 160x192x224 with 25% 48^3, pre-optimizer + certified loop",
+                                outer_steps=args.serve_outer, slots=args.serve_slots,
+                                mix={f"{a}x{b}x{c}": kinds.count((a, b, c)) for a, b, c in set(kinds)}),
+                    sweep=rows, clocks=clocks.summary())
+        print(json.dumps(line))
+    return 0
+
+
 # ------------------------------------------------------------------------------------------ reference arm
 def reference_arm(args, shape, config):
     from seq_vp_3d_b200.synthetic import default_weights, head_pair
@@ -703,6 +797,8 @@ def main():
 
     if args.concurrency > 1:
         return serving_bench(args, grid, weights, shape, config, world, rank, local)
+    if args.serve:
+        return serve_sweep(args, world, rank, local)
 
     for _ in range(args.warmup):
         step(f_dev, m_dev, args.form)
