@@ -128,6 +128,28 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// The mixed form's passes: float32 operands on the tensor cores as 3xTF32 (mma.sync m16n8k8 .tf32, float32
+// accumulate).  Each operand x splits into big = tf32(x) and small = tf32(x - big); the product sums
+// small*big + big*small + big*big, which keeps float32-level accuracy (the small*small term is below float32
+// rounding).  Fragment layout of m16n8k8 (lane: gid = lane / 4, tig = lane % 4): A a0 = A[gid][tig],
+// a1 = A[gid + 8][tig], a2 = A[gid][tig + 4], a3 = A[gid + 8][tig + 4]; B b0 = B[tig][gid], b1 = B[tig + 4][gid];
+// D d0, d1 = D[gid][2 tig + {0, 1}], d2, d3 = D[gid + 8][2 tig + {0, 1}].
+__device__ __forceinline__ unsigned tf32_of(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void tf32_split(float x, unsigned &big, unsigned &small) {
+    big = tf32_of(x);
+    small = tf32_of(x - __uint_as_float(big));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 // TC: the arithmetic type of a pass (double in the plain form, float in the mixed form); inputs and outputs may be
 // either (the mixed form reads the float64 right-hand side and writes the float64 direction).
 template <class TC>
@@ -136,11 +158,12 @@ struct HalfDstT {
     int n, k0, k1;     // n, ceil(n/2), floor(n/2)
 };
 using HalfDst = HalfDstT<double>;
-// Tile product of one K block held in shared memory: FP64 tensor path (8 warps x 16 x 32 outputs as 2 x 4 DMMA
-// tiles; A fragments from sA[k][row], B from sB[k][col]) or, for float, 256 threads x 4 x 4 FMA outputs.
+// Tile product of one K block held in shared memory, 8 warps x 16 x 32 outputs (A fragments from sA[k][row], B
+// from sB[k][col]): FP64 tensor path (2 x 4 DMMA 8x8x4 tiles per warp) or, for float, 3xTF32 (4 m16n8k8 tiles per
+// warp, facc[fc] holding rows gid and gid + 8 of n-tile fc).
 template <class TC>
 __device__ __forceinline__ void tile_product(const TC (*sA)[TM + 4], const TC (*sB)[TN + 4], int lane, int warp,
-                                             double (&dacc)[2][4][2], TC (&acc)[4][4]) {
+                                             double (&dacc)[2][4][2], float (&facc)[4][4]) {
     if constexpr (sizeof(TC) == 8) {
         const int gid = lane >> 2, tig = lane & 3;
         const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
@@ -157,18 +180,24 @@ __device__ __forceinline__ void tile_product(const TC (*sA)[TM + 4], const TC (*
                 for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
         }
     } else {
-        const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+        const int gid = lane >> 2, tig = lane & 3;
+        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
 #pragma unroll
-        for (int kk = 0; kk < TK; kk++) {
-            TC a[4], x[4];
+        for (int kb = 0; kb < TK; kb += 8) {
+            unsigned ab[4], as[4];
+            tf32_split(sA[kb + tig][wr + gid], ab[0], as[0]);
+            tf32_split(sA[kb + tig][wr + gid + 8], ab[1], as[1]);
+            tf32_split(sA[kb + tig + 4][wr + gid], ab[2], as[2]);
+            tf32_split(sA[kb + tig + 4][wr + gid + 8], ab[3], as[3]);
 #pragma unroll
-            for (int r = 0; r < 4; r++) a[r] = sA[kk][ty + 16 * r];
-#pragma unroll
-            for (int c = 0; c < 4; c++) x[c] = sB[kk][tx + 16 * c];
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], x[c], acc[r][c]);
+            for (int fc = 0; fc < 4; fc++) {
+                unsigned b0b, b0s, b1b, b1s;
+                tf32_split(sB[kb + tig][wc + 8 * fc + gid], b0b, b0s);
+                tf32_split(sB[kb + tig + 4][wc + 8 * fc + gid], b1b, b1s);
+                mma_tf32(facc[fc], as, b0b, b1b);
+                mma_tf32(facc[fc], ab, b0s, b1s);
+                mma_tf32(facc[fc], ab, b0b, b1b);
+            }
         }
     }
 }
@@ -193,7 +222,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
                                                        const double *__restrict__ post, double sign) {
     __shared__ TC sM[2][TK][TM + 4];
     __shared__ TC sX[2][TK][TN + 4];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+
     constexpr bool kTensor = sizeof(TC) == 8;    // float64 passes on the FP64 tensor path
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
     const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;   // a warp's 16 x 32 block of the 64 x 64 tile
@@ -206,7 +235,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
     const long long b = blockIdx.z;
     const long long w0 = (long long)blockIdx.y * TN;
     const TI *Xb = X + b * bs;
-    TC acc[4][4] = {};
+    float facc[4][4] = {};
     TC rm[4];
     double ra[4], rb[4];
     auto fetch = [&](int k0) {
@@ -240,7 +269,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
     for (int k0 = 0; k0 < K; k0 += TK) {
         const bool more = k0 + TK < K;
         if (more) fetch(k0 + TK);
-        tile_product<TC>(sM[buf], sX[buf], lane, warp, dacc, acc);
+        tile_product<TC>(sM[buf], sX[buf], lane, warp, dacc, facc);
         if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
         buf ^= 1;
@@ -263,10 +292,138 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
                     store(i0 + wr + 8 * fr + gid, w0 + wc + 8 * fc + 2 * tig + e, dacc[fr][fc][e]);
     } else {
 #pragma unroll
-        for (int r = 0; r < 4; r++)
+        for (int fc = 0; fc < 4; fc++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) store(i0 + ty + 16 * r, w0 + tx + 16 * c, (double)acc[r][c]);
+            for (int e = 0; e < 4; e++)
+                store(i0 + wr + gid + 8 * (e >> 1), w0 + wc + 8 * fc + 2 * tig + (e & 1), (double)facc[fc][e]);
     }
+}
+
+// ---------------------------------------------------------------------------------- float64 left pass, pipelined
+// The float64 left pass (y and z axes) with a 3-stage asynchronous copy pipeline: each K block's operands go
+// straight from global to shared memory (cp.async, 8-byte copies, zero-filled outside the operand) two blocks ahead
+// of the block being multiplied, so the loads of blocks k + 1 and k + 2 are in flight during the DMMA of block k.
+// The raw input rows k and n - 1 - k are staged and folded when the B fragments are read (x_k, x_k + x_m or x_k - x_m
+// formed in float64 exactly as fold_value forms them).  Same products in the same order as dst_left_kernel<double>,
+// so the outputs are bitwise those of the register-prefetch form.
+constexpr int kStages = 3;
+constexpr int kPadH = TK + 1;      // H tile rows (i) of TK doubles, padded
+constexpr int kPadX = TN + 4;      // X tile rows (k) of TN doubles, padded
+constexpr size_t kLeftAsyncSmem = sizeof(double) * kStages * ((size_t)TM * kPadH + 2 * (size_t)TK * kPadX);
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+template <int EPI>
+__global__ void __launch_bounds__(256) dst_left_async_kernel(HalfDst D, const double *__restrict__ X, long long W,
+                                                             long long ldx, long long bs, double *__restrict__ C,
+                                                             const double *__restrict__ den, long long per,
+                                                             const double *__restrict__ post, double sign) {
+    extern __shared__ double dyn[];
+    double *sH = dyn;                                         // [kStages][TM][kPadH]
+    double *sXa = sH + kStages * TM * kPadH;                  // [kStages][TK][kPadX] rows k
+    double *sXb = sXa + kStages * TK * kPadX;                 // [kStages][TK][kPadX] rows n - 1 - k
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+    double dacc[2][4][2] = {};
+    const int t0 = (D.k0 + TM - 1) / TM;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
+    const int rows = g ? D.k1 : D.k0, K = rows;
+    const double *H = g ? D.h1 : D.h0;
+    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
+    const long long b = blockIdx.z;
+    const long long w0 = (long long)blockIdx.y * TN;
+    const double *Xb = X + b * bs;
+    const int nk = (K + TK - 1) / TK;
+    auto load = [&](int stage, int k0) {
+        double *h = sH + stage * TM * kPadH, *xa = sXa + stage * TK * kPadX, *xb = sXb + stage * TK * kPadX;
+#pragma unroll
+        for (int t = 0; t < 4; t++) {                         // H: 64 rows x 16 k
+            const int e = threadIdx.x + 256 * t, ii = e / TK, kk = e % TK, i = i0 + ii, k = k0 + kk;
+            const bool ok = i < rows && k < K;
+            cp_async8(h + ii * kPadH + kk, ok ? H + (long long)i * K + k : H, ok);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; t++) {                         // X rows k and n - 1 - k: 16 x 64 each
+            const int e = threadIdx.x + 256 * t, kk = e / TN, ww = e % TN, k = k0 + kk;
+            const long long w = w0 + ww;
+            const bool ok = k < K && w < W;
+            cp_async8(xa + kk * kPadX + ww, ok ? Xb + (long long)k * ldx + w : Xb, ok);
+            cp_async8(xb + kk * kPadX + ww, ok ? Xb + (long long)(D.n - 1 - k) * ldx + w : Xb, ok);
+        }
+    };
+#pragma unroll
+    for (int st = 0; st < kStages - 1; st++) {
+        if (st < nk) load(st, st * TK);
+        cp_async_commit();
+    }
+    for (int kb = 0; kb < nk; kb++) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        const int nxt = kb + kStages - 1;
+        if (nxt < nk) load(nxt % kStages, nxt * TK);
+        cp_async_commit();
+        const int st = kb % kStages, k0 = kb * TK;
+        const double *h = sH + st * TM * kPadH, *xa = sXa + st * TK * kPadX, *xb = sXb + st * TK * kPadX;
+#pragma unroll
+        for (int kq = 0; kq < TK; kq += 4) {
+            const int kk = kq + tig, k = k0 + kk;
+            const bool mid = k == D.n - 1 - k;
+            double a[2], x[4];
+#pragma unroll
+            for (int fr = 0; fr < 2; fr++) a[fr] = h[(wr + 8 * fr + gid) * kPadH + kk];
+#pragma unroll
+            for (int fc = 0; fc < 4; fc++) {
+                const int col = wc + 8 * fc + gid;
+                x[fc] = fold_value<double>(xa[kk * kPadX + col], xb[kk * kPadX + col], mid, g);
+            }
+#pragma unroll
+            for (int fr = 0; fr < 2; fr++)
+#pragma unroll
+                for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int fr = 0; fr < 2; fr++)
+#pragma unroll
+        for (int fc = 0; fc < 4; fc++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int ii = i0 + wr + 8 * fr + gid;
+                const long long w = w0 + wc + 8 * fc + 2 * tig + e;
+                if (ii >= rows || w >= W) continue;
+                const long long o = b * bs + (long long)(2 * ii + g) * ldx + w;
+                double v = dacc[fr][fc][e];
+                if (EPI == 1) v = v / den[o % per];
+                if (EPI == 2) v = sign * (post[o] * v);
+                C[o] = v;
+            }
+}
+
+// The pipelined pass needs more than the 48 KB default of dynamic shared memory; the attribute belongs to the
+// device's context and is set on the first call per device.
+int allow_left_async() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    SVP_CUDA(cudaGetDevice(&dev));
+    SVP_REQUIRE(dev >= 0 && dev < 64, "allow_left_async: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return SVP_OK;
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kLeftAsyncSmem));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kLeftAsyncSmem));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kLeftAsyncSmem));
+    done[dev] = true;
+    return SVP_OK;
 }
 
 // Right pass over contiguous rows of length n: C[r][i] = sum_k X[r][k] S[i][k]; pre (optional) scales X first.
@@ -275,7 +432,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
                                                         const double *__restrict__ pre, TO *__restrict__ C) {
     __shared__ TC sX[2][TK][TM + 4];
     __shared__ TC sM[2][TK][TN + 4];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+
     constexpr bool kTensor = sizeof(TC) == 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
     const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
@@ -287,7 +444,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
     const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
     const long long r0 = (long long)blockIdx.y * TM;
     const int n = D.n;
-    TC acc[4][4] = {};
+    float facc[4][4] = {};
     TC rm[4];
     double ra[4], rb[4];
     auto fetch = [&](int k0) {
@@ -322,7 +479,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
     for (int k0 = 0; k0 < K; k0 += TK) {
         const bool more = k0 + TK < K;
         if (more) fetch(k0 + TK);
-        tile_product<TC>(sX[buf], sM[buf], lane, warp, dacc, acc);
+        tile_product<TC>(sX[buf], sM[buf], lane, warp, dacc, facc);
         if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
         buf ^= 1;
@@ -340,15 +497,13 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
                 }
     } else {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            long long r = r0 + ty + 16 * q;
-            if (r >= R) continue;
+        for (int fc = 0; fc < 4; fc++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                int ii = i0 + tx + 16 * c;
-                if (ii < cols) C[r * n + 2 * ii + g] = (TO)acc[q][c];
+            for (int e = 0; e < 4; e++) {
+                const long long r = r0 + wr + gid + 8 * (e >> 1);
+                const int ii = i0 + wc + 8 * fc + 2 * tig + (e & 1);
+                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)facc[fc][e];
             }
-        }
     }
 }
 
@@ -419,6 +574,17 @@ static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const do
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
         dim3 grid(tiles, (unsigned)div_up(W, TN), (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
+        if constexpr (sizeof(TC) == 8 && sizeof(TI) == 8 && sizeof(TO) == 8) {
+            static_assert(kLeftAsyncSmem <= 227 * 1024, "left pass shared memory");
+            const size_t sm = kLeftAsyncSmem;
+            int rc = allow_left_async();
+            if (rc) return rc;
+            if (epi == 0) SVP_LAUNCH((dst_left_async_kernel<0><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_async_kernel<1><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_async_kernel<2><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+            SVP_LAUNCH_CHECK("dst pass");
+            return SVP_OK;
+        }
         if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
         else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
         else SVP_LAUNCH((dst_left_kernel<2, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
