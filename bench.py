@@ -60,8 +60,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--outer", type=int, default=200, help="outer steps per registration (config 2: 200)")
-    ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
-                    help="primary form: plain (float64 throughout) or mixed (float32 bulk, float64 decisions)")
+    ap.add_argument("--form", choices=("plain", "mixed"), default="mixed",
+                    help="primary form: mixed (float32 direction bulk on CUDA and tensor cores, float64 energies and "
+                         "decisions, directed-rounding certificate) or plain (float64 throughout, certificates "
+                         "bit-identical to the reference's); the other form is timed beside it (--compare-steps)")
     ap.add_argument("--compare-steps", type=int, default=3,
                     help="pairs of the other form timed for the mixed/plain ratio (0: skip)")
     ap.add_argument("--concurrency", type=int, default=1,

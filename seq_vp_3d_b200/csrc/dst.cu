@@ -299,133 +299,6 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
     }
 }
 
-// ---------------------------------------------------------------------------------- float64 left pass, pipelined
-// The float64 left pass (y and z axes) with a 3-stage asynchronous copy pipeline: each K block's operands go
-// straight from global to shared memory (cp.async, 8-byte copies, zero-filled outside the operand) two blocks ahead
-// of the block being multiplied, so the loads of blocks k + 1 and k + 2 are in flight during the DMMA of block k.
-// The raw input rows k and n - 1 - k are staged and folded when the B fragments are read (x_k, x_k + x_m or x_k - x_m
-// formed in float64 exactly as fold_value forms them).  Same products in the same order as dst_left_kernel<double>,
-// so the outputs are bitwise those of the register-prefetch form.
-constexpr int kStages = 3;
-constexpr int kPadH = TK + 1;      // H tile rows (i) of TK doubles, padded
-constexpr int kPadX = TN + 4;      // X tile rows (k) of TN doubles, padded
-constexpr size_t kLeftAsyncSmem = sizeof(double) * kStages * ((size_t)TM * kPadH + 2 * (size_t)TK * kPadX);
-
-__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool valid) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
-
-template <int EPI>
-__global__ void __launch_bounds__(256) dst_left_async_kernel(HalfDst D, const double *__restrict__ X, long long W,
-                                                             long long ldx, long long bs, double *__restrict__ C,
-                                                             const double *__restrict__ den, long long per,
-                                                             const double *__restrict__ post, double sign) {
-    extern __shared__ double dyn[];
-    double *sH = dyn;                                         // [kStages][TM][kPadH]
-    double *sXa = sH + kStages * TM * kPadH;                  // [kStages][TK][kPadX] rows k
-    double *sXb = sXa + kStages * TK * kPadX;                 // [kStages][TK][kPadX] rows n - 1 - k
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-    double dacc[2][4][2] = {};
-    const int t0 = (D.k0 + TM - 1) / TM;
-    const int g = (int)blockIdx.x < t0 ? 0 : 1;
-    const int rows = g ? D.k1 : D.k0, K = rows;
-    const double *H = g ? D.h1 : D.h0;
-    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
-    const long long b = blockIdx.z;
-    const long long w0 = (long long)blockIdx.y * TN;
-    const double *Xb = X + b * bs;
-    const int nk = (K + TK - 1) / TK;
-    auto load = [&](int stage, int k0) {
-        double *h = sH + stage * TM * kPadH, *xa = sXa + stage * TK * kPadX, *xb = sXb + stage * TK * kPadX;
-#pragma unroll
-        for (int t = 0; t < 4; t++) {                         // H: 64 rows x 16 k
-            const int e = threadIdx.x + 256 * t, ii = e / TK, kk = e % TK, i = i0 + ii, k = k0 + kk;
-            const bool ok = i < rows && k < K;
-            cp_async8(h + ii * kPadH + kk, ok ? H + (long long)i * K + k : H, ok);
-        }
-#pragma unroll
-        for (int t = 0; t < 4; t++) {                         // X rows k and n - 1 - k: 16 x 64 each
-            const int e = threadIdx.x + 256 * t, kk = e / TN, ww = e % TN, k = k0 + kk;
-            const long long w = w0 + ww;
-            const bool ok = k < K && w < W;
-            cp_async8(xa + kk * kPadX + ww, ok ? Xb + (long long)k * ldx + w : Xb, ok);
-            cp_async8(xb + kk * kPadX + ww, ok ? Xb + (long long)(D.n - 1 - k) * ldx + w : Xb, ok);
-        }
-    };
-#pragma unroll
-    for (int st = 0; st < kStages - 1; st++) {
-        if (st < nk) load(st, st * TK);
-        cp_async_commit();
-    }
-    for (int kb = 0; kb < nk; kb++) {
-        cp_async_wait<kStages - 2>();
-        __syncthreads();
-        const int nxt = kb + kStages - 1;
-        if (nxt < nk) load(nxt % kStages, nxt * TK);
-        cp_async_commit();
-        const int st = kb % kStages, k0 = kb * TK;
-        const double *h = sH + st * TM * kPadH, *xa = sXa + st * TK * kPadX, *xb = sXb + st * TK * kPadX;
-#pragma unroll
-        for (int kq = 0; kq < TK; kq += 4) {
-            const int kk = kq + tig, k = k0 + kk;
-            const bool mid = k == D.n - 1 - k;
-            double a[2], x[4];
-#pragma unroll
-            for (int fr = 0; fr < 2; fr++) a[fr] = h[(wr + 8 * fr + gid) * kPadH + kk];
-#pragma unroll
-            for (int fc = 0; fc < 4; fc++) {
-                const int col = wc + 8 * fc + gid;
-                x[fc] = fold_value<double>(xa[kk * kPadX + col], xb[kk * kPadX + col], mid, g);
-            }
-#pragma unroll
-            for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-                for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
-        }
-    }
-    cp_async_wait<0>();
-#pragma unroll
-    for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-        for (int fc = 0; fc < 4; fc++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int ii = i0 + wr + 8 * fr + gid;
-                const long long w = w0 + wc + 8 * fc + 2 * tig + e;
-                if (ii >= rows || w >= W) continue;
-                const long long o = b * bs + (long long)(2 * ii + g) * ldx + w;
-                double v = dacc[fr][fc][e];
-                if (EPI == 1) v = v / den[o % per];
-                if (EPI == 2) v = sign * (post[o] * v);
-                C[o] = v;
-            }
-}
-
-// The pipelined pass needs more than the 48 KB default of dynamic shared memory; the attribute belongs to the
-// device's context and is set on the first call per device.
-int allow_left_async() {
-    static std::mutex mu;
-    static bool done[64] = {};
-    int dev = 0;
-    SVP_CUDA(cudaGetDevice(&dev));
-    SVP_REQUIRE(dev >= 0 && dev < 64, "allow_left_async: device ordinal out of range");
-    std::lock_guard<std::mutex> lock(mu);
-    if (done[dev]) return SVP_OK;
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kLeftAsyncSmem));
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kLeftAsyncSmem));
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_async_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kLeftAsyncSmem));
-    done[dev] = true;
-    return SVP_OK;
-}
-
 // Right pass over contiguous rows of length n: C[r][i] = sum_k X[r][k] S[i][k]; pre (optional) scales X first.
 template <class TC, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long R,
@@ -574,17 +447,6 @@ static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const do
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
         dim3 grid(tiles, (unsigned)div_up(W, TN), (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
-        if constexpr (sizeof(TC) == 8 && sizeof(TI) == 8 && sizeof(TO) == 8) {
-            static_assert(kLeftAsyncSmem <= 227 * 1024, "left pass shared memory");
-            const size_t sm = kLeftAsyncSmem;
-            int rc = allow_left_async();
-            if (rc) return rc;
-            if (epi == 0) SVP_LAUNCH((dst_left_async_kernel<0><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
-            else if (epi == 1) SVP_LAUNCH((dst_left_async_kernel<1><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
-            else SVP_LAUNCH((dst_left_async_kernel<2><<<grid, 256, sm, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
-            SVP_LAUNCH_CHECK("dst pass");
-            return SVP_OK;
-        }
         if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
         else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
         else SVP_LAUNCH((dst_left_kernel<2, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
