@@ -429,16 +429,19 @@ __global__ void __launch_bounds__(256) gather_kernel(Q1Const q, GatherSpec g, co
         long long node = (z * q.ny + y) * q.nx + x;
         double qw = node_weight(x, y, z, q);
         double dimg = warped ? qw * (warped[node] - fixed[node]) : 0.;
-        double s1[3] = {0., 0., 0.}, s2[3] = {0., 0., 0.};
+        // the 8 cells' vertex values summed in the locals' type (float locals: one conversion per sum, not per term)
+        LT t1[3] = {LT(0), LT(0), LT(0)}, t2[3] = {LT(0), LT(0), LT(0)};
 #pragma unroll
         for (int a = 0; a < 8; a++) {
             long long c = ((z - (a >> 2)) * q.cy + (y - ((a >> 1) & 1))) * q.cx + (x - (a & 1));
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                if (L1) s1[r] += (double)L1[(long long)(a * 3 + r) * q.ncell + c];
-                if (L2) s2[r] += (double)L2[(long long)(a * 3 + r) * q.ncell + c];
+                if (L1) t1[r] += L1[(long long)(a * 3 + r) * q.ncell + c];
+                if (L2) t2[r] += L2[(long long)(a * 3 + r) * q.ncell + c];
             }
         }
+        const double s1[3] = {(double)t1[0], (double)t1[1], (double)t1[2]};
+        const double s2[3] = {(double)t2[0], (double)t2[1], (double)t2[2]};
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             double img = image_grad ? dimg * image_grad[3 * node + r] : 0.;
