@@ -256,6 +256,21 @@ int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *bas
                             uint8_t *trial_active, double *terms5, double *diff2, int64_t *barrier_violations,
                             void *stream);
 
+/* svp_trial_energy_active with the JD and curl penalties of the trial and of its differences evaluated in float32
+ * (the mixed form's float32 energy screen; the reference screens trial energies in float32 in its default execution,
+ * backends/accelerated.py:66-77).  The node terms (image, proximity), the localized barrier, its difference, the
+ * barrier violations and the activity mask are those of svp_trial_energy_active bit for bit (closed27 points whose
+ * float32 J comes within 1e-3 of the activation are evaluated in float64); terms5[2..3] and the JD/curl parts of
+ * diff2[0] carry float32 rounding.  band (host) receives an estimate of that error's magnitude: the residuals'
+ * absolute float32 errors (a Gauss-point J: 256 units of 2^-24, a curl component: 32) times the summed residual
+ * magnitudes, plus 64 units of relative rounding of both states' squared-residual sums.  The caller resolves a
+ * decision that falls within the band with svp_energy_difference_masked (float64) and checks the band against float64
+ * evaluations at run time.  diff2[1] (F = image + barrier) is exact as in the float64 call. */
+int svp_trial_energy_screened(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                              double *trial_warped, double *trial_image_grad, const uint8_t *base_active,
+                              uint8_t *trial_active, double *terms5, double *diff2, double *band,
+                              int64_t *barrier_violations, void *stream);
+
 /* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
 #define SVP_TERM_IMAGE 1
 #define SVP_TERM_PROXIMITY 2

@@ -83,6 +83,7 @@ SIGNATURES = {
     "svp_trial_energy": [P, P, P, P, P, P, P, P, P, P],
     "svp_trial_energy_masked": [P, P, P, P, P, P, P, P, P, P, P],
     "svp_trial_energy_active": [P, P, P, P, P, P, P, P, P, P, P, P],
+    "svp_trial_energy_screened": [P, P, P, P, P, P, P, P, P, P, P, P, P],
     "svp_gradient_masked": [P, P, P, P, ctypes.c_int32, P, P, P],
     "svp_outer_gradients_masked": [P, P, P, P, P, P, P, P, P],
     "svp_ggn_diagonal_masked": [P, P, P, P, P, P],

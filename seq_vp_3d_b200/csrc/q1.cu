@@ -1007,6 +1007,130 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
     if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
 }
 
+// ============================================================================================== screened trial
+// The mixed form's line-search trial: the JD and curl penalties at the Gauss points in float32 (reference J and curl
+// in a float slice, both fields' float edges), their per-cell sums in float and the block sums in double-double; the
+// localized barrier and its difference exactly as cell_trial_kernel forms them in float64 (every closed27 point whose
+// float32 J comes within kBarrierGuard of the activation is recomputed in float64; elsewhere J is above the
+// activation in both arithmetics, where the barrier and its difference vanish).  So the barrier sums, the violation
+// count and the activity mask are bitwise cell_trial_kernel's, and only the JD/curl sums carry float32 error, which
+// the host screens against a band (the reference's float32 energy screen, backends/accelerated.py:66-77).
+__device__ __forceinline__ void reference_points32(const double *__restrict__ uref, long long n0, const Q1Const &q,
+                                                   float *sl, int T) {
+    float Er[3][4][3];
+    load_edges_f32(uref, n0, q, Er);
+    sweep<false, float>(Er, q, [&](int p, int, int, int, const float (&Vr)[3][3]) {
+        float Cr[3];
+        curl_of(Vr, Cr);
+        sl[(4 * p) * T] = det_only(Vr);
+        sl[(4 * p + 1) * T] = Cr[0];
+        sl[(4 * p + 2) * T] = Cr[1];
+        sl[(4 * p + 3) * T] = Cr[2];
+    });
+}
+// J at closed27 point (ix, iy, iz) in float64 when the float32 value is within the guard of the activation; else
+// the float32 value (then J > activation in both arithmetics).
+__device__ __forceinline__ double closed_j_guarded(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
+                                                   int iy, int iz, float jf, float guard) {
+    if (!(jf < guard)) return (double)jf;
+    double V64[3][3];
+    closed_point_f64(u, n0, q, ix, iy, iz, V64);
+    return det_only(V64);
+}
+// pb (the screen's error-bound sums, per block): sum w (|ra| + |rb|) of the JD residuals, the same of the curl
+// residual components, sum w ra^2 and sum w |xa|^2 (the base's soft sums), all from the float32 residuals.
+__global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const double *__restrict__ ua,
+                                                          const double *__restrict__ ub,
+                                                          const double *__restrict__ uref, dd *pe, dd *pd, dd *pb,
+                                                          unsigned long long *bad, uint8_t *__restrict__ trial_act,
+                                                          const uint8_t *__restrict__ base_act) {
+    extern __shared__ double smem[];
+    const int T = blockDim.x;
+    // per thread: 108 floats (reference J and curl at the Gauss points), then 27 doubles (the trial's closed27 J);
+    // separate regions, each strided by the block size, so no thread's slots overlap another's
+    float *fsl = (float *)smem + threadIdx.x;
+    double *dsl = smem + 54 * T + threadIdx.x;
+    const float guard = (float)q.act + kBarrierGuard;
+    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}}, dif[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    dd bnd[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+    unsigned long long nbad = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long n0 = cell_node0(c, q);
+        reference_points32(uref, n0, q, fsl, T);
+        float Ea[3][4][3], Eb[3][4][3];
+        load_edges_f32(ua, n0, q, Ea);
+        load_edges_f32(ub, n0, q, Eb);
+        float sj = 0.f, sc = 0.f, dj = 0.f, dc = 0.f, mj = 0.f, mc = 0.f, aj = 0.f, ac = 0.f;
+        sweep2<false, float>(Ea, Eb, q, [&](int p, int, int, int, const float (&Va)[3][3], const float (&Vb)[3][3]) {
+            float Ca[3], Cb[3];
+            const float jr = fsl[(4 * p) * T];
+            const float ja = det_only(Va) - jr, jb = det_only(Vb) - jr;
+            curl_of(Va, Ca);
+            curl_of(Vb, Cb);
+            const float w = q.gwf[p];
+            float cb2 = 0.f, ca2 = 0.f, cd = 0.f, cm = 0.f;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float cr = fsl[(4 * p + 1 + r) * T];
+                const float xa = Ca[r] - cr, xb = Cb[r] - cr;
+                cb2 += xb * xb;
+                ca2 += xa * xa;
+                cd += (xb - xa) * (xb + xa);
+                cm += fabsf(xa) + fabsf(xb);
+            }
+            sj += w * jb * jb;
+            sc += w * cb2;
+            dj += w * ((jb - ja) * (jb + ja));
+            dc += w * cd;
+            mj += w * (fabsf(ja) + fabsf(jb));
+            mc += w * cm;
+            aj += w * ja * ja;
+            ac += w * ca2;
+        });
+        // the trial's closed27 sweep (float32 J, float64 where within the guard): barrier, violations, mask
+        bool active = false;
+        double sb = 0., sbd = 0.;
+        sweep<true, float>(Eb, q, [&](int p, int ix, int iy, int iz, const float (&Vb)[3][3]) {
+            const double jb = closed_j_guarded(ub, n0, q, ix, iy, iz, det_only(Vb), guard);
+            dsl[p * T] = jb;
+            active |= jb < q.act;
+            if (!(jb > q.delta)) { nbad++; return; }
+            if (jb < q.act) {
+                double b, b1, b2;
+                barrier_eval(jb, q.act, q.delta, q.bw, b, b1, b2);
+                sb += b;
+            }
+        });
+        if (active || !base_act || base_act[c]) {
+            sweep<true, float>(Ea, q, [&](int p, int ix, int iy, int iz, const float (&Va)[3][3]) {
+                const double ja = closed_j_guarded(ua, n0, q, ix, iy, iz, det_only(Va), guard), jb = dsl[p * T];
+                if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+            });
+        }
+        if (trial_act) trial_act[c] = active ? 1 : 0;
+        acc[0] = dd_add_d(acc[0], (double)sj);
+        acc[1] = dd_add_d(acc[1], (double)sc);
+        acc[2] = dd_add_d(acc[2], sb);
+        acc_add(dif[0], dd{.5 * q.mu * (double)dj, 0.});
+        acc_add(dif[1], dd{.5 * q.nu * (double)dc, 0.});
+        acc_add(dif[2], dd{q.bw * sbd, 0.});
+        bnd[0] = dd_add_d(bnd[0], (double)mj);
+        bnd[1] = dd_add_d(bnd[1], (double)mc);
+        bnd[2] = dd_add_d(bnd[2], (double)aj);
+        bnd[3] = dd_add_d(bnd[3], (double)ac);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) dif[k] = two_sum(dif[k].hi, dif[k].lo);
+    block_reduce_dd<3>(acc, pe);
+    __syncthreads();     // the reductions share block_reduce_dd's shared array
+    block_reduce_dd<3>(dif, pd);
+    __syncthreads();
+    block_reduce_dd<4>(bnd, pb);
+    for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
+}
+
 // ============================================================================================== node JD measure
 // ext_act > 0 (T69/T73): cells whose closed27 Bernstein coefficients allow a value below min(m_c, ext_act) are
 // appended to cand (order of arrival; each is then estimated independently, so the order does not matter).
@@ -1654,19 +1778,26 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
                                         stream);
 }
 
-extern "C" int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *base_warped,
-                                       const double *trial_u, double *trial_warped, double *trial_image_grad,
-                                       const uint8_t *base_active, uint8_t *trial_active, double *terms5,
-                                       double *diff2, int64_t *barrier_violations, void *stream) {
+// Absolute error estimates of float32 quantities in the screened trial, in units of the float32 unit roundoff
+// 2^-24: a Gauss-point J of I + V and its reference J (cofactor products and a 3-term dot product of entries of size
+// up to ~2, both rounded), a curl component (one rounded difference of each field's derivatives); and the relative
+// rounding of the squared-residual sums.
+constexpr double kScreenJ = 256., kScreenCurl = 32., kScreenSum = 64.;
+
+static int trial_energy(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
+                        double *trial_warped, double *trial_image_grad, const uint8_t *base_active,
+                        uint8_t *trial_active, double *terms5, double *diff2, int64_t *barrier_violations,
+                        bool screened, double *band, void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && terms5 && diff2,
                 "svp_trial_energy: null argument");
     cudaStream_t s = (cudaStream_t)stream;
     unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
-    int rc = pair_partials(p, (long long)nb * 4 + (long long)cb * 6, 1);
+    int rc = pair_partials(p, (long long)nb * 4 + (long long)cb * 10, 1);
     if (rc) return rc;
     if ((rc = allow_slices())) return rc;
     SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
     dd *pne = p->partial, *pnd = pne + (long long)nb * 2, *pce = pnd + (long long)nb * 2, *pcd = pce + (long long)cb * 3;
+    dd *pcb = pcd + (long long)cb * 3;
     SplineRef S = spline_ref(p);
     if (trial_image_grad) {
         svp::KernelTimer _t("warp_trial_kernel_grad", s);
@@ -1678,16 +1809,27 @@ extern "C" int svp_trial_energy_active(svp_pair *p, const double *base_u, const 
                                                                  p->u_ref, trial_warped, nullptr, pne, pnd));
     }
     SVP_LAUNCH_CHECK("warp_trial_kernel");
-    { svp::KernelTimer _t("cell_trial_kernel", s); SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter, trial_active, base_active)); }
+    if (screened) {
+        svp::KernelTimer _t("cell_trial32_kernel", s);
+        SVP_LAUNCH(cell_trial32_kernel<<<cb, CS, slice_bytes(81), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd,
+                                                                      pcb, (unsigned long long *)p->counter,
+                                                                      trial_active, base_active));
+    } else {
+        svp::KernelTimer _t("cell_trial_kernel", s);
+        SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd,
+                                                                     (unsigned long long *)p->counter, trial_active,
+                                                                     base_active));
+    }
     SVP_LAUNCH_CHECK("cell_trial_kernel");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pnd, nb, 2, p->result + 10));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 3, p->result + 14));
+    if (screened) SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcb, cb, 4, p->result + 20));
     SVP_LAUNCH_CHECK("final_reduce_kernel");
-    double tmp[20];
+    double tmp[28];
     long long bad = 0;
-    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof(double) * (screened ? 28 : 20), cudaMemcpyDeviceToHost, s));
     SVP_CUDA(cudaMemcpyAsync(&bad, p->counter, sizeof bad, cudaMemcpyDeviceToHost, s));
     SVP_CUDA(cudaStreamSynchronize(s));
     // energy terms exactly as svp_energy
@@ -1705,7 +1847,34 @@ extern "C" int svp_trial_energy_active(svp_pair *p, const double *base_u, const 
     double jd = tmp[14] + tmp[15], curl = tmp[16] + tmp[17], bar = tmp[18] + tmp[19];
     diff2[0] = (((img + prox) + jd) + curl) + bar;
     diff2[1] = img + bar;
+    if (band) {
+        // |error of diff2[0]| <= mu dJ sum w (|ra| + |rb|) + nu dC sum w (|xa| + |xb|) + 2 dS (soft_a + soft_b):
+        // the residuals' absolute errors times the summed residual magnitudes, plus the rounding of the squares
+        const double u32 = std::ldexp(1., -24);
+        *band = 0.;
+        if (screened) {
+            const double mj = tmp[20] + tmp[21], mc = tmp[22] + tmp[23], aj = tmp[24] + tmp[25], ac = tmp[26] + tmp[27];
+            const double soft = .5 * p->q.mu * (cell3[0] + aj) + .5 * p->q.nu * (cell3[1] + ac);
+            *band = p->q.mu * kScreenJ * u32 * mj + p->q.nu * kScreenCurl * u32 * mc + 2. * kScreenSum * u32 * soft;
+        }
+    }
     return SVP_OK;
+}
+
+extern "C" int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *base_warped,
+                                       const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                       const uint8_t *base_active, uint8_t *trial_active, double *terms5,
+                                       double *diff2, int64_t *barrier_violations, void *stream) {
+    return trial_energy(p, base_u, base_warped, trial_u, trial_warped, trial_image_grad, base_active, trial_active,
+                        terms5, diff2, barrier_violations, false, nullptr, stream);
+}
+
+extern "C" int svp_trial_energy_screened(svp_pair *p, const double *base_u, const double *base_warped,
+                                         const double *trial_u, double *trial_warped, double *trial_image_grad,
+                                         const uint8_t *base_active, uint8_t *trial_active, double *terms5,
+                                         double *diff2, double *band, int64_t *barrier_violations, void *stream) {
+    return trial_energy(p, base_u, base_warped, trial_u, trial_warped, trial_image_grad, base_active, trial_active,
+                        terms5, diff2, barrier_violations, true, band, stream);
 }
 
 extern "C" int svp_trial_energy_masked(svp_pair *p, const double *base_u, const double *base_warped,

@@ -121,6 +121,20 @@ class DevicePair:
                   ptr(base_active), ptr(act), t, d, ctypes.byref(bad), stream_ptr(stream))
         return w, g, np.array(t[:]), int(bad.value), (d[0], d[1]), act
 
+    def trial_energy_screened(self, base_u, base_w, trial_u, with_gradient=True, base_active=None, stream=None):
+        """trial_energy with the JD/curl penalties in float32 (the mixed form's energy screen): the same tuple plus
+        the error estimate of the E difference (the node terms, the barrier and F are the float64 call's bits)."""
+        w = self.node()
+        g = self.node(3) if with_gradient else None
+        act = self.cell_mask()
+        t = (ctypes.c_double * 5)()
+        d = (ctypes.c_double * 2)()
+        band = ctypes.c_double()
+        bad = ctypes.c_int64()
+        _lib.call("svp_trial_energy_screened", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(w), ptr(g),
+                  ptr(base_active), ptr(act), t, d, ctypes.byref(band), ctypes.byref(bad), stream_ptr(stream))
+        return w, g, np.array(t[:]), int(bad.value), (d[0], d[1]), act, band.value
+
     def gradient(self, u, warped, image_grad, term="total", out=None, active=None, stream=None):
         out = self.free() if out is None else out
         _lib.call("svp_gradient_masked", self._h, ptr(u), ptr(warped), ptr(image_grad), _lib.TERMS[term],

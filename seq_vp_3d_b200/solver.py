@@ -26,6 +26,11 @@ from .pair import DevicePair, Scalars, dot
 EPS = float(np.finfo(float).eps)
 InvalidTrial = namedtuple("InvalidTrial", "reason detail count")
 FAST_COSINE_SCREEN = 1e-6
+# the mixed form's float32 energy screen: runtime float64 checks (the first SCREEN_CHECKS screened evaluations and
+# every SCREEN_RECHECK-th) and the decision margin in bands
+SCREEN_CHECKS = 3
+SCREEN_RECHECK = 50
+SCREEN_MARGIN = 2.
 JD_AFFINE_FLOOR = 1e-12
 T62_POLICY = "image_shift_ggn_equilibrated_jd_affine_v1"
 T69_POLICY = "image_shift_ggn_equilibrated_jd_affine_v2"   # T62 + face/interior extension once a certificate was uncertain
@@ -76,6 +81,7 @@ class State:
     norms: tuple = None                # (GF, GD, GE) when computed with the final gradient
     differences: tuple = None          # ((base eval_id, reference version), (dE, dF)) from the one-pass trial
     active: object = None              # per-cell barrier activity mask (from the state's own trial evaluation)
+    band: float = 0.                   # error estimate of the screened (float32) dE in `differences`; 0: float64
 
     @property
     def total(self):
@@ -134,6 +140,12 @@ class Registration:
                                activation=activation, delta=self.delta, precision=precision)
         # the mixed form proves J > delta in the directed-rounding arithmetic (enclosures at least as tight)
         self.certifier = cert_mod.certifier(grid, self.config, directed=precision == "mixed")
+        # the mixed form's float32 energy screen of line-search trials (backends/accelerated.py:66-77 screens the
+        # same way): decisions within SCREEN_MARGIN bands of a threshold are taken on float64 differences, and the
+        # first SCREEN_CHECKS screened evaluations and every SCREEN_RECHECK-th are also evaluated in float64; one
+        # difference outside its band switches the screen off for this registration
+        self.screen = dict(on=precision == "mixed", evaluations=0, checks=0, band_hits=0, violations=0,
+                           max_error_over_band=0.)
         self.q_sum = grid.node_weight_total()
         self.length = float(np.linalg.norm([a[-1] - a[0] for a in grid.axes]))
         self._eval = 0
@@ -166,6 +178,9 @@ class Registration:
         if base is None:
             warped, _ = self.pair.warp(u)
             terms, bad = self.pair.energy(u, warped)
+        elif self.screen["on"]:
+            warped, grad, terms, bad, diff, active, band = self.pair.trial_energy_screened(base.u, base.warped, u,
+                                                                                           base_active=base.active)
         else:
             warped, grad, terms, bad, diff, active = self.pair.trial_energy(base.u, base.warped, u,
                                                                             base_active=base.active)
@@ -175,7 +190,29 @@ class Registration:
         state = State(theta, u, warped, terms, c, self._eval, image_grad=grad, active=active)
         if diff is not None:
             state.differences = ((base.eval_id, self._reference_version), diff)
+            if base is not None and self.screen["on"]:
+                state.band = band
+                self._screen_check(base, state)
         return state
+
+    def _screen_check(self, base, trial):
+        """Runtime check of the float32 screen on the first SCREEN_CHECKS evaluations and every SCREEN_RECHECK-th:
+        the float64 difference replaces the screened one, and a screened value outside its band ends screening."""
+        sc = self.screen
+        sc["evaluations"] += 1
+        k = sc["evaluations"]
+        if not (k <= SCREEN_CHECKS or k % SCREEN_RECHECK == 0):
+            return
+        sc["checks"] += 1
+        dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active, trial.active)
+        err = abs(trial.differences[1][0] - dE)
+        if trial.band > 0:
+            sc["max_error_over_band"] = max(sc["max_error_over_band"], err / trial.band)
+        if err > trial.band:
+            sc["violations"] += 1
+            sc["on"] = False
+        trial.differences = (trial.differences[0], (dE, dF))
+        trial.band = 0.
 
     def promote_trial(self, state):
         if state.image_grad is None:
@@ -212,16 +249,28 @@ class Registration:
             state.norms = (self.gnorm(gF), self.gnorm(gD), self.gnorm(gE))
         return state.norms
 
-    def stable_reductions(self, base, trial):
-        """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:135)."""
+    def stable_reductions(self, base, trial, required=None):
+        """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:135).  A screened (float32) E
+        difference is replaced by the float64 one when the decision it feeds -- certified = actual - resolution
+        against 0 and `required`, |actual| against the resolution -- lies within SCREEN_MARGIN bands."""
         cached = trial.differences
-        if cached is not None and cached[0] == (base.eval_id, self._reference_version):
+        use_cache = cached is not None and cached[0] == (base.eval_id, self._reference_version)
+        if use_cache:
             dE, dF = cached[1]
         else:
             dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active,
                                                  trial.active)
         rE = 16 * EPS * max(base.total, trial.total)
         rF = 16 * EPS * max(base.outer, trial.outer)
+        if use_cache and trial.band > 0:
+            actual, margin = -dE, SCREEN_MARGIN * trial.band
+            edges = (rE, -rE) + ((required + rE,) if required is not None else ())
+            if required is None or not np.isfinite(actual) or min(abs(actual - e) for e in edges) <= margin:
+                self.screen["band_hits"] += 1
+                dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active,
+                                                     trial.active)
+                trial.differences = (cached[0], (dE, dF))
+                trial.band = 0.
         return (-dE, rE), (-dF, rF)
 
     def step_ratio(self, candidate, theta):
@@ -505,7 +554,7 @@ def solve_pg(reg, base, *, target, config, memory, timings=None):
             if valid:
                 v = S.values()
                 relative = float(v[7] / max(reg.length, v[8]))
-                (actual, resolution), _ = reg.stable_reductions(base, trial)
+                (actual, resolution), _ = reg.stable_reductions(base, trial, required)
                 certified = actual - resolution
                 accepted = certified > 0 and certified >= required
                 reason = ("ACCEPTED" if accepted else "ENERGY_RESOLUTION" if abs(actual) <= resolution
@@ -584,6 +633,7 @@ def solve_sequential(reg, theta0=None, *, config=None, inner_config=None, budget
     small_steps = 0
 
     def done(status, reason):
+        counts["screen"] = dict(reg.screen)
         return SequentialResult(status, reason, initial, current, history, G0, GF, threshold, native, mse(current),
                                 counts, perf_counter() - started)
 

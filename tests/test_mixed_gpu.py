@@ -89,3 +89,26 @@ def test_mixed_solve_matches_plain_mse():
         assert res.certified
         out[form] = res.final_mse
     assert abs(out["mixed"] - out["plain"]) <= .01 * out["plain"], out
+
+
+def test_screened_trial(pairs):
+    """The mixed form's float32 energy screen (svp_trial_energy_screened) against the float64 one-pass trial on the
+    same base and trial (the fixture's barrier is active): warped image, image gradient, the image, proximity and
+    barrier terms, the violation count, the activity mask and the F difference are bitwise the float64 call's; the
+    JD and curl terms carry float32 rounding within 1e-5 relative, and the screened E difference lies within the
+    returned band of the float64 one (both directions: u1 -> u2 and u2 -> u1)."""
+    d, plain, mixed, u1, w1, g1 = pairs
+    u2 = torch.from_numpy(d["u2"]).cuda()
+    w2, _ = plain.warp(u2)
+    for (ua, wa, ub) in ((u1, w1, u2), (u2, w2, u1)):
+        ref = plain.trial_energy(ua, wa, ub)
+        got = plain.trial_energy_screened(ua, wa, ub)
+        assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[1]) and torch.equal(got[5], ref[5])
+        rt, gt = ref[2], got[2]
+        assert got[3] == ref[3]
+        assert rt[0] == gt[0] and rt[1] == gt[1] and rt[4] == gt[4]          # image, proximity, barrier
+        for k in (2, 3):                                                    # JD, curl
+            assert abs(gt[k] - rt[k]) <= 1e-5 * abs(rt[k]), (k, gt[k], rt[k])
+        assert got[4][1] == ref[4][1]                                       # F = image + barrier
+        band = got[6]
+        assert band > 0 and abs(got[4][0] - ref[4][0]) <= band, (got[4][0], ref[4][0], band)
