@@ -904,7 +904,7 @@ def main():
                     forms=compare, parity=parity,
                     result=dict(status=r.status, certified=bool(r.certified), outer_accepted=r.counts["outer_accepted"],
                                 trials=r.counts["trials"], native_mse=r.native_mse, final_mse=r.final_mse,
-                                GF_initial=r.GF_initial, GF_final=r.GF_final),
+                                GF_initial=r.GF_initial, GF_final=r.GF_final, screen=r.counts.get("screen")),
                     phases=phase_summary(timer_phase, timers))
         print(json.dumps(line))
     if world > 1:
