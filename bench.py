@@ -182,6 +182,8 @@ def kernel_counts(shape):
     return {
         # base u, trial u, u_ref: 24 B/node each
         "cell_trial_kernel": (3 * 24 * nn, c("cell_trial_kernel")),
+        # the mixed form's screened trial: the same fields in, float32 sweeps (the FLOP above are float32 there)
+        "cell_trial32_kernel": (3 * 24 * nn, None),
         "cell_diff_kernel": (3 * 24 * nn, c("cell_diff_kernel")),
         "cell_energy_kernel": (2 * 24 * nn, c("cell_energy_kernel")),
         # u, u_ref in; 24 doubles per cell out (one locals buffer; two for the outer triple)

@@ -258,9 +258,10 @@ int svp_trial_energy_active(svp_pair *p, const double *base_u, const double *bas
 
 /* svp_trial_energy_active with the JD and curl penalties of the trial and of its differences evaluated in float32
  * (the mixed form's float32 energy screen; the reference screens trial energies in float32 in its default execution,
- * backends/accelerated.py:66-77).  The node terms (image, proximity), the localized barrier, its difference, the
- * barrier violations and the activity mask are those of svp_trial_energy_active bit for bit (closed27 points whose
- * float32 J comes within 1e-3 of the activation are evaluated in float64); terms5[2..3] and the JD/curl parts of
+ * backends/accelerated.py:66-77).  The node terms (image, proximity), the barrier violations and the activity mask
+ * are those of svp_trial_energy_active bit for bit, the localized barrier and its difference equal within rounding
+ * (a cell with some float32 closed27 J within 1e-3 of the activation takes the float64 closed27 sweep); terms5[2..3]
+ * and the JD/curl parts of
  * diff2[0] carry float32 rounding.  band (host) receives an estimate of that error's magnitude: the residuals'
  * absolute float32 errors (a Gauss-point J: 256 units of 2^-24, a curl component: 32) times the summed residual
  * magnitudes, plus 64 units of relative rounding of both states' squared-residual sums.  The caller resolves a

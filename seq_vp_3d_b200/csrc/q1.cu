@@ -687,25 +687,33 @@ __global__ void __launch_bounds__(CS) cell_grad32_kernel(Q1Const q, const double
             scatter_slice(sl, T, q.gnf, q.gmf, q.ihf, L);
         }
         bool any = false;
-        // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term
+        // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term; a
+        // cell with some float32 J within the guard (or active in the mask) takes the float64 closed27 sweep whole:
+        // its edges loaded once, the barrier's J, b' and cofactors exactly as the float64 kernel forms them
         if (barrier && (!active || active[c])) {
-            zero_slice(sl, T, 81);
-            sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
-                if (!(det_only(V) < guard)) return;
-                double V64[3][3];
-                closed_point_f64(u, n0, q, ix, iy, iz, V64);
-                if (!(det_only(V64) < q.act)) return;
-                double A[3][3], J, b, b1, b2;
-                cofactor_det(V64, A, J);
-                barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-                float f[3][3];
+            bool near = active != nullptr;
+            if (!near)
+                sweep<true, float>(E, q, [&](int, int, int, int, const float (&V)[3][3]) {
+                    near |= det_only(V) < guard;
+                });
+            if (near) {
+                double E64[3][4][3];
+                load_edges(u, n0, q, E64);
+                zero_slice(sl, T, 81);
+                sweep<true>(E64, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
+                    if (!(det_only(V) < q.act)) return;
+                    double A[3][3], J, b, b1, b2;
+                    cofactor_det(V, A, J);
+                    barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+                    float f[3][3];
 #pragma unroll
-                for (int r = 0; r < 3; r++)
+                    for (int r = 0; r < 3; r++)
 #pragma unroll
-                    for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
-                add_flux(sl, T, ix, iy, iz, f);
-                any = true;
-            });
+                        for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
+                    add_flux(sl, T, ix, iy, iz, f);
+                    any = true;
+                });
+            }
         }
         float Lb[8][3];
 #pragma unroll
@@ -1028,15 +1036,6 @@ __device__ __forceinline__ void reference_points32(const double *__restrict__ ur
         sl[(4 * p + 3) * T] = Cr[2];
     });
 }
-// J at closed27 point (ix, iy, iz) in float64 when the float32 value is within the guard of the activation; else
-// the float32 value (then J > activation in both arithmetics).
-__device__ __forceinline__ double closed_j_guarded(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
-                                                   int iy, int iz, float jf, float guard) {
-    if (!(jf < guard)) return (double)jf;
-    double V64[3][3];
-    closed_point_f64(u, n0, q, ix, iy, iz, V64);
-    return det_only(V64);
-}
 // pb (the screen's error-bound sums, per block): sum w (|ra| + |rb|) of the JD residuals, the same of the curl
 // residual components, sum w ra^2 and sum w |xa|^2 (the base's soft sums), all from the float32 residuals.
 __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const double *__restrict__ ua,
@@ -1088,25 +1087,49 @@ __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const doubl
             aj += w * ja * ja;
             ac += w * ca2;
         });
-        // the trial's closed27 sweep (float32 J, float64 where within the guard): barrier, violations, mask
-        bool active = false;
+        // the trial's closed27 J: float32 first; a cell with some point within the guard takes the float64 sweep
+        // whole (the float64 kernel's values), whose J are kept for the differences; elsewhere every J is above the
+        // activation in both arithmetics (no barrier, no difference, no violation)
+        bool active = false, near_b = false;
         double sb = 0., sbd = 0.;
-        sweep<true, float>(Eb, q, [&](int p, int ix, int iy, int iz, const float (&Vb)[3][3]) {
-            const double jb = closed_j_guarded(ub, n0, q, ix, iy, iz, det_only(Vb), guard);
-            dsl[p * T] = jb;
-            active |= jb < q.act;
-            if (!(jb > q.delta)) { nbad++; return; }
-            if (jb < q.act) {
-                double b, b1, b2;
-                barrier_eval(jb, q.act, q.delta, q.bw, b, b1, b2);
-                sb += b;
-            }
+        sweep<true, float>(Eb, q, [&](int, int, int, int, const float (&Vb)[3][3]) {
+            near_b |= det_only(Vb) < guard;
         });
-        if (active || !base_act || base_act[c]) {
-            sweep<true, float>(Ea, q, [&](int p, int ix, int iy, int iz, const float (&Va)[3][3]) {
-                const double ja = closed_j_guarded(ua, n0, q, ix, iy, iz, det_only(Va), guard), jb = dsl[p * T];
-                if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+        if (near_b) {
+            double E64[3][4][3];
+            load_edges(ub, n0, q, E64);
+            sweep<true>(E64, q, [&](int p, int, int, int, const double (&Vb)[3][3]) {
+                const double jb = det_only(Vb);
+                dsl[p * T] = jb;
+                active |= jb < q.act;
+                if (!(jb > q.delta)) { nbad++; return; }
+                if (jb < q.act) {
+                    double b, b1, b2;
+                    barrier_eval(jb, q.act, q.delta, q.bw, b, b1, b2);
+                    sb += b;
+                }
             });
+        }
+        if (active || !base_act || base_act[c]) {
+            bool near_a = false;
+            sweep<true, float>(Ea, q, [&](int, int, int, int, const float (&Va)[3][3]) {
+                near_a |= det_only(Va) < guard;
+            });
+            if (near_a) {
+                double E64[3][4][3];
+                load_edges(ua, n0, q, E64);
+                sweep<true>(E64, q, [&](int p, int, int, int, const double (&Va)[3][3]) {
+                    // a trial J above the guard stands for "above the activation": min(J, a) is then a
+                    const double ja = det_only(Va), jb = near_b ? dsl[p * T] : (double)q.act;
+                    if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+                });
+            } else if (active) {
+                // the base is above the activation at every point: each difference is psi(jb) - psi(a)
+                for (int p = 0; p < 27; p++) {
+                    const double jb = dsl[p * T];
+                    if (jb < q.act) sbd += barrier_difference((double)q.act, jb, q.act, q.delta);
+                }
+            }
         }
         if (trial_act) trial_act[c] = active ? 1 : 0;
         acc[0] = dd_add_d(acc[0], (double)sj);
