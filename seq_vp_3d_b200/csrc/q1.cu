@@ -1018,11 +1018,11 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
 // ============================================================================================== screened trial
 // The mixed form's line-search trial: the JD and curl penalties at the Gauss points in float32 (reference J and curl
 // in a float slice, both fields' float edges), their per-cell sums in float and the block sums in double-double; the
-// localized barrier and its difference exactly as cell_trial_kernel forms them in float64 (every closed27 point whose
-// float32 J comes within kBarrierGuard of the activation is recomputed in float64; elsewhere J is above the
-// activation in both arithmetics, where the barrier and its difference vanish).  So the barrier sums, the violation
-// count and the activity mask are bitwise cell_trial_kernel's, and only the JD/curl sums carry float32 error, which
-// the host screens against a band (the reference's float32 energy screen, backends/accelerated.py:66-77).
+// localized barrier and its difference as cell_trial_kernel forms them in float64 (a cell with some float32 closed27 J
+// within kBarrierGuard of the activation takes the float64 closed27 sweep; elsewhere every J is above the activation
+// in both arithmetics, where the barrier and its difference vanish).  So the violation count and the activity mask
+// are cell_trial_kernel's, the barrier sums equal within rounding, and only the JD/curl sums carry float32 error,
+// which the host screens against a band (the reference's float32 energy screen, backends/accelerated.py:66-77).
 __device__ __forceinline__ void reference_points32(const double *__restrict__ uref, long long n0, const Q1Const &q,
                                                    float *sl, int T) {
     float Er[3][4][3];
