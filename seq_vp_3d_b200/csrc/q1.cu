@@ -196,21 +196,6 @@ __device__ __forceinline__ void load_edges(const double *__restrict__ u, long lo
     load_cell(u, n0, q, v);
     cell_edges(v, E);
 }
-// grad u at closed27 point (ix, iy, iz) of the cell in float64, as the plain form's sweep evaluates it
-__device__ __noinline__ void closed_point_f64(const double *__restrict__ u, long long n0, const Q1Const &q, int ix,
-                                              int iy, int iz, double V[3][3]) {
-    double E[3][4][3];
-    load_edges(u, n0, q, E);
-    const double nx = rule_n<true>(q, ix), mx = rule_m<true>(q, ix), ny = rule_n<true>(q, iy), my = rule_m<true>(q, iy);
-    const double nz = rule_n<true>(q, iz), mz = rule_m<true>(q, iz);
-    double X[3], Y[3], Z[3];
-    column<0>(E, my, ny, mz, nz, q.ih[0], X);
-    column<1>(E, mx, nx, mz, nz, q.ih[1], Y);
-    column<2>(E, mx, nx, my, ny, q.ih[2], Z);
-#pragma unroll
-    for (int r = 0; r < 3; r++) { V[r][0] = X[r]; V[r][1] = Y[r]; V[r][2] = Z[r]; }
-}
-
 template <class R>
 __device__ __forceinline__ void zero_slice(R *sl, int T, int n) {
     for (int k = 0; k < n; k++) sl[k * T] = R(0);
@@ -771,11 +756,15 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] += q.ggn_curlf[3 * a + r];
-        if (!active || active[c])
-        sweep<true, float>(E, q, [&](int, int ix, int iy, int iz, const float (&V)[3][3]) {
-            if (!(det_only(V) < guard)) return;
-            double V64[3][3];
-            closed_point_f64(u, n0, q, ix, iy, iz, V64);
+        // the barrier curvature in float64 over the whole closed27 sweep of a cell that is active in the mask (or,
+        // without a mask, has some float32 J within the guard): its edges loaded once
+        bool near = active ? active[c] != 0 : false;
+        if (!active)
+            sweep<true, float>(E, q, [&](int, int, int, int, const float (&V)[3][3]) { near |= det_only(V) < guard; });
+        if (near) {
+        double E64[3][4][3];
+        load_edges(u, n0, q, E64);
+        sweep<true>(E64, q, [&](int, int ix, int iy, int iz, const double (&V64)[3][3]) {
             if (!(det_only(V64) < q.act)) return;
             double A[3][3], J, b, b1, b2;
             cofactor_det(V64, A, J);
@@ -791,6 +780,7 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
                 }
             }
         });
+        }
         store_locals(L, c, q.ncell, out);
     }
 }
