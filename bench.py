@@ -162,6 +162,19 @@ FLOP_PER_CELL = {
     "cell_min_jd_kernel": 2009,
 }
 FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12     # nominal: 148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz
+# float32 operations per cell of the mixed form's cell kernels (the float64 barrier of the flagged cells runs in its
+# own kernels and is not counted here)
+FLOP32_PER_CELL = {
+    # edges 108 + reference sweep 1890 + Gauss sweep2 3780 + 27 x (2 det + 2 curl + 3 curl residual pairs
+    # (squares, stable change, magnitudes) + 8 weighted sums) 2700 + the trial's closed sweep 1350 + 27 x det 459
+    # (the base's closed sweep runs only where the base may be active: not counted)
+    "cell_trial32_kernel": 10287,
+    # edges 72 + soft sweep2 3780 + 27 x 94 (cofactor, det, curls, fluxes) + adjoint scatter 693
+    "cell_grad32_kernel": 7083,
+    # edges 36 + Gauss sweep 1350 + 27 x (cofactor 35 + 8 vertices x 30) + the curl constants 24
+    "cell_ggn_diag32_kernel": 8835,
+}
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12    # nominal: 148 SMs x 128 FP32 FMA/clk x 2 x 1965 MHz
 # DRAM bytes (read + write) per cell measured by ncu on the 160x192x96 pair (2,885,055 cells; profiles/
 # traffic_cell_trial_edge_hull_warp_160x192x96.md); scaled to a launch by the cells it processes (traffic grows with
 # the cell count: every launch streams its fields once, plus neighbour re-reads of the same order)
@@ -182,15 +195,15 @@ def kernel_counts(shape):
     return {
         # base u, trial u, u_ref: 24 B/node each
         "cell_trial_kernel": (3 * 24 * nn, c("cell_trial_kernel")),
-        # the mixed form's screened trial: the same fields in, float32 sweeps (the FLOP above are float32 there)
-        "cell_trial32_kernel": (3 * 24 * nn, None),
+        # the mixed form's screened trial: the same fields in, float32 sweeps; the barrier flags and the mask out
+        "cell_trial32_kernel": (3 * 24 * nn + 2 * nc, None),
         "cell_diff_kernel": (3 * 24 * nn, c("cell_diff_kernel")),
         "cell_energy_kernel": (2 * 24 * nn, c("cell_energy_kernel")),
         # u, u_ref in; 24 doubles per cell out (one locals buffer; two for the outer triple)
         "cell_grad_kernel": (2 * 24 * nn + 192 * nc, c("cell_grad_kernel")),
         "gather_kernel": (192 * nc + nn * (24 + 24 + 8 + 8 + 24) + 3 * 8 * nf, None),
         "cell_ggn_diag_kernel": (24 * nn + 192 * nc, c("cell_ggn_diag_kernel")),
-        # mixed form: the same float64 inputs, float32 locals out (the FLOP counts above are float32 operations here)
+        # mixed form: the same float64 inputs, float32 locals out
         "cell_grad32_kernel": (2 * 24 * nn + 96 * nc, None),
         "cell_ggn_diag32_kernel": (24 * nn + 96 * nc, None),
         "edge_hull_kernel": (24 * nn + 9 * nc, None),
@@ -212,7 +225,8 @@ def kernel_counts(shape):
 # kernels timed for the profile and the phase split only: their work depends on the state (the certificate stages
 # run on the cells the edge hull leaves unproven, the node-measure extension on candidate cells)
 STATE_DEPENDENT_KERNELS = ("prescreen_kernel", "fallback_grid_kernel", "classify_kernel", "jd_extension_kernel",
-                           "jd_root_kernel", "cell_ggn_hvp_kernel")
+                           "jd_root_kernel", "cell_ggn_hvp_kernel", "cell_trial_barrier_kernel",
+                           "cell_grad_barrier32_kernel", "cell_ggn_barrier32_kernel")
 
 
 def phase_summary(phase, timers):
@@ -879,6 +893,13 @@ def main():
                 roofline["fp64"] = dict(flop_per_launch=flop, achieved_tflops=flop / per_launch_s / 1e12,
                                         peak_tflops=FP64_PEAK_TFLOPS, frac=flop / per_launch_s / 1e12 / FP64_PEAK_TFLOPS,
                                         peak_source="nominal (148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz)")
+            if dominant in FLOP32_PER_CELL:
+                # the mixed form's float32 cell kernels: their counted float32 rate against the nominal FP32 peak
+                flop32 = FLOP32_PER_CELL[dominant] * ncell
+                roofline["fp32"] = dict(flop_per_launch=flop32, achieved_tflops=flop32 / per_launch_s / 1e12,
+                                        peak_tflops=FP32_PEAK_TFLOPS,
+                                        frac=flop32 / per_launch_s / 1e12 / FP32_PEAK_TFLOPS,
+                                        peak_source="nominal (148 SMs x 128 FP32 FMA/clk x 2 x 1965 MHz)")
         if args.profile:
             total = sum(v[1] for v in timers.values())
             for k, (c, ms) in sorted(timers.items(), key=lambda kv: -kv[1][1]):

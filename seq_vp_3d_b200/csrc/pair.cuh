@@ -21,6 +21,7 @@ struct svp_pair {
     double *result = nullptr;                 // small device result area (64 doubles)
     long long *counter = nullptr;             // small device counters (8)
     long long *cand = nullptr;                // candidate cells of the T69/T73 node JD extension (ncell)
+    uint8_t *flags = nullptr;                 // (ncell) cells the float32 cell kernels hand to the float64 barrier
     // DST-I Poisson metric
     double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
     int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)
@@ -35,4 +36,5 @@ struct svp_pair {
 namespace svp {
 int pair_partials(svp_pair *p, long long blocks, int k);
 int pair_locals(svp_pair *p, int n);
+int pair_flags(svp_pair *p);
 }  // namespace svp

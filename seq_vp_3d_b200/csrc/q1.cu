@@ -607,10 +607,57 @@ __global__ void __launch_bounds__(256) ggn_node_kernel(Q1Const q, const LT *__re
 // ============================================================================================== mixed form
 // The direction pipeline in float32 (gradient, GGN diagonal): edge differences formed in float64 from the float64
 // state and rounded once, grad u, cofactors, fluxes and the separable adjoint in float32, float32 locals gathered in
-// float64.  The localized barrier stays float64: wherever the float32 J of a closed27 point comes within
-// kBarrierGuard of the activation, that point's grad u is recomputed in float64 (bitwise the plain form's value) and
-// the barrier and its derivatives are evaluated there.
+// float64.  The localized barrier stays float64, in separate kernels that visit only the flagged cells: cells active
+// in the state's mask, or (without a mask) cells with some float32 closed27 J within kBarrierGuard of the
+// activation.  There the whole closed27 sweep is redone in float64 from the float64 state (the plain form's J,
+// cofactors and barrier values) and added to the cell's float32 locals, so the float32 kernels carry neither the
+// float64 sweep nor its registers.
 constexpr float kBarrierGuard = 1e-3f;
+constexpr int CB = 128;               // threads per block of the float64 barrier kernels
+constexpr int kFlagChunk = 256;       // consecutive cells a warp scans at a time for flagged cells
+
+// Calls f(c, flags[c]) for the flagged cells (flags[c] != 0).  Warp w of the grid scans the chunks of kFlagChunk
+// cells w, w + warps, ...; the flagged cells are queued in the warp's shared queue (64 entries) in cell order and
+// handed to the lanes 32 at a time, so the float64 work runs on full warps whatever the flags' pattern, and every cell
+// goes to the same lane on every run (the lanes' sums are deterministic).
+template <class F>
+__device__ __forceinline__ void for_flagged_cells(const Q1Const &q, const uint8_t *__restrict__ flags,
+                                                  long long *queue, F &&f) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long nchunk = (q.ncell + kFlagChunk - 1) / kFlagChunk;
+    long long k = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    long long b = k * kFlagChunk;
+    int qn = 0;
+    for (;;) {
+        // fill the queue to a full warp's worth, or until the warp's chunks are exhausted
+        while (qn < 32 && k < nchunk) {
+            const long long hi = min((k + 1) * kFlagChunk, q.ncell), c = b + lane;
+            const bool on = c < hi && flags[c] != 0;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, on);
+            if (on) queue[qn + __popc(m & ((1u << lane) - 1u))] = c;
+            qn += __popc(m);
+            b += 32;
+            if (b >= hi) {
+                k += warps;
+                b = k * kFlagChunk;
+            }
+        }
+        __syncwarp();
+        if (qn == 0) break;
+        const int take = qn < 32 ? qn : 32;
+        const long long c = lane < take ? queue[lane] : -1;
+        __syncwarp();
+        if (lane + 32 < qn) queue[lane] = queue[lane + 32];
+        __syncwarp();
+        qn -= take;
+        if (c >= 0) f(c, flags[c]);
+    }
+}
+unsigned barrier_blocks(const Q1Const &q) {
+    const long long nchunk = (q.ncell + kFlagChunk - 1) / kFlagChunk;
+    return blocks_for(nchunk * 32, CB, 4);
+}
 
 __device__ __forceinline__ void load_edges_f32(const double *__restrict__ u, long long n0, const Q1Const &q,
                                                float E[3][4][3]) {
@@ -625,15 +672,15 @@ __device__ __forceinline__ void load_edges_f32(const double *__restrict__ u, lon
 #pragma unroll
             for (int r = 0; r < 3; r++) E[j][e][r] = (float)E64[j][e][r];
 }
-__global__ void __launch_bounds__(CS) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
+// The soft part (JD, curl penalties) of the gradient locals; with split, L2 is zeroed for the barrier kernel.  flags
+// (when the state has no mask): 1 for the cells with some float32 closed27 J within the guard.
+__global__ void __launch_bounds__(CS, 8) cell_grad32_kernel(Q1Const q, const double *__restrict__ u,
                                                          const double *__restrict__ uref, double mu_scale,
-                                                         double nu_scale, bool barrier, bool split,
-                                                         float *__restrict__ L1, float *__restrict__ L2,
-                                                       const uint8_t *__restrict__ active) {
+                                                         double nu_scale, bool split, float *__restrict__ L1,
+                                                         float *__restrict__ L2, uint8_t *__restrict__ flags) {
     extern __shared__ float smemf[];
     float *sl = smemf + threadIdx.x;
     const int T = blockDim.x;
-    const float cn[3] = {0.f, .5f, 1.f}, cm[3] = {1.f, .5f, 0.f};
     const float mu = (float)(q.mu * mu_scale), nu = (float)(q.nu * nu_scale);
     const float guard = (float)q.act + kBarrierGuard;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
@@ -671,55 +718,73 @@ __global__ void __launch_bounds__(CS) cell_grad32_kernel(Q1Const q, const double
             });
             scatter_slice(sl, T, q.gnf, q.gmf, q.ihf, L);
         }
-        bool any = false;
-        // cells whose closed27 J are all above the activation (the state's activity mask) have no barrier term; a
-        // cell with some float32 J within the guard (or active in the mask) takes the float64 closed27 sweep whole:
-        // its edges loaded once, the barrier's J, b' and cofactors exactly as the float64 kernel forms them
-        if (barrier && (!active || active[c])) {
-            bool near = active != nullptr;
-            if (!near)
-                sweep<true, float>(E, q, [&](int, int, int, int, const float (&V)[3][3]) {
-                    near |= det_only(V) < guard;
-                });
-            if (near) {
-                double E64[3][4][3];
-                load_edges(u, n0, q, E64);
-                zero_slice(sl, T, 81);
-                sweep<true>(E64, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
-                    if (!(det_only(V) < q.act)) return;
-                    double A[3][3], J, b, b1, b2;
-                    cofactor_det(V, A, J);
-                    barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-                    float f[3][3];
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-#pragma unroll
-                        for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
-                    add_flux(sl, T, ix, iy, iz, f);
-                    any = true;
-                });
-            }
+        // without a mask, the cells with some float32 closed27 J within the guard are flagged for the barrier kernel
+        if (flags) {
+            bool near = false;
+            sweep<true, float>(E, q, [&](int, int, int, int, const float (&V)[3][3]) {
+                near |= det_only(V) < guard;
+            });
+            flags[c] = near ? 1 : 0;
         }
+        store_locals(L1, c, q.ncell, L);
+        if (split) {
+            float Z[8][3];
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) Z[a][r] = 0.f;
+            store_locals(L2, c, q.ncell, Z);
+        }
+    }
+}
+
+// The barrier's locals of the flagged cells in float64: the closed27 sweep from the float64 state, J, b' and the
+// cofactors exactly as the float64 kernel forms them, the flux rounded to float32 and scattered as the float32
+// kernel scatters its own; then added to the cell's locals (L1 += Lb) and, for the outer triple, stored apart (L2).
+__global__ void __launch_bounds__(CB) cell_grad_barrier32_kernel(Q1Const q, const double *__restrict__ u,
+                                                                 const uint8_t *__restrict__ flags, bool split,
+                                                                 float *__restrict__ L1, float *__restrict__ L2) {
+    extern __shared__ float smemf[];
+    __shared__ long long queue[CB / 32][64];
+    float *sl = smemf + threadIdx.x;
+    const int T = blockDim.x;
+    const float cn[3] = {0.f, .5f, 1.f}, cm[3] = {1.f, .5f, 0.f};
+    for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t) {
+        double E64[3][4][3];
+        load_edges(u, cell_node0(c, q), q, E64);
+        zero_slice(sl, T, 81);
+        bool any = false;
+        sweep<true>(E64, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
+            if (!(det_only(V) < q.act)) return;
+            double A[3][3], J, b, b1, b2;
+            cofactor_det(V, A, J);
+            barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
+            float f[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
+            add_flux(sl, T, ix, iy, iz, f);
+            any = true;
+        });
+        if (!any) return;
         float Lb[8][3];
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) Lb[a][r] = 0.f;
-        if (any) scatter_slice(sl, T, cn, cm, q.ihf, Lb);
+        scatter_slice(sl, T, cn, cm, q.ihf, Lb);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) L[a][r] += Lb[a][r];
-        store_locals(L1, c, q.ncell, L);
+            for (int r = 0; r < 3; r++) L1[(size_t)(3 * a + r) * q.ncell + c] += Lb[a][r];
         if (split) store_locals(L2, c, q.ncell, Lb);
-    }
+    });
 }
 
-// GGN diagonal contributions in float32 (Gauss JD/curl part); the closed27 barrier curvature b'' lc^2 in float64
-// at the points the guard selects (lc from the float64 cofactors).
-__global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const double *__restrict__ u,
-                                                             float *__restrict__ L,
-                                                           const uint8_t *__restrict__ active) {
+// GGN diagonal contributions in float32 (Gauss JD/curl part); flags (when the state has no mask) as the gradient's.
+__global__ void __launch_bounds__(CT, 4) cell_ggn_diag32_kernel(Q1Const q, const double *__restrict__ u,
+                                                             float *__restrict__ L, uint8_t *__restrict__ flags) {
     const float guard = (float)q.act + kBarrierGuard;
     const float mu = (float)q.mu;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
@@ -756,16 +821,33 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] += q.ggn_curlf[3 * a + r];
-        // the barrier curvature in float64 over the whole closed27 sweep of a cell that is active in the mask (or,
-        // without a mask, has some float32 J within the guard): its edges loaded once
-        bool near = active ? active[c] != 0 : false;
-        if (!active)
+        if (flags) {
+            bool near = false;
             sweep<true, float>(E, q, [&](int, int, int, int, const float (&V)[3][3]) { near |= det_only(V) < guard; });
-        if (near) {
+            flags[c] = near ? 1 : 0;
+        }
+        store_locals(L, c, q.ncell, out);
+    }
+}
+
+// The barrier curvature b'' lc^2 of the flagged cells in float64 (J, b'' and the cofactors lc from the float64
+// state), added point by point in sweep order to the cell's float32 locals.
+__global__ void __launch_bounds__(CB) cell_ggn_barrier32_kernel(Q1Const q, const double *__restrict__ u,
+                                                                const uint8_t *__restrict__ flags,
+                                                                float *__restrict__ L) {
+    __shared__ long long queue[CB / 32][64];
+    for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t) {
         double E64[3][4][3];
-        load_edges(u, n0, q, E64);
+        load_edges(u, cell_node0(c, q), q, E64);
+        float out[8][3];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out[a][r] = L[(size_t)(3 * a + r) * q.ncell + c];
+        bool any = false;
         sweep<true>(E64, q, [&](int, int ix, int iy, int iz, const double (&V64)[3][3]) {
             if (!(det_only(V64) < q.act)) return;
+            any = true;
             double A[3][3], J, b, b1, b2;
             cofactor_det(V64, A, J);
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
@@ -780,9 +862,8 @@ __global__ void __launch_bounds__(CT, 3) cell_ggn_diag32_kernel(Q1Const q, const
                 }
             }
         });
-        }
-        store_locals(L, c, q.ncell, out);
-    }
+        if (any) store_locals(L, c, q.ncell, out);
+    });
 }
 
 // ============================================================================================== stable differences
@@ -1026,23 +1107,23 @@ __device__ __forceinline__ void reference_points32(const double *__restrict__ ur
         sl[(4 * p + 3) * T] = Cr[2];
     });
 }
-// pb (the screen's error-bound sums, per block): sum w (|ra| + |rb|) of the JD residuals, the same of the curl
+// The soft part of the screened trial (JD and curl penalty sums and differences) in float32; the barrier part runs in
+// cell_trial_barrier_kernel over the cells this kernel flags.  pe, pd: per block, the two soft sums and their two
+// differences; pb (the screen's error-bound sums): sum w (|ra| + |rb|) of the JD residuals, the same of the curl
 // residual components, sum w ra^2 and sum w |xa|^2 (the base's soft sums), all from the float32 residuals.
 __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const double *__restrict__ ua,
                                                           const double *__restrict__ ub,
                                                           const double *__restrict__ uref, dd *pe, dd *pd, dd *pb,
-                                                          unsigned long long *bad, uint8_t *__restrict__ trial_act,
+                                                          uint8_t *__restrict__ flags,
+                                                          uint8_t *__restrict__ trial_act,
                                                           const uint8_t *__restrict__ base_act) {
-    extern __shared__ double smem[];
+    extern __shared__ float smemf[];
     const int T = blockDim.x;
-    // per thread: 108 floats (reference J and curl at the Gauss points), then 27 doubles (the trial's closed27 J);
-    // separate regions, each strided by the block size, so no thread's slots overlap another's
-    float *fsl = (float *)smem + threadIdx.x;
-    double *dsl = smem + 54 * T + threadIdx.x;
+    // per thread: 108 floats (reference J and curl at the Gauss points), strided by the block size
+    float *fsl = smemf + threadIdx.x;
     const float guard = (float)q.act + kBarrierGuard;
-    dd acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}}, dif[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    dd acc[2] = {{0., 0.}, {0., 0.}}, dif[2] = {{0., 0.}, {0., 0.}};
     dd bnd[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-    unsigned long long nbad = 0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         long long n0 = cell_node0(c, q);
@@ -1077,14 +1158,58 @@ __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const doubl
             aj += w * ja * ja;
             ac += w * ca2;
         });
-        // the trial's closed27 J: float32 first; a cell with some point within the guard takes the float64 sweep
-        // whole (the float64 kernel's values), whose J are kept for the differences; elsewhere every J is above the
-        // activation in both arithmetics (no barrier, no difference, no violation)
-        bool active = false, near_b = false;
-        double sb = 0., sbd = 0.;
+        // the closed27 J in float32: a cell with some trial point within the guard (bit 0), or some base point within
+        // the guard where the base may be active (bit 1), is flagged for the float64 barrier kernel; elsewhere every
+        // J is above the activation in both arithmetics (no barrier, no difference, no violation)
+        bool near_b = false, near_a = false;
         sweep<true, float>(Eb, q, [&](int, int, int, int, const float (&Vb)[3][3]) {
             near_b |= det_only(Vb) < guard;
         });
+        if (near_b || !base_act || base_act[c])
+            sweep<true, float>(Ea, q, [&](int, int, int, int, const float (&Va)[3][3]) {
+                near_a |= det_only(Va) < guard;
+            });
+        flags[c] = (near_b ? 1 : 0) | (near_a ? 2 : 0);
+        if (trial_act) trial_act[c] = 0;
+        acc[0] = dd_add_d(acc[0], (double)sj);
+        acc[1] = dd_add_d(acc[1], (double)sc);
+        acc_add(dif[0], dd{.5 * q.mu * (double)dj, 0.});
+        acc_add(dif[1], dd{.5 * q.nu * (double)dc, 0.});
+        bnd[0] = dd_add_d(bnd[0], (double)mj);
+        bnd[1] = dd_add_d(bnd[1], (double)mc);
+        bnd[2] = dd_add_d(bnd[2], (double)aj);
+        bnd[3] = dd_add_d(bnd[3], (double)ac);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++) dif[k] = two_sum(dif[k].hi, dif[k].lo);
+    block_reduce_dd<2>(acc, pe);
+    __syncthreads();     // the reductions share block_reduce_dd's shared array
+    block_reduce_dd<2>(dif, pd);
+    __syncthreads();
+    block_reduce_dd<4>(bnd, pb);
+}
+
+// The barrier part of the screened trial in float64 over the flagged cells, exactly as the float64 trial kernel forms
+// it per cell: the trial's closed27 sweep (barrier, violations, the trial's mask bit; its J kept in the thread's
+// shared slice), then the stable barrier differences against the base where the trial is active or the base may be.
+// pe, pd: per block, the barrier sum and the barrier difference sum.
+__global__ void __launch_bounds__(CB) cell_trial_barrier_kernel(Q1Const q, const double *__restrict__ ua,
+                                                                const double *__restrict__ ub,
+                                                                const uint8_t *__restrict__ flags, dd *pe, dd *pd,
+                                                                unsigned long long *bad,
+                                                                uint8_t *__restrict__ trial_act,
+                                                                const uint8_t *__restrict__ base_act) {
+    extern __shared__ double smem[];
+    __shared__ long long queue[CB / 32][64];
+    double *dsl = smem + threadIdx.x;
+    const int T = blockDim.x;
+    dd acc[1] = {{0., 0.}}, dif[1] = {{0., 0.}};
+    unsigned long long nbad = 0;
+    for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t flag) {
+        const long long n0 = cell_node0(c, q);
+        const bool near_b = flag & 1;
+        bool active = false;
+        double sb = 0., sbd = 0.;
         if (near_b) {
             double E64[3][4][3];
             load_edges(ub, n0, q, E64);
@@ -1101,11 +1226,7 @@ __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const doubl
             });
         }
         if (active || !base_act || base_act[c]) {
-            bool near_a = false;
-            sweep<true, float>(Ea, q, [&](int, int, int, int, const float (&Va)[3][3]) {
-                near_a |= det_only(Va) < guard;
-            });
-            if (near_a) {
+            if (flag & 2) {
                 double E64[3][4][3];
                 load_edges(ua, n0, q, E64);
                 sweep<true>(E64, q, [&](int p, int, int, int, const double (&Va)[3][3]) {
@@ -1121,25 +1242,14 @@ __global__ void __launch_bounds__(CS) cell_trial32_kernel(Q1Const q, const doubl
                 }
             }
         }
-        if (trial_act) trial_act[c] = active ? 1 : 0;
-        acc[0] = dd_add_d(acc[0], (double)sj);
-        acc[1] = dd_add_d(acc[1], (double)sc);
-        acc[2] = dd_add_d(acc[2], sb);
-        acc_add(dif[0], dd{.5 * q.mu * (double)dj, 0.});
-        acc_add(dif[1], dd{.5 * q.nu * (double)dc, 0.});
-        acc_add(dif[2], dd{q.bw * sbd, 0.});
-        bnd[0] = dd_add_d(bnd[0], (double)mj);
-        bnd[1] = dd_add_d(bnd[1], (double)mc);
-        bnd[2] = dd_add_d(bnd[2], (double)aj);
-        bnd[3] = dd_add_d(bnd[3], (double)ac);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; k++) dif[k] = two_sum(dif[k].hi, dif[k].lo);
-    block_reduce_dd<3>(acc, pe);
+        if (trial_act && active) trial_act[c] = 1;
+        acc[0] = dd_add_d(acc[0], sb);
+        acc_add(dif[0], dd{q.bw * sbd, 0.});
+    });
+    dif[0] = two_sum(dif[0].hi, dif[0].lo);
+    block_reduce_dd<1>(acc, pe);
     __syncthreads();     // the reductions share block_reduce_dd's shared array
-    block_reduce_dd<3>(dif, pd);
-    __syncthreads();
-    block_reduce_dd<4>(bnd, pb);
+    block_reduce_dd<1>(dif, pd);
     for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
     if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
 }
@@ -1685,6 +1795,11 @@ int pair_locals(svp_pair *p, int n) {
     return SVP_OK;
 }
 
+int pair_flags(svp_pair *p) {
+    if (!p->flags) SVP_CUDA(cudaMalloc((void **)&p->flags, (size_t)p->q.ncell));
+    return SVP_OK;
+}
+
 }  // namespace svp
 
 using namespace svp;
@@ -1804,13 +1919,14 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && terms5 && diff2,
                 "svp_trial_energy: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
-    int rc = pair_partials(p, (long long)nb * 4 + (long long)cb * 10, 1);
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p), bb = barrier_blocks(p->q);
+    int rc = pair_partials(p, (long long)nb * 4 + (long long)cb * 10 + (long long)bb * 2, 1);
     if (rc) return rc;
     if ((rc = allow_slices())) return rc;
+    if (screened && (rc = pair_flags(p))) return rc;
     SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
     dd *pne = p->partial, *pnd = pne + (long long)nb * 2, *pce = pnd + (long long)nb * 2, *pcd = pce + (long long)cb * 3;
-    dd *pcb = pcd + (long long)cb * 3;
+    dd *pcb = pcd + (long long)cb * 3, *pbe = pcb + (long long)cb * 4, *pbd = pbe + bb;
     SplineRef S = spline_ref(p);
     if (trial_image_grad) {
         svp::KernelTimer _t("warp_trial_kernel_grad", s);
@@ -1823,10 +1939,14 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
     }
     SVP_LAUNCH_CHECK("warp_trial_kernel");
     if (screened) {
-        svp::KernelTimer _t("cell_trial32_kernel", s);
-        SVP_LAUNCH(cell_trial32_kernel<<<cb, CS, slice_bytes(81), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd,
-                                                                      pcb, (unsigned long long *)p->counter,
-                                                                      trial_active, base_active));
+        {
+            svp::KernelTimer _t("cell_trial32_kernel", s);
+            SVP_LAUNCH(cell_trial32_kernel<<<cb, CS, sizeof(float) * 108 * CS, s>>>(
+                p->q, base_u, trial_u, p->u_ref, pce, pcd, pcb, p->flags, trial_active, base_active));
+        }
+        svp::KernelTimer _t("cell_trial_barrier_kernel", s);
+        SVP_LAUNCH(cell_trial_barrier_kernel<<<bb, CB, sizeof(double) * 27 * CB, s>>>(
+            p->q, base_u, trial_u, p->flags, pbe, pbd, (unsigned long long *)p->counter, trial_active, base_active));
     } else {
         svp::KernelTimer _t("cell_trial_kernel", s);
         SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd,
@@ -1835,10 +1955,18 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
     }
     SVP_LAUNCH_CHECK("cell_trial_kernel");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
-    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pnd, nb, 2, p->result + 10));
-    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 3, p->result + 14));
-    if (screened) SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcb, cb, 4, p->result + 20));
+    if (screened) {
+        // soft sums and differences from the float32 kernel, the barrier's from the float64 barrier kernel
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 2, p->result + 4));
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pbe, bb, 1, p->result + 8));
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 2, p->result + 14));
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pbd, bb, 1, p->result + 18));
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcb, cb, 4, p->result + 20));
+    } else {
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
+        SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 3, p->result + 14));
+    }
     SVP_LAUNCH_CHECK("final_reduce_kernel");
     double tmp[28];
     long long bad = 0;
@@ -1913,6 +2041,26 @@ static int run_gather(svp_pair *p, const GatherSpec &g, const LT *L1, const LT *
     return SVP_OK;
 }
 
+// The mixed form's gradient locals: the float32 soft kernel, then the float64 barrier kernel over the flagged cells
+// (the state's mask, or without one the cells the soft kernel flags from its float32 closed27 J).
+static int grad32(svp_pair *p, const double *u, double mu_scale, double nu_scale, bool barrier, bool split,
+                  const uint8_t *active, cudaStream_t s) {
+    int rc;
+    if (barrier && !active && (rc = pair_flags(p))) return rc;
+    uint8_t *flags = barrier && !active ? p->flags : nullptr;
+    {
+        svp::KernelTimer _t("cell_grad32_kernel", s);
+        SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(
+            p->q, u, p->u_ref, mu_scale, nu_scale, split, (float *)p->loc1, (float *)p->loc2, flags));
+    }
+    if (barrier) {
+        svp::KernelTimer _t("cell_grad_barrier32_kernel", s);
+        SVP_LAUNCH(cell_grad_barrier32_kernel<<<barrier_blocks(p->q), CB, sizeof(float) * 81 * CB, s>>>(
+            p->q, u, active ? active : flags, split, (float *)p->loc1, (float *)p->loc2));
+    }
+    return SVP_OK;
+}
+
 extern "C" int svp_gradient_masked(svp_pair *p, const double *u, const double *warped, const double *image_grad,
                                    int32_t terms, const uint8_t *active, double *out, void *stream) {
     SVP_REQUIRE(p && u && out, "svp_gradient: null argument");
@@ -1926,10 +2074,9 @@ extern "C" int svp_gradient_masked(svp_pair *p, const double *u, const double *w
         int rc = pair_locals(p, 1);
         if (rc) return rc;
         if (mixed) {
-            svp::KernelTimer _t("cell_grad32_kernel", s);
-            SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
-                                                       (terms & SVP_TERM_CURL) ? 1. : 0.,
-                                                       (terms & SVP_TERM_BARRIER) != 0, false, (float *)p->loc1, nullptr, active));
+            if ((rc = grad32(p, u, (terms & SVP_TERM_JD) ? 1. : 0., (terms & SVP_TERM_CURL) ? 1. : 0.,
+                             (terms & SVP_TERM_BARRIER) != 0, false, active, s)))
+                return rc;
         } else {
             svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
                                                        (terms & SVP_TERM_CURL) ? 1. : 0.,
@@ -1958,8 +2105,7 @@ extern "C" int svp_outer_gradients_masked(svp_pair *p, const double *u, const do
     if (rc) return rc;
     const bool mixed = p->precision == SVP_PRECISION_MIXED;
     if (mixed) {
-        svp::KernelTimer _t("cell_grad32_kernel", s);
-        SVP_LAUNCH(cell_grad32_kernel<<<slice_blocks(p), CS, sizeof(float) * 81 * CS, s>>>(p->q, u, p->u_ref, 1., 1., true, true, (float *)p->loc1, (float *)p->loc2, active));
+        if ((rc = grad32(p, u, 1., 1., true, true, active, s))) return rc;
     } else {
         svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2, active)); }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
@@ -1980,7 +2126,17 @@ extern "C" int svp_ggn_diagonal_masked(svp_pair *p, const double *u, const doubl
     int rc = pair_locals(p, 1);
     if (rc) return rc;
     if (p->precision == SVP_PRECISION_MIXED) {
-        { svp::KernelTimer _t("cell_ggn_diag32_kernel", s); SVP_LAUNCH(cell_ggn_diag32_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, (float *)p->loc1, active)); }
+        if (!active && (rc = pair_flags(p))) return rc;
+        {
+            svp::KernelTimer _t("cell_ggn_diag32_kernel", s);
+            SVP_LAUNCH(cell_ggn_diag32_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, (float *)p->loc1,
+                                                                           active ? nullptr : p->flags));
+        }
+        {
+            svp::KernelTimer _t("cell_ggn_barrier32_kernel", s);
+            SVP_LAUNCH(cell_ggn_barrier32_kernel<<<barrier_blocks(p->q), CB, 0, s>>>(
+                p->q, u, active ? active : p->flags, (float *)p->loc1));
+        }
         SVP_LAUNCH(ggn_node_kernel<float><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, (const float *)p->loc1, image_grad, nullptr, out));
     } else {
         { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1, active)); }
