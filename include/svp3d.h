@@ -271,6 +271,12 @@ int svp_trial_energy_screened(svp_pair *p, const double *base_u, const double *b
                               double *trial_warped, double *trial_image_grad, const uint8_t *base_active,
                               uint8_t *trial_active, double *terms5, double *diff2, double *band,
                               int64_t *barrier_violations, void *stream);
+/* The same screen for two evaluated states (energy_comparison.py:135 stable_energy_reductions, as the outer commit
+ * compares its start and candidate): diff2 as svp_energy_difference_masked with the JD and curl penalty differences
+ * in float32 and the band of diff2[0]; diff2[1] (F) is exact. */
+int svp_energy_difference_screened(svp_pair *p, const double *base_u, const double *base_warped,
+                                   const double *trial_u, const double *trial_warped, const uint8_t *base_active,
+                                   double *diff2, double *band, void *stream);
 
 /* Gradient terms mask (linearization.py:180 energy_gradient term selection). */
 #define SVP_TERM_IMAGE 1

@@ -88,6 +88,7 @@ SIGNATURES = {
     "svp_outer_gradients_masked": [P, P, P, P, P, P, P, P, P],
     "svp_ggn_diagonal_masked": [P, P, P, P, P, P],
     "svp_energy_difference_masked": [P, P, P, P, P, P, P, P, P],
+    "svp_energy_difference_screened": [P, P, P, P, P, P, P, P, P],
     "svp_pair_set_precision": [P, ctypes.c_int32],
     "svp_dot_dev": [P, P, I64, P, P],
     "svp_bb2_dots_dev": [P, P, P, P, P, P, I64, P, P],

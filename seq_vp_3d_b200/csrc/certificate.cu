@@ -10,8 +10,6 @@
 // This file is compiled with -fmad=false and uses explicit round-to-nearest intrinsics for every certificate
 // operation, so no product can be contracted into an FMA.
 #include <cuda.h>
-#include <cub/cub.cuh>
-#include <thrust/iterator/counting_iterator.h>
 
 #include <cmath>
 #include <cstring>
@@ -1190,8 +1188,8 @@ struct svp_certifier {
     int *tile_bad = nullptr, *tile_fail = nullptr;
     long long *list1 = nullptr, *list2 = nullptr, *list3 = nullptr, *counts = nullptr;
     svp::Accum *acc = nullptr;
-    void *cub_tmp = nullptr;
-    size_t cub_bytes = 0;
+    long long *sel_cnt = nullptr;    // per-block flag counts of the stage-list compaction
+    size_t sel_bytes = 0;
     // fallback workspace (grows on demand)
     long long fb_cap = 0;
     double *fb = nullptr;  // 5 * 27 * cap
@@ -1218,18 +1216,81 @@ int ensure_fallback(svp_certifier *c, long long n) {
     return SVP_OK;
 }
 
-template <class InIt>
-int select_flagged(svp_certifier *c, InIt in, const uint8_t *flags, long long *out, long long *count, long long n,
-                   cudaStream_t s) {
-    size_t need = 0;
-    SVP_CUDA(cub::DeviceSelect::Flagged(nullptr, need, in, flags, out, count, n, s));
-    if (need > c->cub_bytes) {
-        cudaFree(c->cub_tmp);
-        c->cub_tmp = nullptr;
-        SVP_CUDA(cudaMalloc(&c->cub_tmp, need));
-        c->cub_bytes = need;
+// Stage lists: the flagged entries of 0..n-1 (or of a previous list) in their order, in two launches with no
+// inter-block waiting.  Block b owns the contiguous chunk [b chunk, (b + 1) chunk); select_count_kernel counts its
+// flags, select_scatter_kernel sums the counts of the blocks before it and writes its flagged entries in order, a
+// 256-entry tile at a time (warp ballots, then the 8 warps' counts scanned in shared memory).  The last block writes
+// the total.
+constexpr int kSelThreads = 256;
+
+__global__ void __launch_bounds__(kSelThreads) select_count_kernel(const uint8_t *__restrict__ flags, long long n,
+                                                                 long long chunk, long long *__restrict__ cnt) {
+    const long long lo = blockIdx.x * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    int k = 0;
+    for (long long i = lo + threadIdx.x; i < hi; i += kSelThreads) k += flags[i] != 0;
+    for (int o = 16; o; o >>= 1) k += __shfl_xor_sync(0xFFFFFFFFu, k, o);
+    __shared__ int w[kSelThreads / 32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = k;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int j = 0; j < kSelThreads / 32; j++) t += w[j];
+        cnt[blockIdx.x] = t;
     }
-    SVP_CUDA(cub::DeviceSelect::Flagged(c->cub_tmp, c->cub_bytes, in, flags, out, count, n, s));
+}
+
+template <bool LIST>
+__global__ void __launch_bounds__(kSelThreads) select_scatter_kernel(const long long *__restrict__ list,
+                                                                   const uint8_t *__restrict__ flags, long long n,
+                                                                   long long chunk, const long long *__restrict__ cnt,
+                                                                   long long *__restrict__ out,
+                                                                   long long *__restrict__ count) {
+    __shared__ long long red[kSelThreads / 32];
+    __shared__ int wsum[kSelThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long before = 0;
+    for (long long j = threadIdx.x; j < blockIdx.x; j += kSelThreads) before += cnt[j];
+    for (int o = 16; o; o >>= 1) before += __shfl_xor_sync(0xFFFFFFFFu, before, o);
+    if (lane == 0) red[warp] = before;
+    __syncthreads();
+    long long off = 0;
+    for (int j = 0; j < kSelThreads / 32; j++) off += red[j];
+    const long long lo = blockIdx.x * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    for (long long t0 = lo; t0 < hi; t0 += kSelThreads) {
+        const long long i = t0 + threadIdx.x;
+        const bool on = i < hi && flags[i] != 0;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, on);
+        __syncthreads();     // the previous tile's reads of wsum are done
+        if (lane == 0) wsum[warp] = __popc(m);
+        __syncthreads();
+        int wo = 0, tot = 0;
+        for (int j = 0; j < kSelThreads / 32; j++) {
+            wo += j < warp ? wsum[j] : 0;
+            tot += wsum[j];
+        }
+        if (on) out[off + wo + __popc(m & ((1u << lane) - 1u))] = LIST ? list[i] : i;
+        off += tot;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *count = off;
+}
+
+template <bool LIST>
+int select_flagged(svp_certifier *c, const long long *list, const uint8_t *flags, long long *out, long long *count,
+                   long long n, cudaStream_t s) {
+    const long long blocks = n < 1 ? 1 : (long long)blocks_for(n, 8 * kSelThreads, 8);
+    const long long chunk = (div_up(n < 1 ? 1 : n, blocks) + kSelThreads - 1) / kSelThreads * kSelThreads;
+    const size_t need = sizeof(long long) * (size_t)blocks;
+    if (need > c->sel_bytes) {
+        cudaFree(c->sel_cnt);
+        c->sel_cnt = nullptr;
+        c->sel_bytes = 0;
+        SVP_CUDA(cudaMalloc((void **)&c->sel_cnt, need));
+        c->sel_bytes = need;
+    }
+    SVP_LAUNCH(select_count_kernel<<<(unsigned)blocks, kSelThreads, 0, s>>>(flags, n, chunk, c->sel_cnt));
+    SVP_LAUNCH(select_scatter_kernel<LIST><<<(unsigned)blocks, kSelThreads, 0, s>>>(list, flags, n, chunk,
+                                                                                   c->sel_cnt, out, count));
+    SVP_LAUNCH_CHECK("select_flagged");
     return SVP_OK;
 }
 
@@ -1285,7 +1346,7 @@ extern "C" int svp_certifier_destroy(svp_certifier *c) {
     if (!c) return SVP_OK;
     cudaFree(c->margin); cudaFree(c->lower); cudaFree(c->flag); cudaFree(c->sel);
     cudaFree(c->tile_bad); cudaFree(c->tile_fail); cudaFree(c->list1); cudaFree(c->list2); cudaFree(c->list3);
-    cudaFree(c->counts); cudaFree(c->acc); cudaFree(c->cub_tmp); cudaFree(c->fb); cudaFree(c->fb_ok);
+    cudaFree(c->counts); cudaFree(c->acc); cudaFree(c->sel_cnt); cudaFree(c->fb); cudaFree(c->fb_ok);
     cudaFree(c->verdicts); cudaFree(c->heap);
     delete c;
     return SVP_OK;
@@ -1333,7 +1394,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
     }
     SVP_LAUNCH(hull_stage_kernel<<<blocks_for(n, 256, 8), 256, 0, s>>>(c->margin, c->tile_bad, n, tile, c->sel, c->acc));
     SVP_LAUNCH_CHECK("hull stage");
-    int rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list1, c->counts, n, s);
+    int rc = select_flagged<false>(c, nullptr, c->sel, c->list1, c->counts, n, s);
     if (rc) return rc;
     Accum acc;
     long long counts[4];
@@ -1352,7 +1413,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
         SVP_LAUNCH_CHECK("prescreen_kernel");
         SVP_LAUNCH(prescreen_stage_kernel<<<blocks_for(n1, 256, 8), 256, 0, s>>>(c->lower, n1, delta, c->sel, c->acc));
         SVP_LAUNCH_CHECK("prescreen stage");
-        rc = select_flagged(c, c->list1, c->sel, c->list2, c->counts + 1, n1, s);
+        rc = select_flagged<true>(c, c->list1, c->sel, c->list2, c->counts + 1, n1, s);
         if (rc) return rc;
         SVP_CUDA(cudaMemcpyAsync(&n2, c->counts + 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
         SVP_CUDA(cudaStreamSynchronize(s));
@@ -1379,7 +1440,7 @@ extern "C" int svp_certify_map(svp_certifier *c, const double *u, svp_cert_resul
         SVP_LAUNCH(fallback_stage_kernel<<<blocks_for(n2, 256, 8), 256, 0, s>>>(list2, clo, smp, n2, tile, c->tile_fail,
                                                                       c->sel, c->acc));
         SVP_LAUNCH_CHECK("fallback stage");
-        rc = select_flagged(c, thrust::counting_iterator<long long>(0), c->sel, c->list3, c->counts + 2, n2, s);
+        rc = select_flagged<false>(c, nullptr, c->sel, c->list3, c->counts + 2, n2, s);
         if (rc) return rc;
         SVP_CUDA(cudaMemcpyAsync(&n3, c->counts + 2, sizeof(long long), cudaMemcpyDeviceToHost, s));
         SVP_CUDA(cudaStreamSynchronize(s));

@@ -150,55 +150,28 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// TC: the arithmetic type of a pass (double in the plain form, float in the mixed form); inputs and outputs may be
-// either (the mixed form reads the float64 right-hand side and writes the float64 direction).
-template <class TC>
-struct HalfDstT {
-    const TC *h0, *h1;
+// The float64 half matrices of one axis (the plain form's passes; the mixed form's are HalfTf32 below).
+struct HalfDst {
+    const double *h0, *h1;
     int n, k0, k1;     // n, ceil(n/2), floor(n/2)
 };
-using HalfDst = HalfDstT<double>;
-// Tile product of one K block held in shared memory, 8 warps x 16 x 32 outputs (A fragments from sA[k][row], B
-// from sB[k][col]): FP64 tensor path (2 x 4 DMMA 8x8x4 tiles per warp) or, for float, 3xTF32 (4 m16n8k8 tiles per
-// warp, facc[fc] holding rows gid and gid + 8 of n-tile fc).
-template <class TC>
-__device__ __forceinline__ void tile_product(const TC (*sA)[TM + 4], const TC (*sB)[TN + 4], int lane, int warp,
-                                             double (&dacc)[2][4][2], float (&facc)[4][4]) {
-    if constexpr (sizeof(TC) == 8) {
-        const int gid = lane >> 2, tig = lane & 3;
-        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+// Tile product of one K block held in shared memory on the FP64 tensor path: 8 warps x 16 x 32 outputs, 2 x 4 DMMA
+// 8x8x4 tiles per warp (A fragments from sA[k][row], B from sB[k][col]).
+__device__ __forceinline__ void tile_product(const double (*sA)[TM + 4], const double (*sB)[TN + 4], int lane,
+                                             int warp, double (&dacc)[2][4][2]) {
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
 #pragma unroll
-        for (int kb = 0; kb < TK; kb += 4) {
-            double a[2], x[4];
+    for (int kb = 0; kb < TK; kb += 4) {
+        double a[2], x[4];
 #pragma unroll
-            for (int fr = 0; fr < 2; fr++) a[fr] = sA[kb + tig][wr + 8 * fr + gid];
+        for (int fr = 0; fr < 2; fr++) a[fr] = sA[kb + tig][wr + 8 * fr + gid];
 #pragma unroll
-            for (int fc = 0; fc < 4; fc++) x[fc] = sB[kb + tig][wc + 8 * fc + gid];
+        for (int fc = 0; fc < 4; fc++) x[fc] = sB[kb + tig][wc + 8 * fc + gid];
 #pragma unroll
-            for (int fr = 0; fr < 2; fr++)
+        for (int fr = 0; fr < 2; fr++)
 #pragma unroll
-                for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
-        }
-    } else {
-        const int gid = lane >> 2, tig = lane & 3;
-        const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-#pragma unroll
-        for (int kb = 0; kb < TK; kb += 8) {
-            unsigned ab[4], as[4];
-            tf32_split(sA[kb + tig][wr + gid], ab[0], as[0]);
-            tf32_split(sA[kb + tig][wr + gid + 8], ab[1], as[1]);
-            tf32_split(sA[kb + tig + 4][wr + gid], ab[2], as[2]);
-            tf32_split(sA[kb + tig + 4][wr + gid + 8], ab[3], as[3]);
-#pragma unroll
-            for (int fc = 0; fc < 4; fc++) {
-                unsigned b0b, b0s, b1b, b1s;
-                tf32_split(sB[kb + tig][wc + 8 * fc + gid], b0b, b0s);
-                tf32_split(sB[kb + tig + 4][wc + 8 * fc + gid], b1b, b1s);
-                mma_tf32(facc[fc], as, b0b, b1b);
-                mma_tf32(facc[fc], ab, b0s, b1s);
-                mma_tf32(facc[fc], ab, b0b, b1b);
-            }
-        }
+            for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
     }
 }
 
@@ -215,28 +188,26 @@ __device__ __forceinline__ TC fold_value(double xa, double xb, bool mid, int g) 
 // enumerates the 64-row tiles of parity 0, then of parity 1 (the blocks that read the same X run together).  EPI 1
 // divides by den[flat % per], EPI 2 multiplies by sign * post[flat] (the same operation order as the separate
 // elementwise passes).  Two shared-memory buffers: block k + 1 is stored while block k is multiplied.
-template <int EPI, class TC, class TI, class TO>
-__global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long W,
+template <int EPI, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_left_kernel(HalfDst D, const TI *__restrict__ X, long long W,
                                                        long long ldx, long long bs, TO *__restrict__ C,
                                                        const double *__restrict__ den, long long per,
                                                        const double *__restrict__ post, double sign) {
-    __shared__ TC sM[2][TK][TM + 4];
-    __shared__ TC sX[2][TK][TN + 4];
+    __shared__ double sM[2][TK][TM + 4];
+    __shared__ double sX[2][TK][TN + 4];
 
-    constexpr bool kTensor = sizeof(TC) == 8;    // float64 passes on the FP64 tensor path
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
     const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;   // a warp's 16 x 32 block of the 64 x 64 tile
     double dacc[2][4][2] = {};
     const int t0 = (D.k0 + TM - 1) / TM;
     const int g = (int)blockIdx.x < t0 ? 0 : 1;
     const int rows = g ? D.k1 : D.k0, K = rows;
-    const TC *H = g ? D.h1 : D.h0;
+    const double *H = g ? D.h1 : D.h0;
     const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
     const long long b = blockIdx.z;
     const long long w0 = (long long)blockIdx.y * TN;
     const TI *Xb = X + b * bs;
-    float facc[4][4] = {};
-    TC rm[4];
+    double rm[4];
     double ra[4], rb[4];
     auto fetch = [&](int k0) {
 #pragma unroll
@@ -244,7 +215,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
             const int e = threadIdx.x + 256 * t;
             {
                 const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
-                rm[t] = (i < rows && k < K) ? H[(long long)i * K + k] : TC(0);
+                rm[t] = (i < rows && k < K) ? H[(long long)i * K + k] : 0.;
             }
             const int ww = e % TN, kk = e / TN, k = k0 + kk;
             const long long w = w0 + ww;
@@ -259,7 +230,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
             const int e = threadIdx.x + 256 * t;
             sM[buf][e % TK][e / TK] = rm[t];
             const int ww = e % TN, kk = e / TN, k = k0 + kk;
-            sX[buf][kk][ww] = fold_value<TC>(ra[t], rb[t], k == D.n - 1 - k, g);
+            sX[buf][kk][ww] = fold_value<double>(ra[t], rb[t], k == D.n - 1 - k, g);
         }
     };
     fetch(0);
@@ -269,7 +240,7 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
     for (int k0 = 0; k0 < K; k0 += TK) {
         const bool more = k0 + TK < K;
         if (more) fetch(k0 + TK);
-        tile_product<TC>(sM[buf], sX[buf], lane, warp, dacc, facc);
+        tile_product(sM[buf], sX[buf], lane, warp, dacc);
         if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
         buf ^= 1;
@@ -282,43 +253,32 @@ __global__ void __launch_bounds__(256) dst_left_kernel(HalfDstT<TC> D, const TI 
         if (EPI == 2) v = sign * (post[o] * v);
         C[o] = (TO)v;
     };
-    if constexpr (kTensor) {
 #pragma unroll
-        for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-            for (int fc = 0; fc < 4; fc++)
-#pragma unroll
-                for (int e = 0; e < 2; e++)
-                    store(i0 + wr + 8 * fr + gid, w0 + wc + 8 * fc + 2 * tig + e, dacc[fr][fc][e]);
-    } else {
+    for (int fr = 0; fr < 2; fr++)
 #pragma unroll
         for (int fc = 0; fc < 4; fc++)
 #pragma unroll
-            for (int e = 0; e < 4; e++)
-                store(i0 + wr + gid + 8 * (e >> 1), w0 + wc + 8 * fc + 2 * tig + (e & 1), (double)facc[fc][e]);
-    }
+            for (int e = 0; e < 2; e++) store(i0 + wr + 8 * fr + gid, w0 + wc + 8 * fc + 2 * tig + e, dacc[fr][fc][e]);
 }
 
 // Right pass over contiguous rows of length n: C[r][i] = sum_k X[r][k] S[i][k]; pre (optional) scales X first.
-template <class TC, class TI, class TO>
-__global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI *__restrict__ X, long long R,
+template <class TI, class TO>
+__global__ void __launch_bounds__(256) dst_right_kernel(HalfDst D, const TI *__restrict__ X, long long R,
                                                         const double *__restrict__ pre, TO *__restrict__ C) {
-    __shared__ TC sX[2][TK][TM + 4];
-    __shared__ TC sM[2][TK][TN + 4];
+    __shared__ double sX[2][TK][TM + 4];
+    __shared__ double sM[2][TK][TN + 4];
 
-    constexpr bool kTensor = sizeof(TC) == 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
     const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
     double dacc[2][4][2] = {};
     const int t0 = (D.k0 + TN - 1) / TN;
     const int g = (int)blockIdx.x < t0 ? 0 : 1;
     const int cols = g ? D.k1 : D.k0, K = cols;
-    const TC *H = g ? D.h1 : D.h0;
+    const double *H = g ? D.h1 : D.h0;
     const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
     const long long r0 = (long long)blockIdx.y * TM;
     const int n = D.n;
-    float facc[4][4] = {};
-    TC rm[4];
+    double rm[4];
     double ra[4], rb[4];
     auto fetch = [&](int k0) {
 #pragma unroll
@@ -333,7 +293,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
                 rb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
             }
             const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
-            rm[t] = (i < cols && k < K) ? H[(long long)i * K + k] : TC(0);
+            rm[t] = (i < cols && k < K) ? H[(long long)i * K + k] : 0.;
         }
     };
     auto stash = [&](int buf, int k0) {
@@ -341,7 +301,7 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
         for (int t = 0; t < 4; t++) {
             const int e = threadIdx.x + 256 * t;
             const int kk = e % TK, k = k0 + kk;
-            sX[buf][kk][e / TK] = fold_value<TC>(ra[t], rb[t], k == n - 1 - k, g);
+            sX[buf][kk][e / TK] = fold_value<double>(ra[t], rb[t], k == n - 1 - k, g);
             sM[buf][kk][e / TK] = rm[t];
         }
     };
@@ -352,32 +312,220 @@ __global__ void __launch_bounds__(256) dst_right_kernel(HalfDstT<TC> D, const TI
     for (int k0 = 0; k0 < K; k0 += TK) {
         const bool more = k0 + TK < K;
         if (more) fetch(k0 + TK);
-        tile_product<TC>(sX[buf], sM[buf], lane, warp, dacc, facc);
+        tile_product(sX[buf], sM[buf], lane, warp, dacc);
         if (more) stash(buf ^ 1, k0 + TK);
         __syncthreads();
         buf ^= 1;
     }
-    if constexpr (kTensor) {
 #pragma unroll
-        for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-            for (int fc = 0; fc < 4; fc++)
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const long long r = r0 + wr + 8 * fr + gid;
-                    const int ii = i0 + wc + 8 * fc + 2 * tig + e;
-                    if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)dacc[fr][fc][e];
-                }
-    } else {
+    for (int fr = 0; fr < 2; fr++)
 #pragma unroll
         for (int fc = 0; fc < 4; fc++)
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const long long r = r0 + wr + gid + 8 * (e >> 1);
-                const int ii = i0 + wc + 8 * fc + 2 * tig + (e & 1);
-                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)facc[fc][e];
+            for (int e = 0; e < 2; e++) {
+                const long long r = r0 + wr + 8 * fr + gid;
+                const int ii = i0 + wc + 8 * fc + 2 * tig + e;
+                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)dacc[fr][fc][e];
             }
+}
+
+// ---------------------------------------------------------------------------------------- mixed form (3xTF32)
+// The float32 passes keep each operand as its two TF32 parts in shared memory: the half matrices are split once per
+// grid (split_half_kernel), the folded fields once when a K block is staged, so a fragment is loaded, never split.
+// Rows of the staged blocks are padded to TM + 8 words: the fragment loads (rows tig, tig + 4 x columns gid) fall in
+// 32 distinct banks.  The products are those of the per-fragment split (same parts, same mma order), bitwise.
+constexpr int TP = TM + 8;
+
+struct HalfTf32 {
+    const unsigned *b0, *s0, *b1, *s1;   // parity 0 / 1, big / small parts, each k_g x k_g with T[k][a] = H_g[a][k]
+    int n, k0, k1;
+};
+
+// h: H0 (k0 x k0) then H1 (k1 x k1), row-major float32; out: the big parts of H0^T, H1^T, then the small parts.
+__global__ void split_half_kernel(const float *__restrict__ h, int k0, int k1, unsigned *__restrict__ out) {
+    const long long n0 = (long long)k0 * k0, total = n0 + (long long)k1 * k1;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const bool odd = e >= n0;
+        const int kg = odd ? k1 : k0;
+        const long long l = odd ? e - n0 : e;
+        const long long t = (odd ? n0 : 0) + (l % kg) * kg + l / kg;
+        unsigned big, small;
+        tf32_split(h[e], big, small);
+        out[t] = big;
+        out[total + t] = small;
     }
+}
+
+// One K block: 8 warps x 16 x 32 outputs, facc[fc] rows gid and gid + 8 of n-tile fc (m16n8k8 layout).
+__device__ __forceinline__ void tf32_tile_product(const unsigned (*Ab)[TP], const unsigned (*As)[TP],
+                                                  const unsigned (*Bb)[TP], const unsigned (*Bs)[TP], int lane,
+                                                  int warp, float (&facc)[4][4]) {
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+#pragma unroll
+    for (int kb = 0; kb < TK; kb += 8) {
+        const unsigned ab[4] = {Ab[kb + tig][wr + gid], Ab[kb + tig][wr + gid + 8], Ab[kb + tig + 4][wr + gid],
+                                Ab[kb + tig + 4][wr + gid + 8]};
+        const unsigned as[4] = {As[kb + tig][wr + gid], As[kb + tig][wr + gid + 8], As[kb + tig + 4][wr + gid],
+                                As[kb + tig + 4][wr + gid + 8]};
+#pragma unroll
+        for (int fc = 0; fc < 4; fc++) {
+            const int col = wc + 8 * fc + gid;
+            const unsigned b0b = Bb[kb + tig][col], b0s = Bs[kb + tig][col];
+            const unsigned b1b = Bb[kb + tig + 4][col], b1s = Bs[kb + tig + 4][col];
+            mma_tf32(facc[fc], as, b0b, b1b);
+            mma_tf32(facc[fc], ab, b0s, b1s);
+            mma_tf32(facc[fc], ab, b0b, b1b);
+        }
+    }
+}
+
+// Left pass in float32 (see dst_left_kernel): A = H_g from its split parts, B = the folded field split on staging.
+template <int EPI, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_left_tf32_kernel(HalfTf32 D, const TI *__restrict__ X, long long W,
+                                                            long long ldx, long long bs, TO *__restrict__ C,
+                                                            const double *__restrict__ den, long long per,
+                                                            const double *__restrict__ post, double sign) {
+    __shared__ unsigned sAb[2][TK][TP], sAs[2][TK][TP], sBb[2][TK][TP], sBs[2][TK][TP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+    const int t0 = (D.k0 + TM - 1) / TM;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
+    const int rows = g ? D.k1 : D.k0, K = rows;
+    const unsigned *Hb = g ? D.b1 : D.b0, *Hs = g ? D.s1 : D.s0;
+    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
+    const long long b = blockIdx.z;
+    const long long w0 = (long long)blockIdx.y * TN;
+    const TI *Xb = X + b * bs;
+    float facc[4][4] = {};
+    unsigned rhb[4], rhs[4];
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            {
+                const int ii = e % TM, kk = e / TM, i = i0 + ii, k = k0 + kk;
+                const bool ok = i < rows && k < K;
+                rhb[t] = ok ? Hb[(long long)k * rows + i] : 0u;
+                rhs[t] = ok ? Hs[(long long)k * rows + i] : 0u;
+            }
+            const int ww = e % TN, kk = e / TN, k = k0 + kk;
+            const long long w = w0 + ww;
+            const bool ok = k < K && w < W;
+            ra[t] = ok ? (double)Xb[(long long)k * ldx + w] : 0.;
+            rb[t] = ok ? (double)Xb[(long long)(D.n - 1 - k) * ldx + w] : 0.;
+        }
+    };
+    auto stash = [&](int buf, int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            sAb[buf][e / TM][e % TM] = rhb[t];
+            sAs[buf][e / TM][e % TM] = rhs[t];
+            const int ww = e % TN, kk = e / TN, k = k0 + kk;
+            unsigned big, small;
+            tf32_split(fold_value<float>(ra[t], rb[t], k == D.n - 1 - k, g), big, small);
+            sBb[buf][kk][ww] = big;
+            sBs[buf][kk][ww] = small;
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += TK) {
+        const bool more = k0 + TK < K;
+        if (more) fetch(k0 + TK);
+        tf32_tile_product(sAb[buf], sAs[buf], sBb[buf], sBs[buf], lane, warp, facc);
+        if (more) stash(buf ^ 1, k0 + TK);
+        __syncthreads();
+        buf ^= 1;
+    }
+#pragma unroll
+    for (int fc = 0; fc < 4; fc++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int ii = i0 + wr + gid + 8 * (e >> 1);
+            const long long w = w0 + wc + 8 * fc + 2 * tig + (e & 1);
+            if (ii >= rows || w >= W) continue;
+            const long long o = b * bs + (long long)(2 * ii + g) * ldx + w;
+            double v = (double)facc[fc][e];
+            if (EPI == 1) v = v / den[o % per];
+            if (EPI == 2) v = sign * (post[o] * v);
+            C[o] = (TO)v;
+        }
+}
+
+// Right pass in float32 (see dst_right_kernel): A = the folded rows split on staging, B = H_g^T from its parts.
+template <class TI, class TO>
+__global__ void __launch_bounds__(256) dst_right_tf32_kernel(HalfTf32 D, const TI *__restrict__ X, long long R,
+                                                             const double *__restrict__ pre, TO *__restrict__ C) {
+    __shared__ unsigned sAb[2][TK][TP], sAs[2][TK][TP], sBb[2][TK][TP], sBs[2][TK][TP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
+    const int t0 = (D.k0 + TN - 1) / TN;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
+    const int cols = g ? D.k1 : D.k0, K = cols;
+    const unsigned *Hb = g ? D.b1 : D.b0, *Hs = g ? D.s1 : D.s0;
+    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
+    const long long r0 = (long long)blockIdx.y * TM;
+    const int n = D.n;
+    float facc[4][4] = {};
+    unsigned rhb[4], rhs[4];
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            {
+                const int kk = e % TK, rr = e / TK, k = k0 + kk;
+                const long long r = r0 + rr;
+                const bool ok = r < R && k < K;
+                const long long a = r * n + k, m = r * n + (n - 1 - k);
+                ra[t] = ok ? (pre ? pre[a] * (double)X[a] : (double)X[a]) : 0.;
+                rb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
+            }
+            const int ii = e % TN, kk = e / TN, i = i0 + ii, k = k0 + kk;
+            const bool ok = i < cols && k < K;
+            rhb[t] = ok ? Hb[(long long)k * cols + i] : 0u;
+            rhs[t] = ok ? Hs[(long long)k * cols + i] : 0u;
+        }
+    };
+    auto stash = [&](int buf, int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int e = threadIdx.x + 256 * t;
+            const int kk = e % TK, k = k0 + kk;
+            unsigned big, small;
+            tf32_split(fold_value<float>(ra[t], rb[t], k == n - 1 - k, g), big, small);
+            sAb[buf][kk][e / TK] = big;
+            sAs[buf][kk][e / TK] = small;
+            sBb[buf][e / TN][e % TN] = rhb[t];
+            sBs[buf][e / TN][e % TN] = rhs[t];
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += TK) {
+        const bool more = k0 + TK < K;
+        if (more) fetch(k0 + TK);
+        tf32_tile_product(sAb[buf], sAs[buf], sBb[buf], sBs[buf], lane, warp, facc);
+        if (more) stash(buf ^ 1, k0 + TK);
+        __syncthreads();
+        buf ^= 1;
+    }
+#pragma unroll
+    for (int fc = 0; fc < 4; fc++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const long long r = r0 + wr + gid + 8 * (e >> 1);
+            const int ii = i0 + wc + 8 * fc + 2 * tig + (e & 1);
+            if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)facc[fc][e];
+        }
 }
 
 __global__ void scale_kernel(const double *__restrict__ x, const double *__restrict__ s, double sign, long long n,
@@ -429,27 +577,36 @@ template <class TC, class TI, class TO>
 static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const double *pre, int epi, double sign,
                     const double *post, cudaStream_t s) {
     const long long n0 = p->q.fx, n1 = p->q.fy, n2 = p->q.fz;
-    const TC *h = nullptr;
-    if constexpr (sizeof(TC) == 8) h = p->dst_half[axis];
-    else h = p->dst_half32[axis];
-    HalfDstT<TC> D{h, h + (size_t)((p->dst_n[axis] + 1) / 2) * ((p->dst_n[axis] + 1) / 2), p->dst_n[axis],
-                   (p->dst_n[axis] + 1) / 2, p->dst_n[axis] / 2};
-    const unsigned tiles = (unsigned)(div_up(D.k0, TM) + div_up(D.k1, TM));
+    const int n = p->dst_n[axis], k0 = (n + 1) / 2, k1 = n / 2;
+    const unsigned tiles = (unsigned)(div_up(k0, TM) + div_up(k1, TM));
     const long long nf = p->q.nfree;
+    constexpr bool kDouble = sizeof(TC) == 8;
+    HalfDst D{p->dst_half[axis], p->dst_half[axis] + (size_t)k0 * k0, n, k0, k1};
+    const unsigned *t = p->dst_tf32[axis];
+    const long long tot = (long long)k0 * k0 + (long long)k1 * k1;
+    HalfTf32 T{t, t + tot, t + (long long)k0 * k0, t + tot + (long long)k0 * k0, n, k0, k1};
     if (axis == 0) {
         SVP_REQUIRE(epi == 0, "dst_pass: x pass has no epilogue");
         long long R = 3 * n2 * n1;
         dim3 grid(tiles, (unsigned)div_up(R, TM));      // the blocks that share rows run together (L2 reuse)
-        { svp::KernelTimer _t("dst_right_kernel", s); SVP_LAUNCH((dst_right_kernel<TC, TI, TO><<<grid, 256, 0, s>>>(D, in, R, pre, out))); }
+        svp::KernelTimer _t("dst_right_kernel", s);
+        if constexpr (kDouble) SVP_LAUNCH((dst_right_kernel<TI, TO><<<grid, 256, 0, s>>>(D, in, R, pre, out)));
+        else SVP_LAUNCH((dst_right_tf32_kernel<TI, TO><<<grid, 256, 0, s>>>(T, in, R, pre, out)));
     } else {
         SVP_REQUIRE(!pre, "dst_pass: pre-scale only on the x pass");
         long long W = axis == 1 ? n0 : n1 * n0;
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
         dim3 grid(tiles, (unsigned)div_up(W, TN), (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
-        if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
-        else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
-        else SVP_LAUNCH((dst_left_kernel<2, TC, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+        if constexpr (kDouble) {
+            if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_kernel<2, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+        } else {
+            if (epi == 0) SVP_LAUNCH((dst_left_tf32_kernel<0, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_tf32_kernel<1, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_tf32_kernel<2, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+        }
     }
     SVP_LAUNCH_CHECK("dst pass");
     return SVP_OK;
@@ -504,9 +661,21 @@ int pair_dst_setup(svp_pair *p) {
         std::vector<double> H = cached_dst1_half((int)f[k]);
         SVP_CUDA(cudaMalloc((void **)&p->dst_half[k], sizeof(double) * H.size()));
         SVP_CUDA(cudaMemcpy(p->dst_half[k], H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice));
-        std::vector<float> H32(H.begin(), H.end());      // the mixed form's matrices (rounded once)
-        SVP_CUDA(cudaMalloc((void **)&p->dst_half32[k], sizeof(float) * H32.size()));
-        SVP_CUDA(cudaMemcpy(p->dst_half32[k], H32.data(), sizeof(float) * H32.size(), cudaMemcpyHostToDevice));
+        // the mixed form's matrices: rounded once to float32, then split into TF32 parts on the device (the same
+        // cvt.rna the passes use for their staged operands)
+        std::vector<float> H32(H.begin(), H.end());
+        float *h32 = nullptr;
+        SVP_CUDA(cudaMalloc((void **)&h32, sizeof(float) * H32.size()));
+        cudaError_t e = cudaMemcpy(h32, H32.data(), sizeof(float) * H32.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&p->dst_tf32[k], sizeof(unsigned) * 2 * H32.size());
+        if (e == cudaSuccess) {
+            split_half_kernel<<<blocks_for((long long)H32.size(), 256, 4), 256>>>(h32, (int)(f[k] + 1) / 2,
+                                                                                 (int)f[k] / 2, p->dst_tf32[k]);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        cudaFree(h32);
+        if (e != cudaSuccess) return cuda_fail(e, "dst tf32 split");
         p->dst_n[k] = (int)f[k];
     }
     SVP_CUDA(cudaMalloc((void **)&p->dst_tmp, sizeof(double) * 2 * 3 * p->q.nfree));

@@ -25,7 +25,8 @@ struct svp_pair {
     // DST-I Poisson metric
     double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
     int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)
-    float *dst_half32[3] = {nullptr, nullptr, nullptr};     // the same, rounded to float32 (mixed form)
+    // the same rounded to float32 for the mixed form, as TF32 parts: big parts of H0^T, H1^T, then the small parts
+    unsigned *dst_tf32[3] = {nullptr, nullptr, nullptr};
     int precision = 0;                                      // SVP_PRECISION_PLAIN or SVP_PRECISION_MIXED
     double *dst_tmp = nullptr;                          // 2 * 3 * nfree scratch
     double *den = nullptr;                              // (nz-2, ny-2, nx-2) omega (a + b lambda)

@@ -1912,6 +1912,69 @@ extern "C" int svp_energy_difference(svp_pair *p, const double *base_u, const do
 // rounding of the squared-residual sums.
 constexpr double kScreenJ = 256., kScreenCurl = 32., kScreenSum = 64.;
 
+// |error of the E difference| <= mu dJ sum w (|ra| + |rb|) + nu dC sum w (|xa| + |xb|) + 2 dS (soft_a + soft_b): the
+// residuals' absolute errors times the summed residual magnitudes, plus the rounding of the squares.  sums: the
+// trial's JD and curl sums (unweighted by mu/2, nu/2), then the four pb sums of cell_trial32_kernel.
+static double screen_band(const svp_pair *p, const double sums[6]) {
+    const double u32 = std::ldexp(1., -24);
+    const double soft = .5 * p->q.mu * (sums[0] + sums[4]) + .5 * p->q.nu * (sums[1] + sums[5]);
+    return p->q.mu * kScreenJ * u32 * sums[2] + p->q.nu * kScreenCurl * u32 * sums[3] + 2. * kScreenSum * u32 * soft;
+}
+
+// The mixed form's screened E/F difference of two evaluated states: node terms float64 (node_diff_kernel), the JD and
+// curl penalty differences float32 (cell_trial32_kernel, with the error band), the barrier differences float64 over
+// the flagged cells; F (image + barrier) is float64 throughout.
+extern "C" int svp_energy_difference_screened(svp_pair *p, const double *base_u, const double *base_warped,
+                                              const double *trial_u, const double *trial_warped,
+                                              const uint8_t *base_active, double *diff2, double *band,
+                                              void *stream) {
+    SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && diff2 && band,
+                "svp_energy_difference_screened: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p), bb = barrier_blocks(p->q);
+    int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 8 + (long long)bb * 2, 1);
+    if (rc) return rc;
+    if ((rc = allow_slices())) return rc;
+    if ((rc = pair_flags(p))) return rc;
+    SVP_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(long long) * 8, s));
+    dd *pn = p->partial, *pce = pn + (long long)nb * 2, *pcd = pce + (long long)cb * 2, *pcb = pcd + (long long)cb * 2;
+    dd *pbe = pcb + (long long)cb * 4, *pbd = pbe + bb;
+    {
+        svp::KernelTimer _t("node_diff_kernel", s);
+        SVP_LAUNCH(node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed,
+                                                       p->u_ref, pn));
+    }
+    {
+        svp::KernelTimer _t("cell_trial32_kernel", s);
+        SVP_LAUNCH(cell_trial32_kernel<<<cb, CS, sizeof(float) * 108 * CS, s>>>(
+            p->q, base_u, trial_u, p->u_ref, pce, pcd, pcb, p->flags, nullptr, base_active));
+    }
+    {
+        svp::KernelTimer _t("cell_trial_barrier_kernel", s);
+        SVP_LAUNCH(cell_trial_barrier_kernel<<<bb, CB, sizeof(double) * 27 * CB, s>>>(
+            p->q, base_u, trial_u, p->flags, pbe, pbd, (unsigned long long *)p->counter, nullptr, base_active));
+    }
+    SVP_LAUNCH_CHECK("screened difference kernels");
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pn, nb, 2, p->result));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 2, p->result + 4));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pbd, bb, 1, p->result + 8));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 2, p->result + 10));
+    SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcb, cb, 4, p->result + 14));
+    SVP_LAUNCH_CHECK("final_reduce_kernel");
+    double tmp[22];
+    SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    SVP_CUDA(cudaStreamSynchronize(s));
+    // E = image + proximity + jd + curl + barrier; F = image + barrier, as svp_energy_difference combines them
+    double img = tmp[0] + tmp[1], prox = tmp[2] + tmp[3];
+    double jd = tmp[4] + tmp[5], curl = tmp[6] + tmp[7], bar = tmp[8] + tmp[9];
+    diff2[0] = (((img + prox) + jd) + curl) + bar;
+    diff2[1] = img + bar;
+    double sums[6];
+    for (int k = 0; k < 6; k++) sums[k] = tmp[10 + 2 * k] + tmp[11 + 2 * k];
+    *band = screen_band(p, sums);
+    return SVP_OK;
+}
+
 static int trial_energy(svp_pair *p, const double *base_u, const double *base_warped, const double *trial_u,
                         double *trial_warped, double *trial_image_grad, const uint8_t *base_active,
                         uint8_t *trial_active, double *terms5, double *diff2, int64_t *barrier_violations,
@@ -1989,14 +2052,11 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
     diff2[0] = (((img + prox) + jd) + curl) + bar;
     diff2[1] = img + bar;
     if (band) {
-        // |error of diff2[0]| <= mu dJ sum w (|ra| + |rb|) + nu dC sum w (|xa| + |xb|) + 2 dS (soft_a + soft_b):
-        // the residuals' absolute errors times the summed residual magnitudes, plus the rounding of the squares
-        const double u32 = std::ldexp(1., -24);
         *band = 0.;
         if (screened) {
-            const double mj = tmp[20] + tmp[21], mc = tmp[22] + tmp[23], aj = tmp[24] + tmp[25], ac = tmp[26] + tmp[27];
-            const double soft = .5 * p->q.mu * (cell3[0] + aj) + .5 * p->q.nu * (cell3[1] + ac);
-            *band = p->q.mu * kScreenJ * u32 * mj + p->q.nu * kScreenCurl * u32 * mc + 2. * kScreenSum * u32 * soft;
+            const double sums[6] = {cell3[0], cell3[1], tmp[20] + tmp[21], tmp[22] + tmp[23], tmp[24] + tmp[25],
+                                    tmp[26] + tmp[27]};
+            *band = screen_band(p, sums);
         }
     }
     return SVP_OK;

@@ -103,6 +103,15 @@ class DevicePair:
                   ptr(base_active), ptr(trial_active), d, stream_ptr(stream))
         return d[0], d[1]
 
+    def energy_difference_screened(self, base_u, base_w, trial_u, trial_w, base_active=None, stream=None):
+        """energy_difference with the JD/curl penalty differences in float32 (the mixed form's screen): (dE, dF,
+        band), dE within band of the float64 difference, dF the float64 call's value."""
+        d = (ctypes.c_double * 2)()
+        band = ctypes.c_double()
+        _lib.call("svp_energy_difference_screened", self._h, ptr(base_u), ptr(base_w), ptr(trial_u), ptr(trial_w),
+                  ptr(base_active), d, ctypes.byref(band), stream_ptr(stream))
+        return d[0], d[1], band.value
+
     def cell_mask(self):
         return torch.empty(self.grid.n_cells, dtype=torch.uint8, device=self.device)
 

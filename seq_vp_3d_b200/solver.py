@@ -195,24 +195,31 @@ class Registration:
                 self._screen_check(base, state)
         return state
 
-    def _screen_check(self, base, trial):
-        """Runtime check of the float32 screen on the first SCREEN_CHECKS evaluations and every SCREEN_RECHECK-th:
-        the float64 difference replaces the screened one, and a screened value outside its band ends screening."""
+    def _verify(self, base, trial, dE, band):
+        """The screen's runtime check, on the first SCREEN_CHECKS screened evaluations and every SCREEN_RECHECK-th:
+        the float64 (dE, dF) of the two states, or None when no check is due.  A screened dE outside its band ends
+        screening for this registration."""
         sc = self.screen
         sc["evaluations"] += 1
         k = sc["evaluations"]
         if not (k <= SCREEN_CHECKS or k % SCREEN_RECHECK == 0):
-            return
+            return None
         sc["checks"] += 1
-        dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active, trial.active)
-        err = abs(trial.differences[1][0] - dE)
-        if trial.band > 0:
-            sc["max_error_over_band"] = max(sc["max_error_over_band"], err / trial.band)
-        if err > trial.band:
+        exact = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active, trial.active)
+        err = abs(dE - exact[0])
+        if band > 0:
+            sc["max_error_over_band"] = max(sc["max_error_over_band"], err / band)
+        if err > band:
             sc["violations"] += 1
             sc["on"] = False
-        trial.differences = (trial.differences[0], (dE, dF))
-        trial.band = 0.
+        return exact
+
+    def _screen_check(self, base, trial):
+        """The runtime check of a screened trial evaluation: a checked trial keeps the float64 differences."""
+        exact = self._verify(base, trial, trial.differences[1][0], trial.band)
+        if exact is not None:
+            trial.differences = (trial.differences[0], exact)
+            trial.band = 0.
 
     def promote_trial(self, state):
         if state.image_grad is None:
@@ -251,26 +258,36 @@ class Registration:
 
     def stable_reductions(self, base, trial, required=None):
         """(E, F) EnergyReduction pairs (actual, resolution) (energy_comparison.py:135).  A screened (float32) E
-        difference is replaced by the float64 one when the decision it feeds -- certified = actual - resolution
-        against 0 and `required`, |actual| against the resolution -- lies within SCREEN_MARGIN bands."""
+        difference -- the trial's own from its evaluation against this base, or, for any other pair of states in the
+        mixed form (the outer commit's start and candidate), svp_energy_difference_screened -- is replaced by the
+        float64 one when the decision it feeds (certified = actual - resolution against 0 and `required`, |actual|
+        against the resolution) lies within SCREEN_MARGIN bands; F is float64 in both."""
         cached = trial.differences
         use_cache = cached is not None and cached[0] == (base.eval_id, self._reference_version)
+        band = 0.
         if use_cache:
-            dE, dF = cached[1]
+            (dE, dF), band = cached[1], trial.band
+        elif self.screen["on"]:
+            dE, dF, band = self.pair.energy_difference_screened(base.u, base.warped, trial.u, trial.warped,
+                                                                base.active)
+            exact = self._verify(base, trial, dE, band)
+            if exact is not None:
+                (dE, dF), band = exact, 0.
         else:
             dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active,
                                                  trial.active)
         rE = 16 * EPS * max(base.total, trial.total)
         rF = 16 * EPS * max(base.outer, trial.outer)
-        if use_cache and trial.band > 0:
-            actual, margin = -dE, SCREEN_MARGIN * trial.band
+        if band > 0:
+            actual, margin = -dE, SCREEN_MARGIN * band
             edges = (rE, -rE) + ((required + rE,) if required is not None else ())
-            if required is None or not np.isfinite(actual) or min(abs(actual - e) for e in edges) <= margin:
+            if not np.isfinite(actual) or min(abs(actual - e) for e in edges) <= margin:
                 self.screen["band_hits"] += 1
                 dE, dF = self.pair.energy_difference(base.u, base.warped, trial.u, trial.warped, base.active,
                                                      trial.active)
-                trial.differences = (cached[0], (dE, dF))
-                trial.band = 0.
+                if use_cache:
+                    trial.differences = (cached[0], (dE, dF))
+                    trial.band = 0.
         return (-dE, rE), (-dF, rF)
 
     def step_ratio(self, candidate, theta):

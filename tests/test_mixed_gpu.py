@@ -114,3 +114,20 @@ def test_screened_trial(pairs):
         assert abs(got[4][1] - ref[4][1]) <= 1e-12 * (abs(rt[0]) + abs(rt[4]))   # F = image + barrier
         band = got[6]
         assert band > 0 and abs(got[4][0] - ref[4][0]) <= band, (got[4][0], ref[4][0], band)
+
+
+def test_screened_difference(pairs):
+    """svp_energy_difference_screened (the outer commit's screened comparison of two evaluated states) against the
+    float64 svp_energy_difference_masked, both directions: dF (image + barrier, float64 in both; the barrier sums run
+    in a different kernel) within 1e-12 relative, dE within the returned band, and the band is the screened trial's
+    for the same pair of states (the same float32 sums)."""
+    d, plain, mixed, u1, w1, g1 = pairs
+    u2 = torch.from_numpy(d["u2"]).cuda()
+    w2, _ = plain.warp(u2)
+    for (ua, wa, ub, wb) in ((u1, w1, u2, w2), (u2, w2, u1, w1)):
+        ref = plain.energy_difference(ua, wa, ub, wb)
+        dE, dF, band = plain.energy_difference_screened(ua, wa, ub, wb)
+        scale = abs(ref[1]) + abs(plain.energy(ub, wb)[0][4])
+        assert abs(dF - ref[1]) <= 1e-12 * scale, (dF, ref[1])
+        assert band > 0 and abs(dE - ref[0]) <= band, (dE, ref[0], band)
+        assert band == plain.trial_energy_screened(ua, wa, ub)[6]
