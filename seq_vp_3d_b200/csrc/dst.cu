@@ -150,32 +150,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// The float64 half matrices of one axis (the plain form's passes; the mixed form's are HalfTf32 below).
-struct HalfDst {
-    const double *h0, *h1;
-    int n, k0, k1;     // n, ceil(n/2), floor(n/2)
-};
-// Tile product of one K block held in shared memory on the FP64 tensor path: 8 warps x 16 x 32 outputs, 2 x 4 DMMA
-// 8x8x4 tiles per warp (A fragments from sA[k][row], B from sB[k][col]).
-__device__ __forceinline__ void tile_product(const double (*sA)[TM + 4], const double (*sB)[TN + 4], int lane,
-                                             int warp, double (&dacc)[2][4][2]) {
-    const int gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-#pragma unroll
-    for (int kb = 0; kb < TK; kb += 4) {
-        double a[2], x[4];
-#pragma unroll
-        for (int fr = 0; fr < 2; fr++) a[fr] = sA[kb + tig][wr + 8 * fr + gid];
-#pragma unroll
-        for (int fc = 0; fc < 4; fc++) x[fc] = sB[kb + tig][wc + 8 * fc + gid];
-#pragma unroll
-        for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-            for (int fc = 0; fc < 4; fc++) dmma_8x8x4(dacc[fr][fc], a[fr], x[fc]);
-    }
-}
-
-// One K block of the folded operand: the raw pair (x_k, x_(n-1-k)) of each of a thread's 4 entries is fetched into
+// One K block of the folded operand: the raw pair (x_k, x_(n-1-k)) of each of a thread's entries is fetched into
 // registers one block ahead (the loads fly while the previous block's products run) and folded when it is stored
 // to shared memory.  fold = x_k (middle row of odd n), x_k + x_m (parity 0) or x_k - x_m (parity 1), formed in
 // float64 (with the optional pre-scale) and rounded once to the pass's type; entries outside the operand are +0.
@@ -184,348 +159,624 @@ __device__ __forceinline__ TC fold_value(double xa, double xb, bool mid, int g) 
     return (TC)(mid ? xa : (g ? xa - xb : xa + xb));
 }
 
-// Left pass: C[b][i][w] = sum_k S[i][k] X[b][k][w] (rows of length W, stride ldx, batch stride bs).  blockIdx.x
-// enumerates the 64-row tiles of parity 0, then of parity 1 (the blocks that read the same X run together).  EPI 1
-// divides by den[flat % per], EPI 2 multiplies by sign * post[flat] (the same operation order as the separate
-// elementwise passes).  Two shared-memory buffers: block k + 1 is stored while block k is multiplied.
-template <int EPI, class TI, class TO>
-__global__ void __launch_bounds__(256) dst_left_kernel(HalfDst D, const TI *__restrict__ X, long long W,
-                                                       long long ldx, long long bs, TO *__restrict__ C,
-                                                       const double *__restrict__ den, long long per,
-                                                       const double *__restrict__ post, double sign) {
-    __shared__ double sM[2][TK][TM + 4];
-    __shared__ double sX[2][TK][TN + 4];
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;   // a warp's 16 x 32 block of the 64 x 64 tile
-    double dacc[2][4][2] = {};
-    const int t0 = (D.k0 + TM - 1) / TM;
-    const int g = (int)blockIdx.x < t0 ? 0 : 1;
-    const int rows = g ? D.k1 : D.k0, K = rows;
-    const double *H = g ? D.h1 : D.h0;
-    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
-    const long long b = blockIdx.z;
-    const long long w0 = (long long)blockIdx.y * TN;
-    const TI *Xb = X + b * bs;
-    double rm[4];
-    double ra[4], rb[4];
-    auto fetch = [&](int k0) {
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            {
-                const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
-                rm[t] = (i < rows && k < K) ? H[(long long)i * K + k] : 0.;
-            }
-            const int ww = e % TN, kk = e / TN, k = k0 + kk;
-            const long long w = w0 + ww;
-            const bool ok = k < K && w < W;
-            ra[t] = ok ? (double)Xb[(long long)k * ldx + w] : 0.;
-            rb[t] = ok ? (double)Xb[(long long)(D.n - 1 - k) * ldx + w] : 0.;
-        }
-    };
-    auto stash = [&](int buf, int k0) {
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            sM[buf][e % TK][e / TK] = rm[t];
-            const int ww = e % TN, kk = e / TN, k = k0 + kk;
-            sX[buf][kk][ww] = fold_value<double>(ra[t], rb[t], k == D.n - 1 - k, g);
-        }
-    };
-    fetch(0);
-    stash(0, 0);
-    __syncthreads();
-    int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += TK) {
-        const bool more = k0 + TK < K;
-        if (more) fetch(k0 + TK);
-        tile_product(sM[buf], sX[buf], lane, warp, dacc);
-        if (more) stash(buf ^ 1, k0 + TK);
-        __syncthreads();
-        buf ^= 1;
-    }
-    auto store = [&](int ii, long long w, double v) {
-        if (ii >= rows || w >= W) return;
-        long long i = 2 * ii + g;
-        long long o = b * bs + i * ldx + w;
-        if (EPI == 1) v = v / den[o % per];
-        if (EPI == 2) v = sign * (post[o] * v);
-        C[o] = (TO)v;
-    };
-#pragma unroll
-    for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-        for (int fc = 0; fc < 4; fc++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) store(i0 + wr + 8 * fr + gid, w0 + wc + 8 * fc + 2 * tig + e, dacc[fr][fc][e]);
-}
-
-// Right pass over contiguous rows of length n: C[r][i] = sum_k X[r][k] S[i][k]; pre (optional) scales X first.
-template <class TI, class TO>
-__global__ void __launch_bounds__(256) dst_right_kernel(HalfDst D, const TI *__restrict__ X, long long R,
-                                                        const double *__restrict__ pre, TO *__restrict__ C) {
-    __shared__ double sX[2][TK][TM + 4];
-    __shared__ double sM[2][TK][TN + 4];
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-    double dacc[2][4][2] = {};
-    const int t0 = (D.k0 + TN - 1) / TN;
-    const int g = (int)blockIdx.x < t0 ? 0 : 1;
-    const int cols = g ? D.k1 : D.k0, K = cols;
-    const double *H = g ? D.h1 : D.h0;
-    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
-    const long long r0 = (long long)blockIdx.y * TM;
-    const int n = D.n;
-    double rm[4];
-    double ra[4], rb[4];
-    auto fetch = [&](int k0) {
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            {
-                const int kk = e % TK, rr = e / TK, k = k0 + kk;
-                const long long r = r0 + rr;
-                const bool ok = r < R && k < K;
-                const long long a = r * n + k, m = r * n + (n - 1 - k);
-                ra[t] = ok ? (pre ? pre[a] * (double)X[a] : (double)X[a]) : 0.;
-                rb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
-            }
-            const int kk = e % TK, ii = e / TK, i = i0 + ii, k = k0 + kk;
-            rm[t] = (i < cols && k < K) ? H[(long long)i * K + k] : 0.;
-        }
-    };
-    auto stash = [&](int buf, int k0) {
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            const int kk = e % TK, k = k0 + kk;
-            sX[buf][kk][e / TK] = fold_value<double>(ra[t], rb[t], k == n - 1 - k, g);
-            sM[buf][kk][e / TK] = rm[t];
-        }
-    };
-    fetch(0);
-    stash(0, 0);
-    __syncthreads();
-    int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += TK) {
-        const bool more = k0 + TK < K;
-        if (more) fetch(k0 + TK);
-        tile_product(sX[buf], sM[buf], lane, warp, dacc);
-        if (more) stash(buf ^ 1, k0 + TK);
-        __syncthreads();
-        buf ^= 1;
-    }
-#pragma unroll
-    for (int fr = 0; fr < 2; fr++)
-#pragma unroll
-        for (int fc = 0; fc < 4; fc++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const long long r = r0 + wr + 8 * fr + gid;
-                const int ii = i0 + wc + 8 * fc + 2 * tig + e;
-                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)dacc[fr][fc][e];
-            }
-}
-
 // ---------------------------------------------------------------------------------------- mixed form (3xTF32)
 // The float32 passes keep each operand as its two TF32 parts in shared memory: the half matrices are split once per
-// grid (split_half_kernel), the folded fields once when a K block is staged, so a fragment is loaded, never split.
-// Rows of the staged blocks are padded to TM + 8 words: the fragment loads (rows tig, tig + 4 x columns gid) fall in
-// 32 distinct banks.  The products are those of the per-fragment split (same parts, same mma order), bitwise.
-constexpr int TP = TM + 8;
+// grid into zero-padded tiles (split_pad_kernel), the folded fields once when a K block is staged, so a fragment is
+// loaded, never split, and the staging loads need no bounds checks on the matrix side.  A block computes a 128-row x
+// 64-column (left pass) or 128-row x 16 NT-column (right pass) output tile with 8 warps of 32 x 32 (32 x 8 NT), each
+// K block of 16 staged twice-buffered through registers.  Every output is accumulated in k order, three mma per k8
+// step (small x big, big x small, big x big), so any tiling gives the same bits.
+constexpr int QR = 128, QK = 16;           // output rows per block, K block
+constexpr int QC = 64;                     // output columns per block of the left pass
+constexpr int QPA = QR + 8, QPB = QC + 8;  // left pass: [k][row] and [k][col] rows padded to 8 mod 32 words
+constexpr int QPK = QK + 4;                // right pass: [row][k] rows padded to 4 mod 32 words
 
-struct HalfTf32 {
-    const unsigned *b0, *s0, *b1, *s1;   // parity 0 / 1, big / small parts, each k_g x k_g with T[k][a] = H_g[a][k]
-    int n, k0, k1;
+struct PadTf32 {
+    const unsigned *b[2], *s[2];   // per parity: big / small parts, zero-padded to kpad x ipad (left) or ipad x kpad
+    int n, kg[2], ipad[2], kpad[2];
 };
 
-// h: H0 (k0 x k0) then H1 (k1 x k1), row-major float32; out: the big parts of H0^T, H1^T, then the small parts.
-__global__ void split_half_kernel(const float *__restrict__ h, int k0, int k1, unsigned *__restrict__ out) {
-    const long long n0 = (long long)k0 * k0, total = n0 + (long long)k1 * k1;
+// h: H0 (k0 x k0) then H1 (k1 x k1), row-major float32.  out, per parity g: big parts then small parts of H_g in the
+// pass's layout, kmajor: T[k][a] = H_g[a][k] (kpad x ipad), else T[a][k] = H_g[a][k] (ipad x kpad), zeros outside.
+__global__ void split_pad_kernel(const float *__restrict__ h, int kg, long long src, int kmajor, int ipad, int kpad,
+                                 unsigned *__restrict__ big, unsigned *__restrict__ small) {
+    const long long total = (long long)ipad * kpad;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
-        const bool odd = e >= n0;
-        const int kg = odd ? k1 : k0;
-        const long long l = odd ? e - n0 : e;
-        const long long t = (odd ? n0 : 0) + (l % kg) * kg + l / kg;
-        unsigned big, small;
-        tf32_split(h[e], big, small);
-        out[t] = big;
-        out[total + t] = small;
+        const int a = kmajor ? (int)(e % ipad) : (int)(e / kpad), k = kmajor ? (int)(e / ipad) : (int)(e % kpad);
+        unsigned b = 0u, s = 0u;
+        if (a < kg && k < kg) tf32_split(h[src + (long long)a * kg + k], b, s);
+        big[e] = b;
+        small[e] = s;
     }
 }
 
-// One K block: 8 warps x 16 x 32 outputs, facc[fc] rows gid and gid + 8 of n-tile fc (m16n8k8 layout).
-__device__ __forceinline__ void tf32_tile_product(const unsigned (*Ab)[TP], const unsigned (*As)[TP],
-                                                  const unsigned (*Bb)[TP], const unsigned (*Bs)[TP], int lane,
-                                                  int warp, float (&facc)[4][4]) {
-    const int gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-#pragma unroll
-    for (int kb = 0; kb < TK; kb += 8) {
-        const unsigned ab[4] = {Ab[kb + tig][wr + gid], Ab[kb + tig][wr + gid + 8], Ab[kb + tig + 4][wr + gid],
-                                Ab[kb + tig + 4][wr + gid + 8]};
-        const unsigned as[4] = {As[kb + tig][wr + gid], As[kb + tig][wr + gid + 8], As[kb + tig + 4][wr + gid],
-                                As[kb + tig + 4][wr + gid + 8]};
-#pragma unroll
-        for (int fc = 0; fc < 4; fc++) {
-            const int col = wc + 8 * fc + gid;
-            const unsigned b0b = Bb[kb + tig][col], b0s = Bs[kb + tig][col];
-            const unsigned b1b = Bb[kb + tig + 4][col], b1s = Bs[kb + tig + 4][col];
-            mma_tf32(facc[fc], as, b0b, b1b);
-            mma_tf32(facc[fc], ab, b0s, b1s);
-            mma_tf32(facc[fc], ab, b0b, b1b);
-        }
-    }
+template <class TI>
+__device__ __forceinline__ float fold_tf32(TI xa, TI xb, bool mid, int g) {
+    // formed in the input type and rounded once: a float32 sum or difference is the rounded exact value either way
+    return (float)(mid ? xa : (g ? xa - xb : xa + xb));
 }
 
-// Left pass in float32 (see dst_left_kernel): A = H_g from its split parts, B = the folded field split on staging.
+// Left pass along y or z: C[b][2i + g][w] = sum_k H_g[i][k] fold_g(X)[b][k][w] (rows of length W, stride ldx, batch
+// stride bs).  EPI 1 divides by den[index within the batch] (den is one component's array: the z pass's batch stride
+// is its length), EPI 2 multiplies by sign * post[flat] (the operation order of the separate elementwise passes).
+// 3xTF32: A = H_g^T tile [k][row], B = the folded field [k][col].
 template <int EPI, class TI, class TO>
-__global__ void __launch_bounds__(256) dst_left_tf32_kernel(HalfTf32 D, const TI *__restrict__ X, long long W,
+__global__ void __launch_bounds__(256) dst_left_tf32_kernel(PadTf32 D, const TI *__restrict__ X, long long W,
                                                             long long ldx, long long bs, TO *__restrict__ C,
-                                                            const double *__restrict__ den, long long per,
+                                                            const double *__restrict__ den,
                                                             const double *__restrict__ post, double sign) {
-    __shared__ unsigned sAb[2][TK][TP], sAs[2][TK][TP], sBb[2][TK][TP], sBs[2][TK][TP];
+    extern __shared__ __align__(16) unsigned qsm[];
+    unsigned(*sAb)[QK][QPA] = reinterpret_cast<unsigned(*)[QK][QPA]>(qsm);
+    unsigned(*sAs)[QK][QPA] = reinterpret_cast<unsigned(*)[QK][QPA]>(qsm + 2 * QK * QPA);
+    unsigned(*sBb)[QK][QPB] = reinterpret_cast<unsigned(*)[QK][QPB]>(qsm + 4 * QK * QPA);
+    unsigned(*sBs)[QK][QPB] = reinterpret_cast<unsigned(*)[QK][QPB]>(qsm + 4 * QK * QPA + 2 * QK * QPB);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-    const int t0 = (D.k0 + TM - 1) / TM;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int t0 = D.ipad[0] / QR;
     const int g = (int)blockIdx.x < t0 ? 0 : 1;
-    const int rows = g ? D.k1 : D.k0, K = rows;
-    const unsigned *Hb = g ? D.b1 : D.b0, *Hs = g ? D.s1 : D.s0;
-    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TM;
-    const long long b = blockIdx.z;
-    const long long w0 = (long long)blockIdx.y * TN;
-    const TI *Xb = X + b * bs;
-    float facc[4][4] = {};
-    unsigned rhb[4], rhs[4];
-    double ra[4], rb[4];
+    const int rows = g ? D.kg[1] : D.kg[0], K = rows, ip = g ? D.ipad[1] : D.ipad[0];
+    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * QR;
+    const unsigned *Hb = g ? D.b[1] : D.b[0], *Hs = g ? D.s[1] : D.s[0];
+    const long long w0 = (long long)blockIdx.y * QC;
+    const TI *Xb = X + (long long)blockIdx.z * bs;
+    float facc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) facc[a][c][e] = 0.f;
+    // staging: the matrix block (16 x 128 words per part) as two uint4 per thread, the field block (16 rows x 64
+    // columns, each with its mirror row) as two column pairs per thread
+    const int hr = threadIdx.x >> 5, hc = (threadIdx.x & 31) * 4;
+    const int xr = threadIdx.x >> 5, xc = (threadIdx.x & 31) * 2;
+    const bool ok0 = w0 + xc < W, ok1 = w0 + xc + 1 < W;
+    uint4 hb[2], hs[2];
+    TI xa[2][2], xb[2][2];
     auto fetch = [&](int k0) {
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            {
-                const int ii = e % TM, kk = e / TM, i = i0 + ii, k = k0 + kk;
-                const bool ok = i < rows && k < K;
-                rhb[t] = ok ? Hb[(long long)k * rows + i] : 0u;
-                rhs[t] = ok ? Hs[(long long)k * rows + i] : 0u;
-            }
-            const int ww = e % TN, kk = e / TN, k = k0 + kk;
-            const long long w = w0 + ww;
-            const bool ok = k < K && w < W;
-            ra[t] = ok ? (double)Xb[(long long)k * ldx + w] : 0.;
-            rb[t] = ok ? (double)Xb[(long long)(D.n - 1 - k) * ldx + w] : 0.;
+        for (int t = 0; t < 2; t++) {
+            const long long hk = (long long)(k0 + hr + 8 * t) * ip + i0 + hc;
+            hb[t] = *reinterpret_cast<const uint4 *>(Hb + hk);
+            hs[t] = *reinterpret_cast<const uint4 *>(Hs + hk);
+            const int k = k0 + xr + 8 * t;
+            const bool ok = k < K;
+            const TI *ra = Xb + (long long)k * ldx + w0 + xc, *rb = Xb + (long long)(D.n - 1 - k) * ldx + w0 + xc;
+            xa[t][0] = ok && ok0 ? ra[0] : TI(0);
+            xa[t][1] = ok && ok1 ? ra[1] : TI(0);
+            xb[t][0] = ok && ok0 ? rb[0] : TI(0);
+            xb[t][1] = ok && ok1 ? rb[1] : TI(0);
         }
     };
     auto stash = [&](int buf, int k0) {
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            sAb[buf][e / TM][e % TM] = rhb[t];
-            sAs[buf][e / TM][e % TM] = rhs[t];
-            const int ww = e % TN, kk = e / TN, k = k0 + kk;
-            unsigned big, small;
-            tf32_split(fold_value<float>(ra[t], rb[t], k == D.n - 1 - k, g), big, small);
-            sBb[buf][kk][ww] = big;
-            sBs[buf][kk][ww] = small;
+        for (int t = 0; t < 2; t++) {
+            *reinterpret_cast<uint4 *>(&sAb[buf][hr + 8 * t][hc]) = hb[t];
+            *reinterpret_cast<uint4 *>(&sAs[buf][hr + 8 * t][hc]) = hs[t];
+            const int k = k0 + xr + 8 * t;
+            const bool mid = k == D.n - 1 - k;
+            unsigned b0, s0, b1, s1;
+            tf32_split(fold_tf32<TI>(xa[t][0], xb[t][0], mid, g), b0, s0);
+            tf32_split(fold_tf32<TI>(xa[t][1], xb[t][1], mid, g), b1, s1);
+            *reinterpret_cast<uint2 *>(&sBb[buf][xr + 8 * t][xc]) = make_uint2(b0, b1);
+            *reinterpret_cast<uint2 *>(&sBs[buf][xr + 8 * t][xc]) = make_uint2(s0, s1);
         }
     };
     fetch(0);
     stash(0, 0);
     __syncthreads();
     int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += TK) {
-        const bool more = k0 + TK < K;
-        if (more) fetch(k0 + TK);
-        tf32_tile_product(sAb[buf], sAs[buf], sBb[buf], sBs[buf], lane, warp, facc);
-        if (more) stash(buf ^ 1, k0 + TK);
+    for (int k0 = 0; k0 < K; k0 += QK) {
+        const bool more = k0 + QK < K;
+        if (more) fetch(k0 + QK);
+#pragma unroll
+        for (int kb = 0; kb < QK; kb += 8) {
+            unsigned ab[2][4], as[2][4];
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                const int r = wm * 32 + a * 16 + gid;
+                ab[a][0] = sAb[buf][kb + tig][r];
+                ab[a][1] = sAb[buf][kb + tig][r + 8];
+                ab[a][2] = sAb[buf][kb + tig + 4][r];
+                ab[a][3] = sAb[buf][kb + tig + 4][r + 8];
+                as[a][0] = sAs[buf][kb + tig][r];
+                as[a][1] = sAs[buf][kb + tig][r + 8];
+                as[a][2] = sAs[buf][kb + tig + 4][r];
+                as[a][3] = sAs[buf][kb + tig + 4][r + 8];
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int col = wn * 32 + 8 * c + gid;
+                const unsigned b0b = sBb[buf][kb + tig][col], b0s = sBs[buf][kb + tig][col];
+                const unsigned b1b = sBb[buf][kb + tig + 4][col], b1s = sBs[buf][kb + tig + 4][col];
+#pragma unroll
+                for (int a = 0; a < 2; a++) {
+                    mma_tf32(facc[a][c], as[a], b0b, b1b);
+                    mma_tf32(facc[a][c], ab[a], b0s, b1s);
+                    mma_tf32(facc[a][c], ab[a], b0b, b1b);
+                }
+            }
+        }
+        if (more) stash(buf ^ 1, k0 + QK);
         __syncthreads();
         buf ^= 1;
     }
+    const long long cb = (long long)blockIdx.z * bs;
 #pragma unroll
-    for (int fc = 0; fc < 4; fc++)
+    for (int a = 0; a < 2; a++)
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int ii = i0 + wr + gid + 8 * (e >> 1);
-            const long long w = w0 + wc + 8 * fc + 2 * tig + (e & 1);
-            if (ii >= rows || w >= W) continue;
-            const long long o = b * bs + (long long)(2 * ii + g) * ldx + w;
-            double v = (double)facc[fc][e];
-            if (EPI == 1) v = v / den[o % per];
-            if (EPI == 2) v = sign * (post[o] * v);
-            C[o] = (TO)v;
-        }
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int ii = i0 + wm * 32 + a * 16 + gid + 8 * (e >> 1);
+                const long long w = w0 + wn * 32 + 8 * c + 2 * tig + (e & 1);
+                if (ii >= rows || w >= W) continue;
+                const long long io = (long long)(2 * ii + g) * ldx + w, o = cb + io;
+                double v = (double)facc[a][c][e];
+                if (EPI == 1) v = v / den[io];
+                if (EPI == 2) v = sign * (post[o] * v);
+                C[o] = (TO)v;
+            }
 }
 
-// Right pass in float32 (see dst_right_kernel): A = the folded rows split on staging, B = H_g^T from its parts.
-template <class TI, class TO>
-__global__ void __launch_bounds__(256) dst_right_tf32_kernel(HalfTf32 D, const TI *__restrict__ X, long long R,
+// Right pass along x over contiguous rows of length n: C[r][2i + g] = sum_k fold_g(pre X)[r][k] H_g[i][k], pre an
+// optional scale applied first.  3xTF32: A = the folded rows [row][k],
+// B = H_g tile [col][k] with 16 NT columns (NT n8 tiles per warp along the 2 column warps).
+template <int NT, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_right_tf32_kernel(PadTf32 D, const TI *__restrict__ X, long long R,
                                                              const double *__restrict__ pre, TO *__restrict__ C) {
-    __shared__ unsigned sAb[2][TK][TP], sAs[2][TK][TP], sBb[2][TK][TP], sBs[2][TK][TP];
+    constexpr int QN = 16 * NT;
+    extern __shared__ __align__(16) unsigned qsm[];
+    unsigned(*sAb)[QR][QPK] = reinterpret_cast<unsigned(*)[QR][QPK]>(qsm);
+    unsigned(*sAs)[QR][QPK] = reinterpret_cast<unsigned(*)[QR][QPK]>(qsm + 2 * QR * QPK);
+    unsigned(*sBb)[QN][QPK] = reinterpret_cast<unsigned(*)[QN][QPK]>(qsm + 4 * QR * QPK);
+    unsigned(*sBs)[QN][QPK] = reinterpret_cast<unsigned(*)[QN][QPK]>(qsm + 4 * QR * QPK + 2 * QN * QPK);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
-    const int wr = (warp >> 1) * 16, wc = (warp & 1) * 32;
-    const int t0 = (D.k0 + TN - 1) / TN;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int t0 = D.ipad[0] / QN;
     const int g = (int)blockIdx.x < t0 ? 0 : 1;
-    const int cols = g ? D.k1 : D.k0, K = cols;
-    const unsigned *Hb = g ? D.b1 : D.b0, *Hs = g ? D.s1 : D.s0;
-    const int i0 = (g ? (int)blockIdx.x - t0 : (int)blockIdx.x) * TN;
-    const long long r0 = (long long)blockIdx.y * TM;
+    const int cols = g ? D.kg[1] : D.kg[0], K = cols, kp = g ? D.kpad[1] : D.kpad[0];
+    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * QN;
+    const unsigned *Hb = g ? D.b[1] : D.b[0], *Hs = g ? D.s[1] : D.s[0];
+    const long long r0 = (long long)blockIdx.y * QR;
     const int n = D.n;
-    float facc[4][4] = {};
-    unsigned rhb[4], rhs[4];
-    double ra[4], rb[4];
-    auto fetch = [&](int k0) {
+    float facc[2][NT][4];
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            {
-                const int kk = e % TK, rr = e / TK, k = k0 + kk;
-                const long long r = r0 + rr;
-                const bool ok = r < R && k < K;
-                const long long a = r * n + k, m = r * n + (n - 1 - k);
-                ra[t] = ok ? (pre ? pre[a] * (double)X[a] : (double)X[a]) : 0.;
-                rb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int c = 0; c < NT; c++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) facc[a][c][e] = 0.f;
+    // staging: the field block (128 rows x 16 k, each with its mirror) as 8 entries per thread, 16 consecutive k of
+    // a row per half warp; the matrix block (16 NT rows x 16 k per part) as uint4 along k
+    const int xk = threadIdx.x & 15, xr = threadIdx.x >> 4;
+    constexpr int HV = QN * QK / 4, HT = (HV + 255) / 256;
+    TI xa[8], xb[8];
+    uint4 hb[HT], hs[HT];
+    auto fetch = [&](int k0) {
+        const int k = k0 + xk;
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            const long long r = r0 + xr + 16 * t;
+            const bool ok = r < R && k < K;
+            const long long a = r * n + k, m = r * n + (n - 1 - k);
+            if (pre) {
+                xa[t] = ok ? (TI)(pre[a] * (double)X[a]) : TI(0);
+                xb[t] = ok ? (TI)(pre[m] * (double)X[m]) : TI(0);
+            } else {
+                xa[t] = ok ? X[a] : TI(0);
+                xb[t] = ok ? X[m] : TI(0);
             }
-            const int ii = e % TN, kk = e / TN, i = i0 + ii, k = k0 + kk;
-            const bool ok = i < cols && k < K;
-            rhb[t] = ok ? Hb[(long long)k * cols + i] : 0u;
-            rhs[t] = ok ? Hs[(long long)k * cols + i] : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < HT; t++) {
+            const int v = threadIdx.x + 256 * t;
+            if (v < HV) {
+                const long long hk = (long long)(i0 + v / (QK / 4)) * kp + k0 + (v % (QK / 4)) * 4;
+                hb[t] = *reinterpret_cast<const uint4 *>(Hb + hk);
+                hs[t] = *reinterpret_cast<const uint4 *>(Hs + hk);
+            }
         }
     };
     auto stash = [&](int buf, int k0) {
+        const int k = k0 + xk;
+        const bool mid = k == n - 1 - k;
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int e = threadIdx.x + 256 * t;
-            const int kk = e % TK, k = k0 + kk;
-            unsigned big, small;
-            tf32_split(fold_value<float>(ra[t], rb[t], k == n - 1 - k, g), big, small);
-            sAb[buf][kk][e / TK] = big;
-            sAs[buf][kk][e / TK] = small;
-            sBb[buf][e / TN][e % TN] = rhb[t];
-            sBs[buf][e / TN][e % TN] = rhs[t];
+        for (int t = 0; t < 8; t++) {
+            unsigned b, s;
+            tf32_split(fold_tf32<TI>(xa[t], xb[t], mid, g), b, s);
+            sAb[buf][xr + 16 * t][xk] = b;
+            sAs[buf][xr + 16 * t][xk] = s;
+        }
+#pragma unroll
+        for (int t = 0; t < HT; t++) {
+            const int v = threadIdx.x + 256 * t;
+            if (v < HV) {
+                *reinterpret_cast<uint4 *>(&sBb[buf][v / (QK / 4)][(v % (QK / 4)) * 4]) = hb[t];
+                *reinterpret_cast<uint4 *>(&sBs[buf][v / (QK / 4)][(v % (QK / 4)) * 4]) = hs[t];
+            }
         }
     };
     fetch(0);
     stash(0, 0);
     __syncthreads();
     int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += TK) {
-        const bool more = k0 + TK < K;
-        if (more) fetch(k0 + TK);
-        tf32_tile_product(sAb[buf], sAs[buf], sBb[buf], sBs[buf], lane, warp, facc);
-        if (more) stash(buf ^ 1, k0 + TK);
+    for (int k0 = 0; k0 < K; k0 += QK) {
+        const bool more = k0 + QK < K;
+        if (more) fetch(k0 + QK);
+#pragma unroll
+        for (int kb = 0; kb < QK; kb += 8) {
+            unsigned ab[2][4], as[2][4];
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                const int r = wm * 32 + a * 16 + gid;
+                ab[a][0] = sAb[buf][r][kb + tig];
+                ab[a][1] = sAb[buf][r + 8][kb + tig];
+                ab[a][2] = sAb[buf][r][kb + tig + 4];
+                ab[a][3] = sAb[buf][r + 8][kb + tig + 4];
+                as[a][0] = sAs[buf][r][kb + tig];
+                as[a][1] = sAs[buf][r + 8][kb + tig];
+                as[a][2] = sAs[buf][r][kb + tig + 4];
+                as[a][3] = sAs[buf][r + 8][kb + tig + 4];
+            }
+#pragma unroll
+            for (int c = 0; c < NT; c++) {
+                const int col = wn * 8 * NT + 8 * c + gid;
+                const unsigned b0b = sBb[buf][col][kb + tig], b0s = sBs[buf][col][kb + tig];
+                const unsigned b1b = sBb[buf][col][kb + tig + 4], b1s = sBs[buf][col][kb + tig + 4];
+#pragma unroll
+                for (int a = 0; a < 2; a++) {
+                    mma_tf32(facc[a][c], as[a], b0b, b1b);
+                    mma_tf32(facc[a][c], ab[a], b0s, b1s);
+                    mma_tf32(facc[a][c], ab[a], b0b, b1b);
+                }
+            }
+        }
+        if (more) stash(buf ^ 1, k0 + QK);
         __syncthreads();
         buf ^= 1;
     }
 #pragma unroll
-    for (int fc = 0; fc < 4; fc++)
+    for (int a = 0; a < 2; a++)
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const long long r = r0 + wr + gid + 8 * (e >> 1);
-            const int ii = i0 + wc + 8 * fc + 2 * tig + (e & 1);
-            if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)facc[fc][e];
+        for (int c = 0; c < NT; c++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const long long r = r0 + wm * 32 + a * 16 + gid + 8 * (e >> 1);
+                const int ii = i0 + wn * 8 * NT + 8 * c + 2 * tig + (e & 1);
+                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)facc[a][c][e];
+            }
+}
+
+// right-pass column tile: 16 NT columns with NT = ceil(k0 / 16) in 3..8 (one tile per parity up to 128 columns)
+inline int right_nt(int k0) {
+    const int nt = (k0 + 15) / 16;
+    return nt < 3 ? 3 : (nt > 8 ? 8 : nt);
+}
+inline size_t left_tf32_smem() { return sizeof(unsigned) * 4 * QK * (QPA + QPB); }
+inline size_t right_tf32_smem(int nt) { return sizeof(unsigned) * 4 * QPK * (QR + 16 * nt); }
+
+// Padded TF32 tiles of one axis: the right pass (x) stores H_g row-major padded to column tiles of its width, the left
+// passes (y, z) H_g^T padded to 128-row tiles; K is padded to the K block.  Buffer: big g0, big g1, small g0, small g1.
+inline long long pad_geometry(int axis, int n, int kg[2], int ipad[2], int kpad[2]) {
+    kg[0] = (n + 1) / 2;
+    kg[1] = n / 2;
+    const int tile = axis == 0 ? 16 * right_nt(kg[0]) : QR;
+    for (int g = 0; g < 2; g++) {
+        ipad[g] = (kg[g] + tile - 1) / tile * tile;
+        kpad[g] = (kg[g] + QK - 1) / QK * QK;
+    }
+    return 2LL * ((long long)ipad[0] * kpad[0] + (long long)ipad[1] * kpad[1]);
+}
+inline PadTf32 pad_tf32(const unsigned *t, int axis, int n) {
+    PadTf32 T;
+    T.n = n;
+    pad_geometry(axis, n, T.kg, T.ipad, T.kpad);
+    const long long a0 = (long long)T.ipad[0] * T.kpad[0], a1 = (long long)T.ipad[1] * T.kpad[1];
+    T.b[0] = t;
+    T.b[1] = t + a0;
+    T.s[0] = t + a0 + a1;
+    T.s[1] = t + 2 * a0 + a1;
+    return T;
+}
+
+// the TF32 passes' shared memory is above the 48 KB default: set once per device (see allow_slices in q1.cu)
+template <int NT>
+int allow_right_tf32() {
+    SVP_CUDA(cudaFuncSetAttribute(dst_right_tf32_kernel<NT, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)right_tf32_smem(NT)));
+    SVP_CUDA(cudaFuncSetAttribute(dst_right_tf32_kernel<NT, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)right_tf32_smem(NT)));
+    return SVP_OK;
+}
+int allow_tf32() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    SVP_CUDA(cudaGetDevice(&dev));
+    SVP_REQUIRE(dev >= 0 && dev < 64, "allow_tf32: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return SVP_OK;
+    const int ls = (int)left_tf32_smem();
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_tf32_kernel<0, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_tf32_kernel<1, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_tf32_kernel<0, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_tf32_kernel<2, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    int rc;
+    if ((rc = allow_right_tf32<3>()) || (rc = allow_right_tf32<4>()) || (rc = allow_right_tf32<5>()) ||
+        (rc = allow_right_tf32<6>()) || (rc = allow_right_tf32<7>()) || (rc = allow_right_tf32<8>()))
+        return rc;
+    done[dev] = true;
+    return SVP_OK;
+}
+template <class TI, class TO>
+int launch_right_tf32(int nt, dim3 grid, const PadTf32 &T, const TI *in, long long R, const double *pre, TO *out,
+                      cudaStream_t s) {
+    const size_t sm = right_tf32_smem(nt);
+    switch (nt) {
+        case 3: SVP_LAUNCH((dst_right_tf32_kernel<3, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 4: SVP_LAUNCH((dst_right_tf32_kernel<4, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 5: SVP_LAUNCH((dst_right_tf32_kernel<5, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 6: SVP_LAUNCH((dst_right_tf32_kernel<6, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 7: SVP_LAUNCH((dst_right_tf32_kernel<7, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        default: SVP_LAUNCH((dst_right_tf32_kernel<8, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+    }
+    return SVP_OK;
+}
+
+// ------------------------------------------------------------------------------- plain form (FP64 DMMA), tiled
+// The float64 passes with the tiling of the 3xTF32 ones: zero-padded half matrices (pad_half_kernel, the same
+// geometry), a 128 x 64 (left) or 64 x 16 NT (right) output tile per block, 8 warps of 32 x 32 (16 x 8 NT) = 4 x 4
+// (2 x NT) DMMA 8x8x4 tiles, K blocks of 16 staged twice-buffered through registers.  Rows of the staged blocks are
+// padded to 4 mod 16 doubles, so the 64-bit fragment loads of each half warp fall in distinct bank pairs.  Every
+// output is the DMMA sequence over k in order (kb = 0, 4, 8, ...), the accumulation of a plain 8x8x4 tiling, so the
+// values do not depend on the tile shape.
+constexpr int DPA = QR + 4, DPB = QC + 4, DPK = QK + 4;
+
+struct PadF64 {
+    const double *h[2];   // per parity, zero-padded to kpad x ipad (left, k-major) or ipad x kpad (right)
+    int n, kg[2], ipad[2], kpad[2];
+};
+
+__global__ void pad_half_kernel(const double *__restrict__ h, int kg, long long src, int kmajor, int ipad, int kpad,
+                                double *__restrict__ out) {
+    const long long total = (long long)ipad * kpad;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int a = kmajor ? (int)(e % ipad) : (int)(e / kpad), k = kmajor ? (int)(e / ipad) : (int)(e % kpad);
+        out[e] = (a < kg && k < kg) ? h[src + (long long)a * kg + k] : 0.;
+    }
+}
+
+template <int EPI, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_left_dmma_kernel(PadF64 D, const TI *__restrict__ X, long long W,
+                                                            long long ldx, long long bs, TO *__restrict__ C,
+                                                            const double *__restrict__ den,
+                                                            const double *__restrict__ post, double sign) {
+    extern __shared__ __align__(16) double dsm[];
+    double(*sA)[QK][DPA] = reinterpret_cast<double(*)[QK][DPA]>(dsm);
+    double(*sB)[QK][DPB] = reinterpret_cast<double(*)[QK][DPB]>(dsm + 2 * QK * DPA);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int t0 = D.ipad[0] / QR;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
+    const int rows = g ? D.kg[1] : D.kg[0], K = rows, ip = g ? D.ipad[1] : D.ipad[0];
+    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * QR;
+    const double *H = g ? D.h[1] : D.h[0];
+    const long long w0 = (long long)blockIdx.y * QC;
+    const TI *Xb = X + (long long)blockIdx.z * bs;
+    double dacc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) dacc[a][c][0] = dacc[a][c][1] = 0.;
+    // staging: the matrix block (16 x 128) as four double2 per thread, the field block (16 x 64, with mirrors) as
+    // four entries per thread
+    const int hr = threadIdx.x >> 6, hc = (threadIdx.x & 63) * 2;
+    const int xr = threadIdx.x >> 6, xc = threadIdx.x & 63;
+    const bool okw = w0 + xc < W;
+    double2 hv[4];
+    TI xa[4], xb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            hv[t] = *reinterpret_cast<const double2 *>(H + (long long)(k0 + hr + 4 * t) * ip + i0 + hc);
+            const int k = k0 + xr + 4 * t;
+            const bool ok = okw && k < K;
+            xa[t] = ok ? Xb[(long long)k * ldx + w0 + xc] : TI(0);
+            xb[t] = ok ? Xb[(long long)(D.n - 1 - k) * ldx + w0 + xc] : TI(0);
         }
+    };
+    auto stash = [&](int buf, int k0) {
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            *reinterpret_cast<double2 *>(&sA[buf][hr + 4 * t][hc]) = hv[t];
+            const int k = k0 + xr + 4 * t;
+            sB[buf][xr + 4 * t][xc] = fold_value<double>((double)xa[t], (double)xb[t], k == D.n - 1 - k, g);
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += QK) {
+        const bool more = k0 + QK < K;
+        if (more) fetch(k0 + QK);
+#pragma unroll
+        for (int kb = 0; kb < QK; kb += 4) {
+            double a[4], x[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) a[m] = sA[buf][kb + tig][wm * 32 + 8 * m + gid];
+#pragma unroll
+            for (int c = 0; c < 4; c++) x[c] = sB[buf][kb + tig][wn * 32 + 8 * c + gid];
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) dmma_8x8x4(dacc[m][c], a[m], x[c]);
+        }
+        if (more) stash(buf ^ 1, k0 + QK);
+        __syncthreads();
+        buf ^= 1;
+    }
+    const long long cb = (long long)blockIdx.z * bs;
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int ii = i0 + wm * 32 + 8 * m + gid;
+                const long long w = w0 + wn * 32 + 8 * c + 2 * tig + e;
+                if (ii >= rows || w >= W) continue;
+                const long long io = (long long)(2 * ii + g) * ldx + w, o = cb + io;
+                double v = dacc[m][c][e];
+                if (EPI == 1) v = v / den[io];
+                if (EPI == 2) v = sign * (post[o] * v);
+                C[o] = (TO)v;
+            }
+}
+
+// MR m8 row tiles per warp: a block covers 32 MR rows (4 row warps) x 16 NT columns (2 column warps).
+template <int MR, int NT, class TI, class TO>
+__global__ void __launch_bounds__(256) dst_right_dmma_kernel(PadF64 D, const TI *__restrict__ X, long long R,
+                                                             const double *__restrict__ pre, TO *__restrict__ C) {
+    constexpr int QN = 16 * NT, RB = 32 * MR, XT = RB / 16;
+    extern __shared__ __align__(16) double dsm[];
+    double(*sA)[RB][DPK] = reinterpret_cast<double(*)[RB][DPK]>(dsm);
+    double(*sB)[QN][DPK] = reinterpret_cast<double(*)[QN][DPK]>(dsm + 2 * RB * DPK);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int t0 = D.ipad[0] / QN;
+    const int g = (int)blockIdx.x < t0 ? 0 : 1;
+    const int cols = g ? D.kg[1] : D.kg[0], K = cols, kp = g ? D.kpad[1] : D.kpad[0];
+    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * QN;
+    const double *H = g ? D.h[1] : D.h[0];
+    const long long r0 = (long long)blockIdx.y * RB;
+    const int n = D.n;
+    double dacc[MR][NT][2];
+#pragma unroll
+    for (int a = 0; a < MR; a++)
+#pragma unroll
+        for (int c = 0; c < NT; c++) dacc[a][c][0] = dacc[a][c][1] = 0.;
+    const int xk = threadIdx.x & 15, xr = threadIdx.x >> 4;
+    constexpr int HV = QN * QK / 2, HT = (HV + 255) / 256;
+    double xa[XT], xb[XT];
+    double2 hv[HT];
+    auto fetch = [&](int k0) {
+        const int k = k0 + xk;
+#pragma unroll
+        for (int t = 0; t < XT; t++) {
+            const long long r = r0 + xr + 16 * t;
+            const bool ok = r < R && k < K;
+            const long long a = r * n + k, m = r * n + (n - 1 - k);
+            xa[t] = ok ? (pre ? pre[a] * (double)X[a] : (double)X[a]) : 0.;
+            xb[t] = ok ? (pre ? pre[m] * (double)X[m] : (double)X[m]) : 0.;
+        }
+#pragma unroll
+        for (int t = 0; t < HT; t++) {
+            const int v = threadIdx.x + 256 * t;
+            if (v < HV)
+                hv[t] = *reinterpret_cast<const double2 *>(H + (long long)(i0 + v / (QK / 2)) * kp + k0 +
+                                                           (v % (QK / 2)) * 2);
+        }
+    };
+    auto stash = [&](int buf, int k0) {
+        const int k = k0 + xk;
+        const bool mid = k == n - 1 - k;
+#pragma unroll
+        for (int t = 0; t < XT; t++) sA[buf][xr + 16 * t][xk] = fold_value<double>(xa[t], xb[t], mid, g);
+#pragma unroll
+        for (int t = 0; t < HT; t++) {
+            const int v = threadIdx.x + 256 * t;
+            if (v < HV) *reinterpret_cast<double2 *>(&sB[buf][v / (QK / 2)][(v % (QK / 2)) * 2]) = hv[t];
+        }
+    };
+    fetch(0);
+    stash(0, 0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += QK) {
+        const bool more = k0 + QK < K;
+        if (more) fetch(k0 + QK);
+#pragma unroll
+        for (int kb = 0; kb < QK; kb += 4) {
+            double a[MR], x[NT];
+#pragma unroll
+            for (int m = 0; m < MR; m++) a[m] = sA[buf][wm * 8 * MR + 8 * m + gid][kb + tig];
+#pragma unroll
+            for (int c = 0; c < NT; c++) x[c] = sB[buf][wn * 8 * NT + 8 * c + gid][kb + tig];
+#pragma unroll
+            for (int m = 0; m < MR; m++)
+#pragma unroll
+                for (int c = 0; c < NT; c++) dmma_8x8x4(dacc[m][c], a[m], x[c]);
+        }
+        if (more) stash(buf ^ 1, k0 + QK);
+        __syncthreads();
+        buf ^= 1;
+    }
+#pragma unroll
+    for (int m = 0; m < MR; m++)
+#pragma unroll
+        for (int c = 0; c < NT; c++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const long long r = r0 + wm * 8 * MR + 8 * m + gid;
+                const int ii = i0 + wn * 8 * NT + 8 * c + 2 * tig + e;
+                if (r < R && ii < cols) C[r * n + 2 * ii + g] = (TO)dacc[m][c][e];
+            }
+}
+
+inline size_t left_dmma_smem() { return sizeof(double) * 2 * QK * (DPA + DPB); }
+// the right float64 pass: 64-row blocks (2 m8 tiles per warp) keep two 256-thread blocks resident per SM
+constexpr int DMR = 2;
+inline size_t right_dmma_smem(int nt) { return sizeof(double) * 2 * DPK * (32 * DMR + 16 * nt); }
+inline PadF64 pad_f64(const double *t, int axis, int n) {
+    PadF64 T;
+    T.n = n;
+    pad_geometry(axis, n, T.kg, T.ipad, T.kpad);
+    T.h[0] = t;
+    T.h[1] = t + (long long)T.ipad[0] * T.kpad[0];
+    return T;
+}
+template <int NT>
+int allow_right_dmma() {
+    SVP_CUDA(cudaFuncSetAttribute(dst_right_dmma_kernel<DMR, NT, double, double>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)right_dmma_smem(NT)));
+    return SVP_OK;
+}
+int allow_dmma() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    SVP_CUDA(cudaGetDevice(&dev));
+    SVP_REQUIRE(dev >= 0 && dev < 64, "allow_dmma: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return SVP_OK;
+    const int ls = (int)left_dmma_smem();
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<0, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<1, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<2, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    int rc;
+    if ((rc = allow_right_dmma<3>()) || (rc = allow_right_dmma<4>()) || (rc = allow_right_dmma<5>()) ||
+        (rc = allow_right_dmma<6>()) || (rc = allow_right_dmma<7>()) || (rc = allow_right_dmma<8>()))
+        return rc;
+    done[dev] = true;
+    return SVP_OK;
+}
+template <class TI, class TO>
+int launch_right_dmma(int nt, dim3 grid, const PadF64 &T, const TI *in, long long R, const double *pre, TO *out,
+                      cudaStream_t s) {
+    const size_t sm = right_dmma_smem(nt);
+    switch (nt) {
+        case 3: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 3, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 4: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 4, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 5: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 5, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 6: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 6, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        case 7: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 7, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+        default: SVP_LAUNCH((dst_right_dmma_kernel<DMR, 8, TI, TO><<<grid, 256, sm, s>>>(T, in, R, pre, out))); break;
+    }
+    return SVP_OK;
 }
 
 __global__ void scale_kernel(const double *__restrict__ x, const double *__restrict__ s, double sign, long long n,
@@ -571,41 +822,49 @@ int apply_axis(const double *M, int axis, long long batch, long long n2, long lo
 
 std::vector<double> dst1_matrix(int n);
 
-// One DST-I pass along `axis` of (3, n2, n1, n0) fields with the folded half matrices; see dst_left_kernel for
+// One DST-I pass along `axis` of (3, n2, n1, n0) fields with the folded half matrices; see dst_left_tf32_kernel for
 // pre / EPI.
 template <class TC, class TI, class TO>
 static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const double *pre, int epi, double sign,
                     const double *post, cudaStream_t s) {
     const long long n0 = p->q.fx, n1 = p->q.fy, n2 = p->q.fz;
-    const int n = p->dst_n[axis], k0 = (n + 1) / 2, k1 = n / 2;
-    const unsigned tiles = (unsigned)(div_up(k0, TM) + div_up(k1, TM));
-    const long long nf = p->q.nfree;
+    const int n = p->dst_n[axis], k0 = (n + 1) / 2;
     constexpr bool kDouble = sizeof(TC) == 8;
-    HalfDst D{p->dst_half[axis], p->dst_half[axis] + (size_t)k0 * k0, n, k0, k1};
-    const unsigned *t = p->dst_tf32[axis];
-    const long long tot = (long long)k0 * k0 + (long long)k1 * k1;
-    HalfTf32 T{t, t + tot, t + (long long)k0 * k0, t + tot + (long long)k0 * k0, n, k0, k1};
+    PadF64 D = pad_f64(p->dst_pad[axis], axis, n);
+    PadTf32 T = pad_tf32(p->dst_tf32[axis], axis, n);
+    {
+        int rc = kDouble ? allow_dmma() : allow_tf32();
+        if (rc) return rc;
+    }
     if (axis == 0) {
         SVP_REQUIRE(epi == 0, "dst_pass: x pass has no epilogue");
         long long R = 3 * n2 * n1;
-        dim3 grid(tiles, (unsigned)div_up(R, TM));      // the blocks that share rows run together (L2 reuse)
         svp::KernelTimer _t("dst_right_kernel", s);
-        if constexpr (kDouble) SVP_LAUNCH((dst_right_kernel<TI, TO><<<grid, 256, 0, s>>>(D, in, R, pre, out)));
-        else SVP_LAUNCH((dst_right_tf32_kernel<TI, TO><<<grid, 256, 0, s>>>(T, in, R, pre, out)));
+        // the column tiles of one row block lead the grid: the blocks that share rows run together (L2 reuse)
+        const int nt = right_nt(k0);
+        dim3 grid((unsigned)((T.ipad[0] + T.ipad[1]) / (16 * nt)), (unsigned)div_up(R, kDouble ? 32 * DMR : QR));
+        int rc;
+        if constexpr (kDouble) rc = launch_right_dmma<TI, TO>(nt, grid, D, in, R, pre, out, s);
+        else rc = launch_right_tf32<TI, TO>(nt, grid, T, in, R, pre, out, s);
+        if (rc) return rc;
     } else {
         SVP_REQUIRE(!pre, "dst_pass: pre-scale only on the x pass");
+        SVP_REQUIRE(epi != 1 || axis == 2, "dst_pass: the 1/den epilogue rides in the z pass (batch stride = nfree)");
         long long W = axis == 1 ? n0 : n1 * n0;
         long long ldx = W, bs = axis == 1 ? n1 * n0 : n2 * n1 * n0;
-        dim3 grid(tiles, (unsigned)div_up(W, TN), (unsigned)(axis == 1 ? 3 * n2 : 3));
+        // the row tiles of both parities lead the grid: the blocks that read the same field columns run together
+        dim3 qgrid((unsigned)((T.ipad[0] + T.ipad[1]) / QR), (unsigned)div_up(W, QC), (unsigned)(axis == 1 ? 3 * n2 : 3));
         svp::KernelTimer _t("dst_left_kernel", s);
         if constexpr (kDouble) {
-            if (epi == 0) SVP_LAUNCH((dst_left_kernel<0, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
-            else if (epi == 1) SVP_LAUNCH((dst_left_kernel<1, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
-            else SVP_LAUNCH((dst_left_kernel<2, TI, TO><<<grid, 256, 0, s>>>(D, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+            const size_t ds = left_dmma_smem();
+            if (epi == 0) SVP_LAUNCH((dst_left_dmma_kernel<0, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_dmma_kernel<1, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, p->den, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_dmma_kernel<2, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, post, sign)));
         } else {
-            if (epi == 0) SVP_LAUNCH((dst_left_tf32_kernel<0, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, nullptr, 1, nullptr, 1.)));
-            else if (epi == 1) SVP_LAUNCH((dst_left_tf32_kernel<1, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, p->den, nf, nullptr, 1.)));
-            else SVP_LAUNCH((dst_left_tf32_kernel<2, TI, TO><<<grid, 256, 0, s>>>(T, in, W, ldx, bs, out, nullptr, 1, post, sign)));
+            const size_t qs = left_tf32_smem();
+            if (epi == 0) SVP_LAUNCH((dst_left_tf32_kernel<0, TI, TO><<<qgrid, 256, qs, s>>>(T, in, W, ldx, bs, out, nullptr, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_tf32_kernel<1, TI, TO><<<qgrid, 256, qs, s>>>(T, in, W, ldx, bs, out, p->den, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_tf32_kernel<2, TI, TO><<<qgrid, 256, qs, s>>>(T, in, W, ldx, bs, out, nullptr, post, sign)));
         }
     }
     SVP_LAUNCH_CHECK("dst pass");
@@ -661,17 +920,37 @@ int pair_dst_setup(svp_pair *p) {
         std::vector<double> H = cached_dst1_half((int)f[k]);
         SVP_CUDA(cudaMalloc((void **)&p->dst_half[k], sizeof(double) * H.size()));
         SVP_CUDA(cudaMemcpy(p->dst_half[k], H.data(), sizeof(double) * H.size(), cudaMemcpyHostToDevice));
+        {
+            int kg[2], ipad[2], kpad[2];
+            const long long words = pad_geometry(k, (int)f[k], kg, ipad, kpad) / 2;
+            SVP_CUDA(cudaMalloc((void **)&p->dst_pad[k], sizeof(double) * words));
+            const PadF64 T = pad_f64(p->dst_pad[k], k, (int)f[k]);
+            for (int g = 0; g < 2; g++) {
+                pad_half_kernel<<<blocks_for((long long)ipad[g] * kpad[g], 256, 4), 256>>>(
+                    p->dst_half[k], kg[g], g ? (long long)kg[0] * kg[0] : 0, k != 0, ipad[g], kpad[g],
+                    const_cast<double *>(T.h[g]));
+                SVP_CUDA(cudaGetLastError());
+            }
+            SVP_CUDA(cudaStreamSynchronize(0));
+        }
         // the mixed form's matrices: rounded once to float32, then split into TF32 parts on the device (the same
         // cvt.rna the passes use for their staged operands)
         std::vector<float> H32(H.begin(), H.end());
         float *h32 = nullptr;
         SVP_CUDA(cudaMalloc((void **)&h32, sizeof(float) * H32.size()));
         cudaError_t e = cudaMemcpy(h32, H32.data(), sizeof(float) * H32.size(), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&p->dst_tf32[k], sizeof(unsigned) * 2 * H32.size());
+        int kg[2], ipad[2], kpad[2];
+        const long long words = pad_geometry(k, (int)f[k], kg, ipad, kpad);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&p->dst_tf32[k], sizeof(unsigned) * words);
         if (e == cudaSuccess) {
-            split_half_kernel<<<blocks_for((long long)H32.size(), 256, 4), 256>>>(h32, (int)(f[k] + 1) / 2,
-                                                                                 (int)f[k] / 2, p->dst_tf32[k]);
-            e = cudaGetLastError();
+            const PadTf32 T = pad_tf32(p->dst_tf32[k], k, (int)f[k]);
+            for (int g = 0; g < 2 && e == cudaSuccess; g++) {
+                const long long src = g ? (long long)kg[0] * kg[0] : 0;
+                split_pad_kernel<<<blocks_for((long long)ipad[g] * kpad[g], 256, 4), 256>>>(
+                    h32, kg[g], src, k != 0, ipad[g], kpad[g], const_cast<unsigned *>(T.b[g]),
+                    const_cast<unsigned *>(T.s[g]));
+                e = cudaGetLastError();
+            }
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(0);
         cudaFree(h32);

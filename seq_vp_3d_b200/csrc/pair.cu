@@ -190,7 +190,7 @@ extern "C" int svp_pair_destroy(svp_pair *p) {
     if (!p) return SVP_OK;
     cudaFree(p->fixed); cudaFree(p->coeff); cudaFree(p->u_ref);
     for (int k = 0; k < 3; k++) {
-        cudaFree(p->knots[k]); cudaFree(p->spline_rcp[k]); cudaFree(p->dst_half[k]); cudaFree(p->dst_tf32[k]);
+        cudaFree(p->knots[k]); cudaFree(p->spline_rcp[k]); cudaFree(p->dst_half[k]); cudaFree(p->dst_pad[k]); cudaFree(p->dst_tf32[k]);
     }
     cudaFree(p->loc1); cudaFree(p->loc2); cudaFree(p->cellbuf); cudaFree(p->partial); cudaFree(p->result);
     cudaFree(p->counter); cudaFree(p->cand); cudaFree(p->flags); cudaFree(p->dst_tmp); cudaFree(p->den);

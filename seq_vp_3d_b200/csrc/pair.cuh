@@ -24,6 +24,7 @@ struct svp_pair {
     uint8_t *flags = nullptr;                 // (ncell) cells the float32 cell kernels hand to the float64 barrier
     // DST-I Poisson metric
     double *dst_half[3] = {nullptr, nullptr, nullptr};  // folded orthonormal DST-I half matrices, x, y, z
+    double *dst_pad[3] = {nullptr, nullptr, nullptr};   // the same zero-padded to the passes' tiles (PadF64)
     int dst_n[3] = {0, 0, 0};                               // their transform lengths (free nodes per axis)
     // the same rounded to float32 for the mixed form, as TF32 parts: big parts of H0^T, H1^T, then the small parts
     unsigned *dst_tf32[3] = {nullptr, nullptr, nullptr};
