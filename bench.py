@@ -179,6 +179,8 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12    # nominal: 148 SMs x 128 FP
 # traffic_cell_trial_edge_hull_warp_160x192x96.md); scaled to a launch by the cells it processes (traffic grows with
 # the cell count: every launch streams its fields once, plus neighbour re-reads of the same order)
 TRAFFIC_PER_CELL = {"cell_trial_kernel": (325667584 + 1371392) / 2885055,
+                    # full size, 160x192x224 (6,772,287 cells; profiles/cell_kernels_head_pair_160x192x224.md)
+                    "cell_trial32_kernel": (813766656 + 19263232) / 6772287,
                     "edge_hull_kernel": (74312512 + 8776576) / 2885055,
                     "warp_trial_kernel_grad": (312493568 + 74758400) / 2885055}
 
