@@ -532,7 +532,7 @@ int launch_right_tf32(int nt, dim3 grid, const PadTf32 &T, const TI *in, long lo
 // padded to 4 mod 16 doubles, so the 64-bit fragment loads of each half warp fall in distinct bank pairs.  Every
 // output is the DMMA sequence over k in order (kb = 0, 4, 8, ...), the accumulation of a plain 8x8x4 tiling, so the
 // values do not depend on the tile shape.
-constexpr int DPA = QR + 4, DPB = QC + 4, DPK = QK + 4;
+constexpr int DPB = QC + 4, DPK = QK + 4;
 
 struct PadF64 {
     const double *h[2];   // per parity, zero-padded to kpad x ipad (left, k-major) or ipad x kpad (right)
@@ -549,39 +549,45 @@ __global__ void pad_half_kernel(const double *__restrict__ h, int kg, long long 
     }
 }
 
-template <int EPI, class TI, class TO>
+// MR m8 row tiles per warp: a block covers 32 MR rows (4 row warps) x 64 columns (2 column warps).
+template <int MR, int EPI, class TI, class TO>
 __global__ void __launch_bounds__(256) dst_left_dmma_kernel(PadF64 D, const TI *__restrict__ X, long long W,
                                                             long long ldx, long long bs, TO *__restrict__ C,
                                                             const double *__restrict__ den,
                                                             const double *__restrict__ post, double sign) {
+    constexpr int RB = 32 * MR, PA = RB + 4;
     extern __shared__ __align__(16) double dsm[];
-    double(*sA)[QK][DPA] = reinterpret_cast<double(*)[QK][DPA]>(dsm);
-    double(*sB)[QK][DPB] = reinterpret_cast<double(*)[QK][DPB]>(dsm + 2 * QK * DPA);
+    double(*sA)[QK][PA] = reinterpret_cast<double(*)[QK][PA]>(dsm);
+    double(*sB)[QK][DPB] = reinterpret_cast<double(*)[QK][DPB]>(dsm + 2 * QK * PA);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
     const int wm = warp >> 1, wn = warp & 1;
-    const int t0 = D.ipad[0] / QR;
+    const int t0 = D.ipad[0] / RB;
     const int g = (int)blockIdx.x < t0 ? 0 : 1;
     const int rows = g ? D.kg[1] : D.kg[0], K = rows, ip = g ? D.ipad[1] : D.ipad[0];
-    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * QR;
+    const int i0 = ((int)blockIdx.x - (g ? t0 : 0)) * RB;
     const double *H = g ? D.h[1] : D.h[0];
     const long long w0 = (long long)blockIdx.y * QC;
     const TI *Xb = X + (long long)blockIdx.z * bs;
-    double dacc[4][4][2];
+    double dacc[MR][4][2];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < MR; a++)
 #pragma unroll
         for (int c = 0; c < 4; c++) dacc[a][c][0] = dacc[a][c][1] = 0.;
-    // staging: the matrix block (16 x 128) as four double2 per thread, the field block (16 x 64, with mirrors) as
-    // four entries per thread
-    const int hr = threadIdx.x >> 6, hc = (threadIdx.x & 63) * 2;
+    // staging: the matrix block (16 x 32 MR) as MR double2 per thread (16 MR per row), the field block (16 x 64,
+    // with mirrors) as four entries per thread
     const int xr = threadIdx.x >> 6, xc = threadIdx.x & 63;
     const bool okw = w0 + xc < W;
-    double2 hv[4];
+    double2 hv[MR];
     TI xa[4], xb[4];
     auto fetch = [&](int k0) {
 #pragma unroll
+        for (int t = 0; t < MR; t++) {
+            const int v = threadIdx.x + 256 * t;
+            hv[t] = *reinterpret_cast<const double2 *>(H + (long long)(k0 + v / (16 * MR)) * ip + i0 +
+                                                       (v % (16 * MR)) * 2);
+        }
+#pragma unroll
         for (int t = 0; t < 4; t++) {
-            hv[t] = *reinterpret_cast<const double2 *>(H + (long long)(k0 + hr + 4 * t) * ip + i0 + hc);
             const int k = k0 + xr + 4 * t;
             const bool ok = okw && k < K;
             xa[t] = ok ? Xb[(long long)k * ldx + w0 + xc] : TI(0);
@@ -590,8 +596,12 @@ __global__ void __launch_bounds__(256) dst_left_dmma_kernel(PadF64 D, const TI *
     };
     auto stash = [&](int buf, int k0) {
 #pragma unroll
+        for (int t = 0; t < MR; t++) {
+            const int v = threadIdx.x + 256 * t;
+            *reinterpret_cast<double2 *>(&sA[buf][v / (16 * MR)][(v % (16 * MR)) * 2]) = hv[t];
+        }
+#pragma unroll
         for (int t = 0; t < 4; t++) {
-            *reinterpret_cast<double2 *>(&sA[buf][hr + 4 * t][hc]) = hv[t];
             const int k = k0 + xr + 4 * t;
             sB[buf][xr + 4 * t][xc] = fold_value<double>((double)xa[t], (double)xb[t], k == D.n - 1 - k, g);
         }
@@ -605,13 +615,13 @@ __global__ void __launch_bounds__(256) dst_left_dmma_kernel(PadF64 D, const TI *
         if (more) fetch(k0 + QK);
 #pragma unroll
         for (int kb = 0; kb < QK; kb += 4) {
-            double a[4], x[4];
+            double a[MR], x[4];
 #pragma unroll
-            for (int m = 0; m < 4; m++) a[m] = sA[buf][kb + tig][wm * 32 + 8 * m + gid];
+            for (int m = 0; m < MR; m++) a[m] = sA[buf][kb + tig][wm * 8 * MR + 8 * m + gid];
 #pragma unroll
             for (int c = 0; c < 4; c++) x[c] = sB[buf][kb + tig][wn * 32 + 8 * c + gid];
 #pragma unroll
-            for (int m = 0; m < 4; m++)
+            for (int m = 0; m < MR; m++)
 #pragma unroll
                 for (int c = 0; c < 4; c++) dmma_8x8x4(dacc[m][c], a[m], x[c]);
         }
@@ -621,12 +631,12 @@ __global__ void __launch_bounds__(256) dst_left_dmma_kernel(PadF64 D, const TI *
     }
     const long long cb = (long long)blockIdx.z * bs;
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int m = 0; m < MR; m++)
 #pragma unroll
         for (int c = 0; c < 4; c++)
 #pragma unroll
             for (int e = 0; e < 2; e++) {
-                const int ii = i0 + wm * 32 + 8 * m + gid;
+                const int ii = i0 + wm * 8 * MR + 8 * m + gid;
                 const long long w = w0 + wn * 32 + 8 * c + 2 * tig + e;
                 if (ii >= rows || w >= W) continue;
                 const long long io = (long long)(2 * ii + g) * ldx + w, o = cb + io;
@@ -727,7 +737,9 @@ __global__ void __launch_bounds__(256) dst_right_dmma_kernel(PadF64 D, const TI 
             }
 }
 
-inline size_t left_dmma_smem() { return sizeof(double) * 2 * QK * (DPA + DPB); }
+// the left float64 passes: DML m8 row tiles per warp (blocks of 32 DML rows)
+constexpr int DML = 4;
+inline size_t left_dmma_smem() { return sizeof(double) * 2 * QK * (32 * DML + 4 + DPB); }
 // the right float64 pass: 64-row blocks (2 m8 tiles per warp) keep two 256-thread blocks resident per SM
 constexpr int DMR = 2;
 inline size_t right_dmma_smem(int nt) { return sizeof(double) * 2 * DPK * (32 * DMR + 16 * nt); }
@@ -754,9 +766,9 @@ int allow_dmma() {
     std::lock_guard<std::mutex> lock(mu);
     if (done[dev]) return SVP_OK;
     const int ls = (int)left_dmma_smem();
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<0, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<1, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
-    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<2, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<DML, 0, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<DML, 1, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
+    SVP_CUDA(cudaFuncSetAttribute(dst_left_dmma_kernel<DML, 2, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls));
     int rc;
     if ((rc = allow_right_dmma<3>()) || (rc = allow_right_dmma<4>()) || (rc = allow_right_dmma<5>()) ||
         (rc = allow_right_dmma<6>()) || (rc = allow_right_dmma<7>()) || (rc = allow_right_dmma<8>()))
@@ -857,9 +869,10 @@ static int dst_pass(const svp_pair *p, int axis, const TI *in, TO *out, const do
         svp::KernelTimer _t("dst_left_kernel", s);
         if constexpr (kDouble) {
             const size_t ds = left_dmma_smem();
-            if (epi == 0) SVP_LAUNCH((dst_left_dmma_kernel<0, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, nullptr, 1.)));
-            else if (epi == 1) SVP_LAUNCH((dst_left_dmma_kernel<1, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, p->den, nullptr, 1.)));
-            else SVP_LAUNCH((dst_left_dmma_kernel<2, TI, TO><<<qgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, post, sign)));
+            dim3 dgrid((unsigned)((D.ipad[0] + D.ipad[1]) / (32 * DML)), qgrid.y, qgrid.z);
+            if (epi == 0) SVP_LAUNCH((dst_left_dmma_kernel<DML, 0, TI, TO><<<dgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, nullptr, 1.)));
+            else if (epi == 1) SVP_LAUNCH((dst_left_dmma_kernel<DML, 1, TI, TO><<<dgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, p->den, nullptr, 1.)));
+            else SVP_LAUNCH((dst_left_dmma_kernel<DML, 2, TI, TO><<<dgrid, 256, ds, s>>>(D, in, W, ldx, bs, out, nullptr, post, sign)));
         } else {
             const size_t qs = left_tf32_smem();
             if (epi == 0) SVP_LAUNCH((dst_left_tf32_kernel<0, TI, TO><<<qgrid, 256, qs, s>>>(T, in, W, ldx, bs, out, nullptr, nullptr, 1.)));
