@@ -470,8 +470,9 @@ def parity_leg(grid, fixed, moving, weights, u_dev, planes):
                                          bound_at_least_plain=bool(rd.min_jd_lower_bound is not None and
                                                                    r.min_jd_lower_bound is not None and
                                                                    rd.min_jd_lower_bound >= r.min_jd_lower_bound))
-    mixed["note"] = ("float32 gradient / GGN diagonal / DST-I against the float64 path on the final state; energies, "
-                     "differences and decisions are float64 in both forms")
+    mixed["note"] = ("float32 gradient / GGN diagonal / DST-I against the float64 path on the final state; the "
+                     "energies of record are float64 in both forms (energy_terms_rel); the mixed form screens its E "
+                     "differences in float32 and retakes them in float64 near every decision (result.screen)")
     out["mixed_form_errors"] = mixed
     del pair, mp, warped, image_grad, g_dev
     # DST-I apply at full size
