@@ -261,3 +261,29 @@ def test_vector_kernels_bitwise(big):
         pos, neg = v[r] > 0, v[r] < 0
         best = min(best, np.min((axis[-1] - pts[..., r][pos]) / v[r][pos]), np.min((axis[0] - pts[..., r][neg]) / v[r][neg]))
     assert P.step_bound(ud, dev(p)) == best
+
+
+@pytest.mark.parametrize("shape", [(9, 10, 263), (10, 261, 9), (260, 9, 10), (7, 8, 11)])
+def test_poisson_apply_tile_edges(shape):
+    """The folded DST-I passes where a half axis spans more than one 128-wide tile (x: 261 free nodes, k0 = 131;
+    y: 259, odd, with the middle row; z: 258) and on a grid of short odd and even axes, in both forms, against the
+    oracle's dense float64 DST-I (oracle/q1.py poisson_apply, scipy's dstn type 1 'ortho' restated), with and without
+    the scale and sign epilogue.  Plain within 1e-12, mixed (3xTF32) within the mixed form's 1e-5."""
+    from seq_vp_3d_b200.grid import make_grid_3d
+    from seq_vp_3d_b200.pair import DevicePair
+    nz, ny, nx = shape
+    spacing = (1.0, 0.9, 1.1)
+    rng = np.random.default_rng(11)
+    grid = make_grid_3d(nx=nx, ny=ny, nz=nz, hx=spacing[0], hy=spacing[1], hz=spacing[2], unit="mm")
+    og = Q.make_grid(shape, spacing)
+    img = rng.random(shape)
+    nf = 3 * int(np.prod(og.interior_shape))
+    rhs = rng.normal(size=nf)
+    scale = rng.random(nf) + .5
+    a, b = 0.02, 0.03
+    ref = Q.poisson_apply(og, a, b, rhs)
+    ref_scaled = -scale * Q.poisson_apply(og, a, b, scale * rhs)
+    for form, tol in (("plain", TOL), ("mixed", 1e-5)):
+        P = DevicePair(grid, img, img, np.zeros(shape + (3,)), lam=a, mu=.03, nu=.03, kappa=.002, precision=form)
+        assert rel(P.poisson_apply(a, b, dev(rhs)), ref) < tol, form
+        assert rel(P.poisson_apply(a, b, dev(rhs), scale=dev(scale), sign=-1.), ref_scaled) < tol, form
