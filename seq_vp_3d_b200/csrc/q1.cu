@@ -629,11 +629,28 @@ __device__ __forceinline__ void for_flagged_cells(const Q1Const &q, const uint8_
     long long k = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     long long b = k * kFlagChunk;
     int qn = 0;
+    // a chunk's 256 flags are read once, 8 per lane (one 64-bit load where the chunk is whole and aligned), and the
+    // flag of cell chunk + 32 j + l is byte l % 8 of lane 4 j + l / 8's word; cells past the end read as zero
+    const bool wide = (reinterpret_cast<uintptr_t>(flags) & 7) == 0;
+    unsigned long long word = 0;
     for (;;) {
         // fill the queue to a full warp's worth, or until the warp's chunks are exhausted
         while (qn < 32 && k < nchunk) {
-            const long long hi = min((k + 1) * kFlagChunk, q.ncell), c = b + lane;
-            const bool on = c < hi && flags[c] != 0;
+            const long long c0 = k * kFlagChunk, hi = min(c0 + kFlagChunk, q.ncell), c = b + lane;
+            if (b == c0) {
+                const long long f0 = c0 + 8 * lane;
+                if (wide && c0 + kFlagChunk <= q.ncell) {
+                    word = *reinterpret_cast<const unsigned long long *>(flags + f0);
+                } else {
+                    word = 0;
+#pragma unroll
+                    for (int t = 0; t < 8; t++)
+                        if (f0 + t < q.ncell) word |= (unsigned long long)flags[f0 + t] << (8 * t);
+                }
+            }
+            const int j = (int)((b - c0) >> 5);
+            const unsigned long long v = __shfl_sync(0xFFFFFFFFu, word, 4 * j + (lane >> 3));
+            const bool on = c < hi && ((v >> (8 * (lane & 7))) & 0xFFull) != 0;
             const unsigned m = __ballot_sync(0xFFFFFFFFu, on);
             if (on) queue[qn + __popc(m & ((1u << lane) - 1u))] = c;
             qn += __popc(m);
