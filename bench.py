@@ -231,6 +231,49 @@ STATE_DEPENDENT_KERNELS = ("prescreen_kernel", "fallback_grid_kernel", "classify
                            "cell_grad_barrier32_kernel", "cell_ggn_barrier32_kernel")
 
 
+class Ranks:
+    """One process per GPU (RANK, WORLD_SIZE, LOCAL_RANK from the launcher's environment) and the two collectives the
+    bench takes: a barrier around every timed region and the maximum over ranks of its device time.  Registrations
+    are independent replicas, so nothing else crosses ranks.  backend "nccl" on the GPUs; the CPU tests run the same
+    code over "gloo" with device "cpu"."""
+
+    def __init__(self, backend="nccl", device="cuda", timeout_s=600):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x):
+        """The maximum of x over the ranks (every rank gets it)."""
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def whole_job_rate(pairs_per_rank, seconds, world):
+    """Whole-job pairs/hour: every rank registers pairs_per_rank pairs; seconds is the max over ranks."""
+    return world * pairs_per_rank / seconds * 3600.
+
+
 def phase_summary(phase, timers):
     """Host-clock seconds of one pair's pre-optimizer, transfer and certified loop, the device time of the loop's
     timed kernels and the loop's remainder: host control, syncs and launch gaps."""
@@ -750,11 +793,8 @@ def main():
         return reference_arm(args, shape, config)
 
     import torch
-    import torch.distributed as dist
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    ranks = Ranks("nccl", "cuda")
     import ctypes
     from seq_vp_3d_b200 import _lib
     from seq_vp_3d_b200.grid import make_grid_3d
@@ -784,16 +824,10 @@ def main():
         return res
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        ranks.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     def launches():
         n = ctypes.c_int64()
@@ -836,14 +870,14 @@ def main():
     with Clocks(local) as clocks:
         seconds, per_pair, results = timed_pairs(args.form, args.steps, f_dev, m_dev)
     n1 = launches()
-    value = world * args.steps / seconds * 3600.
+    value = whole_job_rate(args.steps, seconds, world)
     # ---------------------------------------------------------------- e2e: public API from pinned host buffers
     f_host = torch.from_numpy(fixed).pin_memory()
     m_host = torch.from_numpy(moving).pin_memory()
     u_out = torch.empty(grid.shape + (3,), dtype=torch.float64).pin_memory()
     w_out = torch.empty(grid.shape, dtype=torch.float64).pin_memory()
     e2e_seconds, _, _ = timed_pairs(args.form, args.steps, f_host, m_host, copy_back=(u_out, w_out))
-    e2e_value = world * args.steps / e2e_seconds * 3600.
+    e2e_value = whole_job_rate(args.steps, e2e_seconds, world)
     h2d = 2 * fixed.nbytes
     d2h = u_out.numel() * 8 + w_out.numel() * 8
     # ---------------------------------------------------------------- the other form, for the mixed/plain ratio
@@ -852,7 +886,7 @@ def main():
     if args.compare_steps > 0:
         step(f_dev, m_dev, other)
         o_seconds, _, o_results = timed_pairs(other, args.compare_steps, f_dev, m_dev)
-        o_value = world * args.compare_steps / o_seconds * 3600.
+        o_value = whole_job_rate(args.compare_steps, o_seconds, world)
         by = {args.form: (value, results[-1], args.steps), other: (o_value, o_results[-1], args.compare_steps)}
         compare = {k: dict(value=v, ms_per_pair=3.6e6 / v * world, pairs=n, final_mse=r.final_mse,
                            certified=bool(r.certified), outer_accepted=r.counts["outer_accepted"])
@@ -933,9 +967,7 @@ def main():
                                 GF_initial=r.GF_initial, GF_final=r.GF_final, screen=r.counts.get("screen")),
                     phases=phase_summary(timer_phase, timers))
         print(json.dumps(line))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
