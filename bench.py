@@ -228,7 +228,8 @@ def kernel_counts(shape):
 # run on the cells the edge hull leaves unproven, the node-measure extension on candidate cells)
 STATE_DEPENDENT_KERNELS = ("prescreen_kernel", "fallback_grid_kernel", "classify_kernel", "jd_extension_kernel",
                            "jd_root_kernel", "cell_ggn_hvp_kernel", "cell_trial_barrier_kernel",
-                           "cell_grad_barrier32_kernel", "cell_ggn_barrier32_kernel")
+                           "cell_grad_barrier32_kernel", "cell_ggn_barrier32_kernel", "cell_grad_barrier_kernel",
+                           "cell_ggn_barrier_kernel", "cell_trial_diff_kernel")
 
 
 class Ranks:

@@ -454,7 +454,7 @@ __device__ __forceinline__ void point_D(const Q1Const &q, int ix, int iy, int iz
 
 __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const double *__restrict__ u,
                                                            double *__restrict__ L,
-                                                           const uint8_t *__restrict__ active) {
+                                                           const uint8_t *__restrict__ active, bool barrier) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < q.ncell;
          c += (long long)gridDim.x * blockDim.x) {
         double E[3][4][3], out[8][3];
@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(CT) cell_ggn_diag_kernel(Q1Const q, const doub
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) out[a][r] += q.ggn_curl[3 * a + r];
-        if (!active || active[c])
+        if (barrier && (!active || active[c]))
         sweep<true>(E, q, [&](int, int ix, int iy, int iz, const double (&V)[3][3]) {
             if (!(det_only(V) < q.act)) return;
             double A[3][3], J, b, b1, b2;
@@ -756,16 +756,20 @@ __global__ void __launch_bounds__(CS, 8) cell_grad32_kernel(Q1Const q, const dou
 }
 
 // The barrier's locals of the flagged cells in float64: the closed27 sweep from the float64 state, J, b' and the
-// cofactors exactly as the float64 kernel forms them, the flux rounded to float32 and scattered as the float32
-// kernel scatters its own; then added to the cell's locals (L1 += Lb) and, for the outer triple, stored apart (L2).
-__global__ void __launch_bounds__(CB) cell_grad_barrier32_kernel(Q1Const q, const double *__restrict__ u,
-                                                                 const uint8_t *__restrict__ flags, bool split,
-                                                                 float *__restrict__ L1, float *__restrict__ L2) {
-    extern __shared__ float smemf[];
+// cofactors exactly as the float64 kernel forms them, the flux rounded to the locals' type LT (float32 in the mixed
+// form, float64 in the plain one) and scattered as the soft kernel scatters its own; then added to the cell's locals
+// (L1 += Lb) and, for the outer triple, stored apart (L2).  In the plain form the values are those of the fused
+// float64 kernel (the same sweep of the same edges, the same add).
+template <class LT>
+__global__ void __launch_bounds__(CB) cell_grad_barrier_kernel(Q1Const q, const double *__restrict__ u,
+                                                               const uint8_t *__restrict__ flags, bool split,
+                                                               LT *__restrict__ L1, LT *__restrict__ L2) {
+    extern __shared__ __align__(16) unsigned char smemb[];
     __shared__ long long queue[CB / 32][64];
-    float *sl = smemf + threadIdx.x;
+    LT *sl = reinterpret_cast<LT *>(smemb) + threadIdx.x;
     const int T = blockDim.x;
-    const float cn[3] = {0.f, .5f, 1.f}, cm[3] = {1.f, .5f, 0.f};
+    const LT cn[3] = {LT(0), LT(.5), LT(1)}, cm[3] = {LT(1), LT(.5), LT(0)};
+    const LT ih[3] = {(LT)q.ih[0], (LT)q.ih[1], (LT)q.ih[2]};
     for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t) {
         double E64[3][4][3];
         load_edges(u, cell_node0(c, q), q, E64);
@@ -776,21 +780,21 @@ __global__ void __launch_bounds__(CB) cell_grad_barrier32_kernel(Q1Const q, cons
             double A[3][3], J, b, b1, b2;
             cofactor_det(V, A, J);
             barrier_eval(J, q.act, q.delta, q.bw, b, b1, b2);
-            float f[3][3];
+            LT f[3][3];
 #pragma unroll
             for (int r = 0; r < 3; r++)
 #pragma unroll
-                for (int jj = 0; jj < 3; jj++) f[r][jj] = (float)(A[r][jj] * b1);
+                for (int jj = 0; jj < 3; jj++) f[r][jj] = (LT)(A[r][jj] * b1);
             add_flux(sl, T, ix, iy, iz, f);
             any = true;
         });
         if (!any) return;
-        float Lb[8][3];
+        LT Lb[8][3];
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) Lb[a][r] = 0.f;
-        scatter_slice(sl, T, cn, cm, q.ihf, Lb);
+            for (int r = 0; r < 3; r++) Lb[a][r] = LT(0);
+        scatter_slice(sl, T, cn, cm, ih, Lb);
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
@@ -848,15 +852,17 @@ __global__ void __launch_bounds__(CT, 4) cell_ggn_diag32_kernel(Q1Const q, const
 }
 
 // The barrier curvature b'' lc^2 of the flagged cells in float64 (J, b'' and the cofactors lc from the float64
-// state), added point by point in sweep order to the cell's float32 locals.
-__global__ void __launch_bounds__(CB) cell_ggn_barrier32_kernel(Q1Const q, const double *__restrict__ u,
-                                                                const uint8_t *__restrict__ flags,
-                                                                float *__restrict__ L) {
+// state), rounded to the locals' type LT and added point by point in sweep order to the cell's locals (in the plain
+// form the additions of the fused float64 kernel).
+template <class LT>
+__global__ void __launch_bounds__(CB) cell_ggn_barrier_kernel(Q1Const q, const double *__restrict__ u,
+                                                              const uint8_t *__restrict__ flags,
+                                                              LT *__restrict__ L) {
     __shared__ long long queue[CB / 32][64];
     for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t) {
         double E64[3][4][3];
         load_edges(u, cell_node0(c, q), q, E64);
-        float out[8][3];
+        LT out[8][3];
 #pragma unroll
         for (int a = 0; a < 8; a++)
 #pragma unroll
@@ -875,7 +881,8 @@ __global__ void __launch_bounds__(CB) cell_ggn_barrier32_kernel(Q1Const q, const
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double lc = A[r][0] * D[0] + A[r][1] * D[1] + A[r][2] * D[2];
-                    out[a][r] += (float)(b2 * lc * lc);
+                    if constexpr (sizeof(LT) == 8) out[a][r] += b2 * lc * lc;   // the fused kernel's expression
+                    else out[a][r] += (LT)(b2 * lc * lc);
                 }
             }
         });
@@ -1036,7 +1043,8 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
                                                         const double *__restrict__ ub,
                                                         const double *__restrict__ uref, dd *pe, dd *pd,
                                                         unsigned long long *bad, uint8_t *__restrict__ trial_act,
-                                                        const uint8_t *__restrict__ base_act) {
+                                                        const uint8_t *__restrict__ base_act,
+                                                        uint8_t *__restrict__ flags) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -1081,7 +1089,12 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
                 sb += b;
             }
         });
-        if (active || !base_act || base_act[c]) {
+        // the barrier differences of the cells where the trial or the base is active: here, or (flags) in
+        // cell_trial_diff_kernel over those cells alone
+        const bool needs = active || !base_act || base_act[c];
+        if (flags) {
+            flags[c] = needs ? 1 : 0;
+        } else if (needs) {
             load_edges(ua, n0, q, Ea);
             sweep<true>(Ea, q, [&](int p, int, int, int, const double (&Va)[3][3]) {
                 const double ja = det_only(Va), jb = sl[p * T];
@@ -1101,6 +1114,34 @@ __global__ void __launch_bounds__(CS) cell_trial_kernel(Q1Const q, const double 
     block_reduce_dd<3>(dif, pd);
     for (int o = 16; o; o >>= 1) nbad += __shfl_xor_sync(0xFFFFFFFFu, nbad, o);
     if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, nbad);
+}
+
+// The float64 trial's barrier differences of the flagged cells (trial or base active), as cell_trial_kernel forms
+// them per cell: the trial's closed27 J from its edges, the base's, psi differences where either is below the
+// activation.  pd: per block, the barrier difference sum.
+__global__ void __launch_bounds__(CB) cell_trial_diff_kernel(Q1Const q, const double *__restrict__ ua,
+                                                             const double *__restrict__ ub,
+                                                             const uint8_t *__restrict__ flags, dd *pd) {
+    extern __shared__ double smem[];
+    __shared__ long long queue[CB / 32][64];
+    double *dsl = smem + threadIdx.x;
+    const int T = blockDim.x;
+    dd dif[1] = {{0., 0.}};
+    for_flagged_cells(q, flags, queue[threadIdx.x >> 5], [&](long long c, uint8_t) {
+        const long long n0 = cell_node0(c, q);
+        double E[3][4][3];
+        load_edges(ub, n0, q, E);
+        sweep<true>(E, q, [&](int p, int, int, int, const double (&Vb)[3][3]) { dsl[p * T] = det_only(Vb); });
+        load_edges(ua, n0, q, E);
+        double sbd = 0.;
+        sweep<true>(E, q, [&](int p, int, int, int, const double (&Va)[3][3]) {
+            const double ja = det_only(Va), jb = dsl[p * T];
+            if (ja < q.act || jb < q.act) sbd += barrier_difference(ja, jb, q.act, q.delta);
+        });
+        acc_add(dif[0], dd{q.bw * sbd, 0.});
+    });
+    dif[0] = two_sum(dif[0].hi, dif[0].lo);
+    block_reduce_dd<1>(dif, pd);
 }
 
 // ============================================================================================== screened trial
@@ -1787,6 +1828,8 @@ int allow_slices() {
                                   (int)slice_bytes(108)));
     SVP_CUDA(cudaFuncSetAttribute(cell_trial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)slice_bytes(108)));
+    SVP_CUDA(cudaFuncSetAttribute(cell_grad_barrier_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * 81 * CB)));
     done[dev] = true;
     return SVP_OK;
 }
@@ -2028,10 +2071,21 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
         SVP_LAUNCH(cell_trial_barrier_kernel<<<bb, CB, sizeof(double) * 27 * CB, s>>>(
             p->q, base_u, trial_u, p->flags, pbe, pbd, (unsigned long long *)p->counter, trial_active, base_active));
     } else {
-        svp::KernelTimer _t("cell_trial_kernel", s);
-        SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pce, pcd,
-                                                                     (unsigned long long *)p->counter, trial_active,
-                                                                     base_active));
+        // with the base's mask, the barrier differences of the cells where the trial or the base is active run in
+        // cell_trial_diff_kernel over those cells alone (per cell the fused kernel's values)
+        const bool apart = base_active != nullptr;
+        if (apart && (rc = pair_flags(p))) return rc;
+        {
+            svp::KernelTimer _t("cell_trial_kernel", s);
+            SVP_LAUNCH(cell_trial_kernel<<<cb, CS, slice_bytes(108), s>>>(
+                p->q, base_u, trial_u, p->u_ref, pce, pcd, (unsigned long long *)p->counter, trial_active,
+                base_active, apart ? p->flags : nullptr));
+        }
+        if (apart) {
+            svp::KernelTimer _t("cell_trial_diff_kernel", s);
+            SVP_LAUNCH(cell_trial_diff_kernel<<<bb, CB, sizeof(double) * 27 * CB, s>>>(p->q, base_u, trial_u,
+                                                                                     p->flags, pbd));
+        }
     }
     SVP_LAUNCH_CHECK("cell_trial_kernel");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pne, nb, 2, p->result));
@@ -2046,6 +2100,8 @@ static int trial_energy(svp_pair *p, const double *base_u, const double *base_wa
     } else {
         SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pce, cb, 3, p->result + 4));
         SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pcd, cb, 3, p->result + 14));
+        // the barrier difference from its own kernel in place of the fused kernel's (zero) one
+        if (base_active) SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pbd, bb, 1, p->result + 18));
     }
     SVP_LAUNCH_CHECK("final_reduce_kernel");
     double tmp[28];
@@ -2118,6 +2174,28 @@ static int run_gather(svp_pair *p, const GatherSpec &g, const LT *L1, const LT *
     return SVP_OK;
 }
 
+// The plain form's gradient locals: with the state's activity mask, the soft float64 kernel and then the barrier
+// kernel over the active cells (the values of the fused kernel: the same sweep, the same add); without a mask the
+// fused kernel sweeps the barrier of every cell.
+static int grad64(svp_pair *p, const double *u, double mu_scale, double nu_scale, bool barrier, bool split,
+                  const uint8_t *active, cudaStream_t s) {
+    const bool apart = barrier && active;
+    int rc = allow_slices();
+    if (rc) return rc;
+    {
+        svp::KernelTimer _t("cell_grad_kernel", s);
+        SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(
+            p->q, u, p->u_ref, mu_scale, nu_scale, barrier && !apart, split, p->loc1, split ? p->loc2 : nullptr,
+            active));
+    }
+    if (apart) {
+        svp::KernelTimer _t("cell_grad_barrier_kernel", s);
+        SVP_LAUNCH(cell_grad_barrier_kernel<double><<<barrier_blocks(p->q), CB, sizeof(double) * 81 * CB, s>>>(
+            p->q, u, active, split, p->loc1, split ? p->loc2 : nullptr));
+    }
+    return SVP_OK;
+}
+
 // The mixed form's gradient locals: the float32 soft kernel, then the float64 barrier kernel over the flagged cells
 // (the state's mask, or without one the cells the soft kernel flags from its float32 closed27 J).
 static int grad32(svp_pair *p, const double *u, double mu_scale, double nu_scale, bool barrier, bool split,
@@ -2132,7 +2210,7 @@ static int grad32(svp_pair *p, const double *u, double mu_scale, double nu_scale
     }
     if (barrier) {
         svp::KernelTimer _t("cell_grad_barrier32_kernel", s);
-        SVP_LAUNCH(cell_grad_barrier32_kernel<<<barrier_blocks(p->q), CB, sizeof(float) * 81 * CB, s>>>(
+        SVP_LAUNCH(cell_grad_barrier_kernel<float><<<barrier_blocks(p->q), CB, sizeof(float) * 81 * CB, s>>>(
             p->q, u, active ? active : flags, split, (float *)p->loc1, (float *)p->loc2));
     }
     return SVP_OK;
@@ -2155,9 +2233,10 @@ extern "C" int svp_gradient_masked(svp_pair *p, const double *u, const double *w
                              (terms & SVP_TERM_BARRIER) != 0, false, active, s)))
                 return rc;
         } else {
-            svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, (terms & SVP_TERM_JD) ? 1. : 0.,
-                                                       (terms & SVP_TERM_CURL) ? 1. : 0.,
-                                                       (terms & SVP_TERM_BARRIER) != 0, false, p->loc1, nullptr, active)); }
+            if ((rc = grad64(p, u, (terms & SVP_TERM_JD) ? 1. : 0., (terms & SVP_TERM_CURL) ? 1. : 0.,
+                             (terms & SVP_TERM_BARRIER) != 0, false, active, s)))
+                return rc;
+        }
         SVP_LAUNCH_CHECK("cell_grad_kernel");
     }
     GatherSpec g{};
@@ -2184,7 +2263,8 @@ extern "C" int svp_outer_gradients_masked(svp_pair *p, const double *u, const do
     if (mixed) {
         if ((rc = grad32(p, u, 1., 1., true, true, active, s))) return rc;
     } else {
-        svp::KernelTimer _t("cell_grad_kernel", s); SVP_LAUNCH(cell_grad_kernel<<<slice_blocks(p), CS, slice_bytes(81), s>>>(p->q, u, p->u_ref, 1., 1., true, true, p->loc1, p->loc2, active)); }
+        if ((rc = grad64(p, u, 1., 1., true, true, active, s))) return rc;
+    }
     SVP_LAUNCH_CHECK("cell_grad_kernel");
     GatherSpec g{};
     g.nout = 3;
@@ -2211,12 +2291,20 @@ extern "C" int svp_ggn_diagonal_masked(svp_pair *p, const double *u, const doubl
         }
         {
             svp::KernelTimer _t("cell_ggn_barrier32_kernel", s);
-            SVP_LAUNCH(cell_ggn_barrier32_kernel<<<barrier_blocks(p->q), CB, 0, s>>>(
+            SVP_LAUNCH(cell_ggn_barrier_kernel<float><<<barrier_blocks(p->q), CB, 0, s>>>(
                 p->q, u, active ? active : p->flags, (float *)p->loc1));
         }
         SVP_LAUNCH(ggn_node_kernel<float><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, (const float *)p->loc1, image_grad, nullptr, out));
     } else {
-        { svp::KernelTimer _t("cell_ggn_diag_kernel", s); SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1, active)); }
+        // with the state's mask, the barrier curvature of the active cells in its own kernel (the same values)
+        {
+            svp::KernelTimer _t("cell_ggn_diag_kernel", s);
+            SVP_LAUNCH(cell_ggn_diag_kernel<<<cell_blocks(p), CT, 0, s>>>(p->q, u, p->loc1, active, active == nullptr));
+        }
+        if (active) {
+            svp::KernelTimer _t("cell_ggn_barrier_kernel", s);
+            SVP_LAUNCH(cell_ggn_barrier_kernel<double><<<barrier_blocks(p->q), CB, 0, s>>>(p->q, u, active, p->loc1));
+        }
         SVP_LAUNCH(ggn_node_kernel<double><<<node_blocks(p->q.nfree), 256, 0, s>>>(p->q, p->loc1, image_grad, nullptr, out));
     }
     SVP_LAUNCH_CHECK("ggn diagonal");
