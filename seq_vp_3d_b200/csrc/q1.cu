@@ -945,7 +945,8 @@ __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *
                                                        const double *__restrict__ ub,
                                                        const double *__restrict__ uref, dd *partial,
                                                        const uint8_t *__restrict__ act_a,
-                                                       const uint8_t *__restrict__ act_b) {
+                                                       const uint8_t *__restrict__ act_b,
+                                                       uint8_t *__restrict__ flags) {
     extern __shared__ double smem[];
     double *sl = smem + threadIdx.x;
     const int T = blockDim.x;
@@ -971,8 +972,12 @@ __global__ void __launch_bounds__(CS) cell_diff_kernel(Q1Const q, const double *
             }
         });
         double sb = 0.;
-        // with both masks, a cell inactive in both fields has no barrier difference at all
-        if (!(act_a && act_b && !act_a[c] && !act_b[c]))
+        // with both masks, a cell inactive in both fields has no barrier difference at all; with flags, the cells
+        // that have one are handed to cell_trial_diff_kernel (the same per-cell value)
+        const bool needs = !(act_a && act_b && !act_a[c] && !act_b[c]);
+        if (flags)
+            flags[c] = needs ? 1 : 0;
+        else if (needs)
             sweep2<true>(Ea, Eb, q, [&](int, int, int, int, const double (&Va)[3][3], const double (&Vb)[3][3]) {
                 double ja = det_only(Va), jb = det_only(Vb);
                 if (ja < q.act || jb < q.act) sb += barrier_difference(ja, jb, q.act, q.delta);
@@ -1935,18 +1940,32 @@ extern "C" int svp_energy_difference_masked(svp_pair *p, const double *base_u, c
                                             void *stream) {
     SVP_REQUIRE(p && base_u && base_warped && trial_u && trial_warped && diff2, "svp_energy_difference: null");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p);
-    int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3, 1);
+    unsigned nb = node_blocks(p->q.nnode), cb = slice_blocks(p), bb = barrier_blocks(p->q);
+    int rc = pair_partials(p, (long long)nb * 2 + (long long)cb * 3 + bb, 1);
     if (rc) return rc;
     rc = allow_slices();
     if (rc) return rc;
+    // with both states' masks, the barrier differences of the cells active in either run in cell_trial_diff_kernel
+    // over those cells alone (per cell the same value)
+    const bool apart = base_active && trial_active;
+    if (apart && (rc = pair_flags(p))) return rc;
     { svp::KernelTimer _t("node_diff_kernel", s); SVP_LAUNCH(node_diff_kernel<<<nb, 256, 0, s>>>(p->q, base_u, base_warped, trial_u, trial_warped, p->fixed, p->u_ref,
                                         p->partial)); }
-    dd *pc = p->partial + (long long)nb * 2;
-    { svp::KernelTimer _t("cell_diff_kernel", s); SVP_LAUNCH(cell_diff_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pc, base_active, trial_active)); }
+    dd *pc = p->partial + (long long)nb * 2, *pb = pc + (long long)cb * 3;
+    {
+        svp::KernelTimer _t("cell_diff_kernel", s);
+        SVP_LAUNCH(cell_diff_kernel<<<cb, CS, slice_bytes(108), s>>>(p->q, base_u, trial_u, p->u_ref, pc, base_active,
+                                                                    trial_active, apart ? p->flags : nullptr));
+    }
+    if (apart) {
+        svp::KernelTimer _t("cell_trial_diff_kernel", s);
+        SVP_LAUNCH(cell_trial_diff_kernel<<<bb, CB, sizeof(double) * 27 * CB, s>>>(p->q, base_u, trial_u, p->flags,
+                                                                                 pb));
+    }
     SVP_LAUNCH_CHECK("difference kernels");
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(p->partial, nb, 2, p->result));
     SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pc, cb, 3, p->result + 4));
+    if (apart) SVP_LAUNCH(final_reduce_kernel<<<1, 256, 0, s>>>(pb, bb, 1, p->result + 8));
     SVP_LAUNCH_CHECK("final_reduce_kernel");
     double tmp[10];
     SVP_CUDA(cudaMemcpyAsync(tmp, p->result, sizeof tmp, cudaMemcpyDeviceToHost, s));
